@@ -1,0 +1,368 @@
+"""Host-side mirror of the reference's element assembler, backed by libfne_asm.so.
+
+``CudaElementAssemblerBase`` keeps the public surface of
+``ReorderedElementAssemblerBase`` (``src/core/petsc/reordered_element_base.py:642``):
+``energy_fn(vec)`` (:1579), ``gradient_fn(vec, g)`` (:1613),
+``assemble_hessian(u_owned, variant=2)`` (:1635), ``update_dirichlet(u0)``
+(:1560), ``create_vec(full)`` (:1568), ``cleanup()`` (:1777),
+``callback_summary()`` / ``setup_summary()`` / ``iter_timings``, and the same
+layout (``self.layout``: ``perm, iperm, lo, hi, n_free, total_to_free_reord,
+owned_rows, owned_cols``).  Vectors may be CUDA tensors (zero copy), NumPy
+arrays, or objects with an ``.array`` attribute (PETSc ``Vec``).  The owned
+Hessian values land in ``self.owned_values`` (a CUDA tensor, COO order of
+``layout.owned_rows/owned_cols``); when a PETSc matrix is attached as
+``self.A`` they are handed to ``A.setValuesCOO`` unchanged, as the reference
+does (:1046-1050).
+
+Family subclasses mirror the reference's ``_make_local_element_kernels``
+implementations; the kernels themselves are in ``csrc/fne_asm.cu``.
+"""
+
+from __future__ import annotations
+
+import time
+from types import SimpleNamespace
+
+import numpy as np
+import torch
+
+from fenics_nonlinear_energies_b200 import _lib
+from fenics_nonlinear_energies_b200._lib import check, lib
+
+_DTYPES = {"fp64": _lib.FNE_FP64, "fp32": _lib.FNE_FP32}
+
+
+def _comm_rank_size(comm):
+    if comm is None:
+        return 0, 1
+    if hasattr(comm, "Get_rank"):
+        return int(comm.Get_rank()), int(comm.Get_size())
+    return int(getattr(comm, "rank", 0)), int(getattr(comm, "size", 1))
+
+
+class CudaElementAssemblerBase:
+    """Element energy / gradient / Hessian assembly on one CUDA device."""
+
+    family = 0
+    npe = 3
+    block_size = 1
+    coordinate_key = "nodes"
+    dirichlet_key = "u_0"
+    local_elem_data_keys: tuple[str, ...] = ()
+
+    def __init__(self, params, comm=None, adjacency=None, *, reorder_mode="block_xyz", perm_override=None,
+                 precision="fp64", hess_dtype=None, device=None, **_ignored_solver_kwargs):
+        if not torch.cuda.is_available():
+            raise RuntimeError("CudaElementAssemblerBase needs a CUDA device (no CPU fallback)")
+        t_setup = time.perf_counter()
+        self.params = params
+        self.comm = comm
+        self.rank, self.size = _comm_rank_size(comm)
+        self.precision = str(precision)
+        if self.precision not in _DTYPES:
+            raise ValueError(f"precision must be 'fp64' or 'fp32', got {precision!r}")
+        if hess_dtype is None:
+            hess_dtype = torch.float64
+        if self.precision == "fp64" and hess_dtype != torch.float64:
+            raise ValueError("fp64 mode produces float64 Hessian values")
+        self.hess_dtype = hess_dtype
+        self.device = torch.device(device if device is not None else f"cuda:{torch.cuda.current_device()}")
+        torch.cuda.set_device(self.device)
+        self.iter_timings: list[dict] = []
+        self._setup_timings: dict[str, float] = {}
+        self._callback_stats = {
+            "energy": {"calls": 0, "kernel": 0.0, "total": 0.0},
+            "gradient": {"calls": 0, "kernel": 0.0, "total": 0.0},
+            "hessian": {"calls": 0, "hvp_compute": 0.0, "extraction": 0.0, "coo_assembly": 0.0, "total": 0.0},
+        }
+
+        freedofs = np.asarray(params["freedofs"], dtype=np.int64)
+        elems = np.asarray(params["elems"], dtype=np.int64)
+        n_total = len(np.asarray(params[self.dirichlet_key]))
+        t0 = time.perf_counter()
+        lay = _lib.build_layout(
+            freedofs=freedofs, elems=elems, n_total=n_total, block_size=self.block_size,
+            reorder=reorder_mode, coords=np.asarray(params[self.coordinate_key], dtype=np.float64),
+            perm_override=perm_override, adjacency=adjacency, rank=self.rank, size=self.size,
+        )
+        self._setup_timings["global_layout"] = time.perf_counter() - t0
+        self.layout = SimpleNamespace(**lay)
+        self.part = SimpleNamespace(perm=lay["perm"], iperm=lay["iperm"], lo=lay["lo"], hi=lay["hi"],
+                                    n_free=lay["n_free"], n_owned=lay["hi"] - lay["lo"])
+        self.n_owned = lay["hi"] - lay["lo"]
+        self.dirichlet_full = np.asarray(params[self.dirichlet_key], dtype=np.float64).copy()
+        weights = (lay["elem_owner"] == self.rank).astype(np.float64)
+
+        t0 = time.perf_counter()
+        keep = []
+        d = _lib.Desc()
+        d.family = self.family
+        d.precision = _DTYPES[self.precision]
+        d.hess_fp32 = 1 if hess_dtype == torch.float32 else 0
+        el, d.elems = _lib.i64(elems)
+        t2f, d.total_to_free_reord = _lib.i64(lay["total_to_free_reord"])
+        orows, d.owned_rows = _lib.i64(lay["owned_rows"])
+        ocols, d.owned_cols = _lib.i64(lay["owned_cols"])
+        w, d.energy_weights = _lib.f64(weights)
+        dirv, d.dirichlet = _lib.f64(self.dirichlet_full)
+        keep += [el, t2f, orows, ocols, w, dirv]
+        d.n_elem, d.npe, d.block_size = int(el.shape[0]), self.npe, self.block_size
+        d.n_total, d.n_free = int(n_total), int(lay["n_free"])
+        d.lo, d.hi, d.nnz = int(lay["lo"]), int(lay["hi"]), int(orows.size)
+        rhs = self._build_rhs_owned()
+        self._f_owned = rhs
+        if rhs is not None:
+            r, d.rhs_owned = _lib.f64(rhs)
+            keep.append(r)
+        for slot, arr in zip(("e0", "e1", "e2", "e3"), self._element_arrays()):
+            a, p = _lib.f64(arr)
+            keep.append(a)
+            setattr(d, slot, p)
+        for i, v in enumerate(self._scalars()):
+            d.s[i] = float(v)
+        d.nq = int(self._nq())
+        d.dirichlet_only_energy = 1 if (self._adds_dirichlet_only_energy() and self.rank == 0) else 0
+        self._handle = _lib.C.c_void_p()
+        check(lib.fne_create(_lib.C.byref(d), _lib.C.byref(self._handle)))
+        del keep
+        self._setup_timings["kernel_build"] = time.perf_counter() - t0
+        info = _lib.Info()
+        check(lib.fne_info_get(self._handle, _lib.C.byref(info)))
+        self.info = {k: getattr(info, k) for k, _ in _lib.Info._fields_}
+
+        dev = self.device
+        self._u = torch.zeros(max(1, int(lay["n_free"])), dtype=torch.float64, device=dev)
+        self._grad = torch.zeros(max(1, self.n_owned), dtype=torch.float64, device=dev)
+        self._energy = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.owned_values = torch.zeros(int(orows.size), dtype=hess_dtype, device=dev)
+        self.A = None  # optional PETSc Mat (drop-in handoff)
+        self._ev0 = torch.cuda.Event(enable_timing=True)
+        self._ev1 = torch.cuda.Event(enable_timing=True)
+        self._setup_timings["total"] = time.perf_counter() - t_setup
+
+    # ---- family hooks (overridden) -----------------------------------------
+    def _element_arrays(self):
+        return [np.asarray(self.params[k], dtype=np.float64) for k in self.local_elem_data_keys]
+
+    def _scalars(self):
+        return []
+
+    def _nq(self):
+        return 0
+
+    def _build_rhs_owned(self):
+        return None
+
+    def _adds_dirichlet_only_energy(self):
+        return False
+
+    # ---- vector helpers -----------------------------------------------------
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _as_u(self, vec):
+        """Device float64 view of the full reordered free vector."""
+        arr = getattr(vec, "array", vec)
+        if isinstance(arr, torch.Tensor):
+            if arr.device == self.device and arr.dtype == torch.float64 and arr.is_contiguous():
+                if arr.numel() == self.layout.n_free:
+                    return arr
+            self._u[: self.layout.n_free].copy_(arr.reshape(-1), non_blocking=True)
+            return self._u
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        if a.size != self.layout.n_free:
+            raise ValueError(f"vector has {a.size} entries, expected {self.layout.n_free}")
+        self._u[: a.size].copy_(torch.from_numpy(a), non_blocking=False)
+        return self._u
+
+    def create_vec(self, full_array_reordered=None):
+        """Device vector of the owned range (the reference returns a PETSc Vec)."""
+        v = torch.zeros(self.n_owned, dtype=torch.float64, device=self.device)
+        if full_array_reordered is not None:
+            a = torch.as_tensor(np.asarray(full_array_reordered, dtype=np.float64))
+            v.copy_(a[self.layout.lo: self.layout.hi])
+        return v
+
+    # ---- device-level API ---------------------------------------------------
+    def eval(self, u, flags, *, energy=None, grad=None, hess=None):
+        """One fused kernel pass on the current stream; returns the output tensors."""
+        u = self._as_u(u)
+        energy = self._energy if energy is None else energy
+        grad = self._grad if grad is None else grad
+        hess = self.owned_values if hess is None else hess
+        check(lib.fne_eval(
+            self._handle, u.data_ptr(), int(flags),
+            energy.data_ptr() if flags & _lib.FNE_ENERGY else None,
+            grad.data_ptr() if flags & _lib.FNE_GRAD else None,
+            hess.data_ptr() if flags & _lib.FNE_HESS else None,
+            self._stream(),
+        ))
+        return energy, grad, hess
+
+    def energy_device(self, u):
+        """Energy as a 1-element CUDA tensor (no host synchronisation)."""
+        return self.eval(u, _lib.FNE_ENERGY)[0]
+
+    # ---- reference callbacks ------------------------------------------------
+    def energy_fn(self, vec):
+        t = time.perf_counter()
+        self._ev0.record()
+        e = self.eval(vec, _lib.FNE_ENERGY)[0]
+        self._ev1.record()
+        val = float(e.item())
+        st = self._callback_stats["energy"]
+        st["calls"] += 1
+        st["kernel"] += self._ev0.elapsed_time(self._ev1) * 1e-3
+        st["total"] += time.perf_counter() - t
+        return val
+
+    def gradient_fn(self, vec, g):
+        t = time.perf_counter()
+        self._ev0.record()
+        _, grad, _ = self.eval(vec, _lib.FNE_GRAD)
+        self._ev1.record()
+        out = getattr(g, "array", g)
+        if isinstance(out, torch.Tensor):
+            out.copy_(grad[: self.n_owned])
+        else:
+            out[:] = grad[: self.n_owned].cpu().numpy()
+        st = self._callback_stats["gradient"]
+        st["calls"] += 1
+        torch.cuda.current_stream(self.device).synchronize()
+        st["kernel"] += self._ev0.elapsed_time(self._ev1) * 1e-3
+        st["total"] += time.perf_counter() - t
+
+    def assemble_hessian(self, u_owned, variant=2):
+        del variant
+        return self.assemble_hessian_element(u_owned)
+
+    def assemble_hessian_element(self, u_owned):
+        t_total = time.perf_counter()
+        self._ev0.record()
+        self.eval(u_owned, _lib.FNE_HESS)
+        self._ev1.record()
+        self._ev1.synchronize()
+        t_k = self._ev0.elapsed_time(self._ev1) * 1e-3
+        timings = {"elem_hessian_compute": t_k, "scatter": 0.0, "hvp_compute": t_k, "extraction": 0.0,
+                   "allgatherv": 0.0, "ghost_exchange": 0.0, "build_v_local": 0.0, "p2p_exchange": 0.0,
+                   "n_hvps": 0, "assembly_mode": "element_overlap_cuda"}
+        t0 = time.perf_counter()
+        if self.A is not None:
+            self.A.setValuesCOO(self.owned_values.double().cpu().numpy(), addv=1)
+            self.A.assemble()
+        timings["coo_assembly"] = time.perf_counter() - t0
+        timings["total"] = time.perf_counter() - t_total
+        self.iter_timings.append(timings)
+        st = self._callback_stats["hessian"]
+        st["calls"] += 1
+        st["hvp_compute"] += t_k
+        st["coo_assembly"] += timings["coo_assembly"]
+        st["total"] += timings["total"]
+        return timings
+
+    def update_dirichlet(self, u_0_new):
+        self.dirichlet_full = np.ascontiguousarray(u_0_new, dtype=np.float64).copy()
+        a, p = _lib.f64(self.dirichlet_full)
+        check(lib.fne_set_dirichlet(self._handle, p))
+
+    def owned_values_host(self):
+        return self.owned_values.cpu().numpy()
+
+    def setup_summary(self):
+        return {k: float(v) for k, v in self._setup_timings.items()}
+
+    def callback_summary(self):
+        return {k: dict(v) for k, v in self._callback_stats.items()}
+
+    def memory_summary(self):
+        return {"device_bytes": int(self.info["device_bytes"]), "owned_nnz": int(self.layout.owned_rows.size),
+                "local_elements": int(self.info["n_elem"])}
+
+    def cleanup(self):
+        if getattr(self, "_handle", None):
+            lib.fne_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.cleanup()
+        except Exception:
+            pass
+
+
+class PLaplaceCudaAssembler(CudaElementAssemblerBase):
+    """``PLaplaceReorderedElementAssembler`` (plaplace/jax_petsc/reordered_element_assembler.py:22-72)."""
+
+    family = _lib.FNE_PLAPLACE
+    npe, block_size = 3, 1
+    coordinate_key, dirichlet_key = "nodes", "u_0"
+    local_elem_data_keys = ("dvx", "dvy", "vol")
+
+    def _scalars(self):
+        return [float(self.params["p"])]
+
+    def _build_rhs_owned(self):
+        """``_build_rhs_owned`` (:67-72): f[freedofs][perm][lo:hi]."""
+        rhs = np.asarray(self.params["f"], dtype=np.float64)
+        free = np.asarray(self.params["freedofs"], dtype=np.int64)
+        return np.ascontiguousarray(rhs[free][self.layout.perm][self.layout.lo: self.layout.hi])
+
+
+class GLCudaAssembler(CudaElementAssemblerBase):
+    """``GLReorderedElementAssembler`` (ginzburg_landau/jax_petsc/reordered_element_assembler.py:27-97)."""
+
+    family = _lib.FNE_GINZBURG_LANDAU
+    npe, block_size = 3, 1
+    coordinate_key, dirichlet_key = "nodes", "u_0"
+    local_elem_data_keys = ("dvx", "dvy", "vol")
+
+    def _scalars(self):
+        ip = np.asarray(self.params["ip"], dtype=np.float64).reshape(3, 3)
+        w = np.asarray(self.params["w"], dtype=np.float64).reshape(3)
+        return [float(self.params["eps"]), *ip.ravel().tolist(), *w.tolist()]
+
+    def _adds_dirichlet_only_energy(self):
+        return True
+
+
+class HECudaAssembler(CudaElementAssemblerBase):
+    """``HEReorderedElementAssembler`` (hyperelasticity/jax_petsc/reordered_element_assembler.py:16-101)."""
+
+    family = _lib.FNE_NEOHOOKEAN
+    npe, block_size = 4, 3
+    coordinate_key, dirichlet_key = "nodes2coord", "u_0_ref"
+    local_elem_data_keys = ("dphix", "dphiy", "dphiz", "vol")
+
+    def __init__(self, params, comm=None, adjacency=None, *, use_abs_det=False, **kw):
+        self.use_abs_det = bool(use_abs_det)
+        super().__init__(params, comm, adjacency, **kw)
+
+    def _scalars(self):
+        return [float(self.params["C1"]), float(self.params["D1"]), 1.0 if self.use_abs_det else 0.0]
+
+
+class EnergyFunction(torch.autograd.Function):
+    """``J(u)`` with ``dJ/du`` from the hand-written adjoint kernels.
+
+    forward: one fused ENERGY|GRAD pass (the gradient is kept for backward);
+    backward: ``grad_out * gradient``.  The Hessian is not part of the autograd
+    graph: call ``assembler.assemble_hessian`` explicitly.
+    """
+
+    @staticmethod
+    def forward(ctx, u, assembler):
+        e, g, _ = assembler.eval(u.detach().contiguous(), _lib.FNE_ENERGY | _lib.FNE_GRAD,
+                                 energy=torch.empty(1, dtype=torch.float64, device=assembler.device),
+                                 grad=torch.empty(assembler.n_owned, dtype=torch.float64, device=assembler.device))
+        ctx.save_for_backward(g)
+        return e[0]
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (g,) = ctx.saved_tensors
+        return grad_out * g, None
+
+
+def energy(u, assembler):
+    """Differentiable energy: ``energy(u, asm).backward()`` fills ``u.grad``."""
+    return EnergyFunction.apply(u, assembler)

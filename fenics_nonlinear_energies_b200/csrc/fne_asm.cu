@@ -1,0 +1,1098 @@
+// libfne_asm.so -- element energy / gradient / Hessian assembly on sm_100a.
+//
+// Two kernel shapes (one per launch, no atomics, bit-reproducible):
+//
+//  * row-gather kernels (k_rows_tri, k_rows_tet): one thread per OUTPUT ROW
+//    of the owned COO pattern.  A CTA owns a contiguous block of rows, which
+//    is a contiguous slice of the COO value array -- the reference's overlap
+//    domain (every element touching an owned row is evaluated, owned rows
+//    need no reduction; src/core/petsc/reordered_element_base.py:509-597)
+//    applied at CTA granularity.  A thread walks the incidences of its row's
+//    node, evaluates the element's gradient entry and Hessian row with
+//    hand-written adjoints, and accumulates them in shared memory laid out
+//    exactly like the CTA's output slice; the slice is then written with
+//    fully coalesced stores.  The energy (FP64) is added once per element by
+//    the incidence that carries the element's energy flag.
+//  * element kernels (k_energy_*): one thread per element, FP64 energy only
+//    (the golden-section / trust-region line-search callback).
+//
+// Energies always reduce in FP64: warp shuffles, a per-CTA partial, and the
+// last CTA to finish (atomic ticket, no waiting) sums the partials in index
+// order, so the result does not depend on CTA scheduling.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "fne_internal.h"
+
+namespace fne {
+static thread_local std::string g_err;
+int set_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace fne
+
+using namespace fne;
+
+// ---------------------------------------------------------------------------
+// parameters and element records
+// ---------------------------------------------------------------------------
+struct Phys {
+  double p;       // p-Laplace exponent
+  double eps;     // GL
+  double ip[9];   // GL ip[a*3+q]
+  double w[3];    // GL quadrature weights
+  double C1, D1;  // Neo-Hookean
+  int absdet;
+};
+
+// P1 triangle record.  FP32: 48 B (3 x 16 B loads); FP64: 80 B (5 x 16 B).
+struct __align__(16) TriRecF {
+  int src[3];
+  int wflag;
+  float dvx[3];
+  float vol;
+  float dvy[3];
+  float pad;
+};
+struct __align__(16) TriRecD {
+  int src[3];
+  int wflag;
+  double vol, dvx[3], dvy[3], pad;
+};
+// P1 tetrahedron record.  FP32: 80 B; FP64: 128 B.
+struct __align__(16) TetRecF {
+  int src[4];
+  float gx[4], gy[4], gz[4];
+  float vol;
+  int wflag;
+  float pad[2];
+};
+struct __align__(16) TetRecD {
+  int src[4];
+  double gx[4], gy[4], gz[4];
+  double vol;
+  int wflag;
+  int pad;
+};
+
+template <typename Real>
+struct TriRecT;
+template <>
+struct TriRecT<float> {
+  using T = TriRecF;
+};
+template <>
+struct TriRecT<double> {
+  using T = TriRecD;
+};
+template <typename Real>
+struct TetRecT;
+template <>
+struct TetRecT<float> {
+  using T = TetRecF;
+};
+template <>
+struct TetRecT<double> {
+  using T = TetRecD;
+};
+
+template <typename Real>
+struct TriElem {
+  int src[3];
+  int wflag;
+  Real dvx[3], dvy[3], vol;
+};
+template <typename Real>
+struct TetElem {
+  int src[4];
+  int wflag;
+  Real g[4][3];
+  Real vol;
+};
+
+__device__ __forceinline__ void load_tri(const TriRecF* __restrict__ R, int e, TriElem<float>& t) {
+  const int4* p = reinterpret_cast<const int4*>(R + e);
+  const int4 c0 = __ldg(p);
+  const float4 c1 = __ldg(reinterpret_cast<const float4*>(p + 1));
+  const float4 c2 = __ldg(reinterpret_cast<const float4*>(p + 2));
+  t.src[0] = c0.x; t.src[1] = c0.y; t.src[2] = c0.z; t.wflag = c0.w;
+  t.dvx[0] = c1.x; t.dvx[1] = c1.y; t.dvx[2] = c1.z; t.vol = c1.w;
+  t.dvy[0] = c2.x; t.dvy[1] = c2.y; t.dvy[2] = c2.z;
+}
+__device__ __forceinline__ void load_tri(const TriRecD* __restrict__ R, int e, TriElem<double>& t) {
+  const int4* p = reinterpret_cast<const int4*>(R + e);
+  const int4 c0 = __ldg(p);
+  const double2 d0 = __ldg(reinterpret_cast<const double2*>(p + 1));
+  const double2 d1 = __ldg(reinterpret_cast<const double2*>(p + 2));
+  const double2 d2 = __ldg(reinterpret_cast<const double2*>(p + 3));
+  const double2 d3 = __ldg(reinterpret_cast<const double2*>(p + 4));
+  t.src[0] = c0.x; t.src[1] = c0.y; t.src[2] = c0.z; t.wflag = c0.w;
+  t.vol = d0.x; t.dvx[0] = d0.y; t.dvx[1] = d1.x; t.dvx[2] = d1.y;
+  t.dvy[0] = d2.x; t.dvy[1] = d2.y; t.dvy[2] = d3.x;
+}
+__device__ __forceinline__ void load_tet(const TetRecF* __restrict__ R, int e, TetElem<float>& t) {
+  const int4* p = reinterpret_cast<const int4*>(R + e);
+  const int4 c0 = __ldg(p);
+  const float4 x = __ldg(reinterpret_cast<const float4*>(p + 1));
+  const float4 y = __ldg(reinterpret_cast<const float4*>(p + 2));
+  const float4 z = __ldg(reinterpret_cast<const float4*>(p + 3));
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p + 4));
+  t.src[0] = c0.x; t.src[1] = c0.y; t.src[2] = c0.z; t.src[3] = c0.w;
+  t.g[0][0] = x.x; t.g[1][0] = x.y; t.g[2][0] = x.z; t.g[3][0] = x.w;
+  t.g[0][1] = y.x; t.g[1][1] = y.y; t.g[2][1] = y.z; t.g[3][1] = y.w;
+  t.g[0][2] = z.x; t.g[1][2] = z.y; t.g[2][2] = z.z; t.g[3][2] = z.w;
+  t.vol = v.x;
+  t.wflag = __float_as_int(v.y);
+}
+__device__ __forceinline__ void load_tet(const TetRecD* __restrict__ R, int e, TetElem<double>& t) {
+  const int4* p = reinterpret_cast<const int4*>(R + e);
+  const int4 c0 = __ldg(p);
+  t.src[0] = c0.x; t.src[1] = c0.y; t.src[2] = c0.z; t.src[3] = c0.w;
+  const double2* q = reinterpret_cast<const double2*>(p + 1);
+  double2 a;
+  a = __ldg(q + 0); t.g[0][0] = a.x; t.g[1][0] = a.y;
+  a = __ldg(q + 1); t.g[2][0] = a.x; t.g[3][0] = a.y;
+  a = __ldg(q + 2); t.g[0][1] = a.x; t.g[1][1] = a.y;
+  a = __ldg(q + 3); t.g[2][1] = a.x; t.g[3][1] = a.y;
+  a = __ldg(q + 4); t.g[0][2] = a.x; t.g[1][2] = a.y;
+  a = __ldg(q + 5); t.g[2][2] = a.x; t.g[3][2] = a.y;
+  a = __ldg(q + 6); t.vol = a.x;
+  t.wflag = __double2loint(a.y);
+}
+
+__device__ __forceinline__ double gather(const double* __restrict__ u, const double* __restrict__ dir,
+                                         int code, int c) {
+  return code >= 0 ? __ldg(u + code + c) : __ldg(dir + (-1 - code) + c);
+}
+
+// ---------------------------------------------------------------------------
+// physics: p-Laplace, Ginzburg-Landau (P1 triangles, scalar)
+// ---------------------------------------------------------------------------
+enum { FAM_PLAP = 1, FAM_GL = 2 };
+enum { W_E = 1, W_G = 2, W_H = 4 };
+
+// Row a of the element gradient and Hessian.  Hand-written adjoints of
+//   p-Laplace:  e = vol/p * s^(p/2),  s = Fx^2 + Fy^2
+//     g_a = vol s^(p/2-1) G_a,  G_a = Fx dvx_a + Fy dvy_a
+//     H_ab = vol [ s^(p/2-1) (dvx_a dvx_b + dvy_a dvy_b) + (p-2) s^(p/2-2) G_a G_b ]
+//     (at s = 0 the limit: 0 for p > 2, where JAX's autodiff gives inf*0)
+//   GL:  e = vol [ eps/2 s + 1/4 sum_q w_q (n_q^2 - 1)^2 ],  n_q = sum_b v_b ip[b][q]
+//     g_a = vol [ eps G_a + sum_q w_q (n_q^2 - 1) n_q ip[a][q] ]
+//     H_ab = vol [ eps (dvx_a dvx_b + dvy_a dvy_b) + sum_q w_q (3 n_q^2 - 1) ip[a][q] ip[b][q] ]
+template <typename Real, int FAM>
+__device__ __forceinline__ void tri_row(const Phys& P, int a, const Real v[3], const TriElem<Real>& t,
+                                        Real& ga, Real h[3]) {
+  const Real fx = v[0] * t.dvx[0] + v[1] * t.dvx[1] + v[2] * t.dvx[2];
+  const Real fy = v[0] * t.dvy[0] + v[1] * t.dvy[1] + v[2] * t.dvy[2];
+  const Real dxa = a == 0 ? t.dvx[0] : (a == 1 ? t.dvx[1] : t.dvx[2]);
+  const Real dya = a == 0 ? t.dvy[0] : (a == 1 ? t.dvy[1] : t.dvy[2]);
+  if (FAM == FAM_PLAP) {
+    const Real s = fx * fx + fy * fy;
+    const Real p = (Real)P.p;
+    Real t1, t2;
+    if (s > Real(0)) {
+      if (P.p == 3.0) {
+        t1 = sqrt(s);
+        t2 = Real(1) / t1;
+      } else {
+        t1 = pow(s, p * Real(0.5) - Real(1));
+        t2 = (p - Real(2)) * pow(s, p * Real(0.5) - Real(2));
+      }
+    } else {
+      t1 = P.p == 2.0 ? Real(1) : (P.p > 2.0 ? Real(0) : Real(INFINITY));
+      t2 = Real(0);
+    }
+    const Real Ga = fx * dxa + fy * dya;
+    ga = t.vol * t1 * Ga;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      h[b] = t.vol * (t1 * (dxa * t.dvx[b] + dya * t.dvy[b]) + t2 * Ga * (fx * t.dvx[b] + fy * t.dvy[b]));
+  } else {
+    const Real eps = (Real)P.eps;
+    Real ipa[3], n[3], c1[3], c2[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      n[q] = v[0] * (Real)P.ip[q] + v[1] * (Real)P.ip[3 + q] + v[2] * (Real)P.ip[6 + q];
+      ipa[q] = (Real)(a == 0 ? P.ip[q] : (a == 1 ? P.ip[3 + q] : P.ip[6 + q]));
+      c1[q] = (Real)P.w[q] * (n[q] * n[q] - Real(1)) * n[q];
+      c2[q] = (Real)P.w[q] * (Real(3) * n[q] * n[q] - Real(1)) * ipa[q];
+    }
+    ga = t.vol * (eps * (fx * dxa + fy * dya) + c1[0] * ipa[0] + c1[1] * ipa[1] + c1[2] * ipa[2]);
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      h[b] = t.vol * (eps * (dxa * t.dvx[b] + dya * t.dvy[b]) + c2[0] * (Real)P.ip[3 * b] +
+                      c2[1] * (Real)P.ip[3 * b + 1] + c2[2] * (Real)P.ip[3 * b + 2]);
+  }
+}
+
+// FP64 element energy (always double, from the stored geometry).
+template <typename Real, int FAM>
+__device__ __forceinline__ double tri_energy(const Phys& P, const double v[3], const TriElem<Real>& t) {
+  const double fx = v[0] * (double)t.dvx[0] + v[1] * (double)t.dvx[1] + v[2] * (double)t.dvx[2];
+  const double fy = v[0] * (double)t.dvy[0] + v[1] * (double)t.dvy[1] + v[2] * (double)t.dvy[2];
+  const double s = fx * fx + fy * fy;
+  if (FAM == FAM_PLAP) {
+    const double ps = P.p == 3.0 ? s * sqrt(s) : pow(s, 0.5 * P.p);
+    return (1.0 / P.p) * ps * (double)t.vol;
+  } else {
+    double pot = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double n = v[0] * P.ip[q] + v[1] * P.ip[3 + q] + v[2] * P.ip[6 + q];
+      const double m = n * n - 1.0;
+      pot += 0.25 * m * m * P.w[q];
+    }
+    return (0.5 * P.eps * s + pot) * (double)t.vol;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// physics: compressible Neo-Hookean (P1 tetrahedra, 3 DOFs per node)
+//   W(F) = C1 (|F|^2 - 3 - 2 ln J) + D1 (J - 1)^2,  F = sum_a y_a (x) g_a,  J = det F
+//   dW/dF = 2 C1 F + c3 cof(F),            c3 = -2 C1 / J + 2 D1 (J - s)
+//   H_(a,c)(b,d) = vol [ 2 C1 (g_a.g_b) delta_cd + c2 (cof g_a)_c (cof g_b)_d
+//                        + c3 eps_cdm (F (g_a x g_b))_m ],   c2 = 2 C1 / J^2 + 2 D1
+//   (s = 1, or sign(J) when |J| enters the energy; the last term is the
+//   contraction of d^2 J / dF^2 = eps_cdm eps_jlp F_mp with g_a, g_b).
+// ---------------------------------------------------------------------------
+template <typename Real>
+struct HeState {
+  Real F[3][3], cof[3][3], J, c2, c3;
+};
+
+template <typename Real>
+__device__ __forceinline__ void he_state(const Phys& P, const Real y[4][3], const TetElem<Real>& t,
+                                         HeState<Real>& S) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      S.F[i][j] = y[0][i] * t.g[0][j] + y[1][i] * t.g[1][j] + y[2][i] * t.g[2][j] + y[3][i] * t.g[3][j];
+  const Real(&F)[3][3] = S.F;
+  S.cof[0][0] = F[1][1] * F[2][2] - F[1][2] * F[2][1];
+  S.cof[0][1] = F[1][2] * F[2][0] - F[1][0] * F[2][2];
+  S.cof[0][2] = F[1][0] * F[2][1] - F[1][1] * F[2][0];
+  S.cof[1][0] = F[0][2] * F[2][1] - F[0][1] * F[2][2];
+  S.cof[1][1] = F[0][0] * F[2][2] - F[0][2] * F[2][0];
+  S.cof[1][2] = F[0][1] * F[2][0] - F[0][0] * F[2][1];
+  S.cof[2][0] = F[0][1] * F[1][2] - F[0][2] * F[1][1];
+  S.cof[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
+  S.cof[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
+  S.J = F[0][0] * S.cof[0][0] + F[0][1] * S.cof[0][1] + F[0][2] * S.cof[0][2];
+  const Real C1 = (Real)P.C1, D1 = (Real)P.D1;
+  const Real sg = P.absdet ? (S.J > Real(0) ? Real(1) : (S.J < Real(0) ? Real(-1) : Real(0))) : Real(1);
+  const Real iJ = Real(1) / S.J;
+  S.c2 = Real(2) * C1 * iJ * iJ + Real(2) * D1;
+  S.c3 = -Real(2) * C1 * iJ + Real(2) * D1 * (S.J - sg);
+}
+
+// Gradient entry (a, c) and Hessian row (a, c) over all 12 element DOFs.
+template <typename Real>
+__device__ __forceinline__ void he_row(const Phys& P, int a, int c, const HeState<Real>& S,
+                                       const TetElem<Real>& t, Real& gac, Real h[4][3], bool want_h) {
+  Real ga[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    ga[j] = a == 0 ? t.g[0][j] : (a == 1 ? t.g[1][j] : (a == 2 ? t.g[2][j] : t.g[3][j]));
+  const Real C1 = (Real)P.C1;
+  const Real Fc0 = c == 0 ? S.F[0][0] : (c == 1 ? S.F[1][0] : S.F[2][0]);
+  const Real Fc1 = c == 0 ? S.F[0][1] : (c == 1 ? S.F[1][1] : S.F[2][1]);
+  const Real Fc2 = c == 0 ? S.F[0][2] : (c == 1 ? S.F[1][2] : S.F[2][2]);
+  const Real Cc0 = c == 0 ? S.cof[0][0] : (c == 1 ? S.cof[1][0] : S.cof[2][0]);
+  const Real Cc1 = c == 0 ? S.cof[0][1] : (c == 1 ? S.cof[1][1] : S.cof[2][1]);
+  const Real Cc2 = c == 0 ? S.cof[0][2] : (c == 1 ? S.cof[1][2] : S.cof[2][2]);
+  const Real Pg = Real(2) * C1 * (Fc0 * ga[0] + Fc1 * ga[1] + Fc2 * ga[2]);
+  const Real cga_c = Cc0 * ga[0] + Cc1 * ga[1] + Cc2 * ga[2];  // (cof g_a)_c
+  gac = t.vol * (Pg + S.c3 * cga_c);
+  if (!want_h) return;
+  const Real k1 = t.vol * Real(2) * C1, k2 = t.vol * S.c2 * cga_c, k3 = t.vol * S.c3;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const Real* gb = t.g[b];
+    const Real dot = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+    // (cof g_b)_d
+    Real cgb[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) cgb[d] = S.cof[d][0] * gb[0] + S.cof[d][1] * gb[1] + S.cof[d][2] * gb[2];
+    // w = F (g_a x g_b)
+    const Real x0 = ga[1] * gb[2] - ga[2] * gb[1];
+    const Real x1 = ga[2] * gb[0] - ga[0] * gb[2];
+    const Real x2 = ga[0] * gb[1] - ga[1] * gb[0];
+    Real w[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) w[m] = S.F[m][0] * x0 + S.F[m][1] * x1 + S.F[m][2] * x2;
+    // skew row c of eps_cdm w_m: c=0 -> (0, w2, -w1); c=1 -> (-w2, 0, w0); c=2 -> (w1, -w0, 0)
+    const Real s0 = c == 0 ? Real(0) : (c == 1 ? -w[2] : w[1]);
+    const Real s1 = c == 0 ? w[2] : (c == 1 ? Real(0) : -w[0]);
+    const Real s2 = c == 0 ? -w[1] : (c == 1 ? w[0] : Real(0));
+    h[b][0] = k2 * cgb[0] + k3 * s0 + (c == 0 ? k1 * dot : Real(0));
+    h[b][1] = k2 * cgb[1] + k3 * s1 + (c == 1 ? k1 * dot : Real(0));
+    h[b][2] = k2 * cgb[2] + k3 * s2 + (c == 2 ? k1 * dot : Real(0));
+  }
+}
+
+// FP64 element energy of one tetrahedron.
+template <typename Real>
+__device__ __forceinline__ double he_energy(const Phys& P, const double y[4][3], const TetElem<Real>& t) {
+  double F[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      F[i][j] = y[0][i] * (double)t.g[0][j] + y[1][i] * (double)t.g[1][j] + y[2][i] * (double)t.g[2][j] +
+                y[3][i] * (double)t.g[3][j];
+  double I1 = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) I1 += F[i][j] * F[i][j];
+  double J = F[0][0] * (F[1][1] * F[2][2] - F[1][2] * F[2][1]) - F[0][1] * (F[1][0] * F[2][2] - F[1][2] * F[2][0]) +
+             F[0][2] * (F[1][0] * F[2][1] - F[1][1] * F[2][0]);
+  if (P.absdet) J = fabs(J);
+  return (P.C1 * (I1 - 3.0 - 2.0 * log(J)) + P.D1 * (J - 1.0) * (J - 1.0)) * (double)t.vol;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 reduction: per-CTA partial + last-CTA finalisation (no spin-waits)
+// ---------------------------------------------------------------------------
+struct EnergyOut {
+  double* partials;
+  unsigned* counter;
+  double* out;            // destination of the total
+  const double* addend;   // optional constant added to the total (device)
+};
+
+__device__ __forceinline__ double block_sum(double v, double* ws) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) ws[wid] = v;
+  __syncthreads();
+  v = 0.0;
+  if (wid == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    v = lane < nw ? ws[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;  // valid in thread 0
+}
+
+__device__ void energy_finalize(double v, const EnergyOut& eo) {
+  __shared__ double ws[32];
+  __shared__ int is_last;
+  v = block_sum(v, ws);
+  if (threadIdx.x == 0) {
+    eo.partials[blockIdx.x] = v;
+    __threadfence();
+    const unsigned ticket = atomicAdd(eo.counter, 1u);
+    is_last = ticket == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  double s = 0.0;
+  for (int j = threadIdx.x; j < (int)gridDim.x; j += blockDim.x) s += __ldcg(eo.partials + j);
+  s = block_sum(s, ws);
+  if (threadIdx.x == 0) {
+    eo.out[0] = s + (eo.addend ? *eo.addend : 0.0);
+    *eo.counter = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// row-gather kernels
+// ---------------------------------------------------------------------------
+struct RowArgs {
+  int n_rows;
+  const int* __restrict__ row_ptr;
+  const int* __restrict__ row_node;
+  const unsigned char* __restrict__ row_comp;
+  const int* __restrict__ row_gpos;
+  const int* __restrict__ inc_ptr;
+  const int* __restrict__ inc_elem;
+  const unsigned* __restrict__ inc_info;
+  const double* __restrict__ u;
+  const double* __restrict__ dir;
+  const double* __restrict__ rhs;  // may be null
+  long long lo;
+};
+
+constexpr int kTriRows = 256;
+constexpr int kTetRows = 128;
+
+template <typename Real, int FAM, int WANT, typename HOut>
+__global__ void __launch_bounds__(kTriRows) k_rows_tri(RowArgs A, const typename TriRecT<Real>::T* __restrict__ R,
+                                                       Phys P, double* __restrict__ grad,
+                                                       HOut* __restrict__ hess, EnergyOut eo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* sacc = reinterpret_cast<Real*>(smem_raw);
+  const int r0 = blockIdx.x * blockDim.x;
+  const int r = r0 + threadIdx.x;
+  const int rend = min(r0 + (int)blockDim.x, A.n_rows);
+  const int cs = A.row_ptr[r0];
+  const int clen = A.row_ptr[rend] - cs;
+  if (WANT & W_H) {
+    for (int j = threadIdx.x; j < clen; j += blockDim.x) sacc[j] = Real(0);
+    __syncthreads();
+  }
+  double eacc = 0.0;
+  if (r < A.n_rows) {
+    const int node = A.row_node[r];
+    const int base = A.row_ptr[r] - cs;
+    const int ib = A.inc_ptr[node], ie = A.inc_ptr[node + 1];
+    Real g = Real(0);
+    for (int i = ib; i < ie; ++i) {
+      const int el = __ldg(A.inc_elem + i);
+      const unsigned info = __ldg(A.inc_info + i);
+      TriElem<Real> t;
+      load_tri(R, el, t);
+      double vd[3];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) vd[b] = gather(A.u, A.dir, t.src[b], 0);
+      const Real v[3] = {(Real)vd[0], (Real)vd[1], (Real)vd[2]};
+      const int a = info & 7u;
+      Real ga, h[3];
+      tri_row<Real, FAM>(P, a, v, t, ga, h);
+      if (WANT & W_G) g += ga;
+      if (WANT & W_H) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          const unsigned off = (info >> (kOffShift + kOffBits * b)) & 127u;
+          if (off != kNoCol) sacc[base + off] += h[b];
+        }
+      }
+      if ((WANT & W_E) && (info & kEnergyFlag)) eacc += tri_energy<Real, FAM>(P, vd, t);
+    }
+    const int gp = A.row_gpos[r];
+    if (WANT & W_G) grad[gp] = (double)g - (A.rhs ? A.rhs[gp] : 0.0);
+    if ((WANT & W_E) && A.rhs) eacc -= A.rhs[gp] * A.u[A.lo + gp];
+  }
+  if (WANT & W_H) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < clen; j += blockDim.x) hess[cs + j] = (HOut)sacc[j];
+  }
+  if (WANT & W_E) energy_finalize(eacc, eo);
+}
+
+template <typename Real, int WANT, typename HOut>
+__global__ void __launch_bounds__(kTetRows) k_rows_tet(RowArgs A, const typename TetRecT<Real>::T* __restrict__ R,
+                                                       Phys P, double* __restrict__ grad,
+                                                       HOut* __restrict__ hess, EnergyOut eo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* sacc = reinterpret_cast<Real*>(smem_raw);
+  const int r0 = blockIdx.x * blockDim.x;
+  const int r = r0 + threadIdx.x;
+  const int rend = min(r0 + (int)blockDim.x, A.n_rows);
+  const int cs = A.row_ptr[r0];
+  const int clen = A.row_ptr[rend] - cs;
+  if (WANT & W_H) {
+    for (int j = threadIdx.x; j < clen; j += blockDim.x) sacc[j] = Real(0);
+    __syncthreads();
+  }
+  double eacc = 0.0;
+  if (r < A.n_rows) {
+    const int node = A.row_node[r];
+    const int c = A.row_comp[r];
+    const int base = A.row_ptr[r] - cs;
+    const int ib = A.inc_ptr[node], ie = A.inc_ptr[node + 1];
+    Real g = Real(0);
+    for (int i = ib; i < ie; ++i) {
+      const int el = __ldg(A.inc_elem + i);
+      const unsigned info = __ldg(A.inc_info + i);
+      TetElem<Real> t;
+      load_tet(R, el, t);
+      double yd[4][3];
+      Real y[4][3];
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          yd[b][d] = gather(A.u, A.dir, t.src[b], d);
+          y[b][d] = (Real)yd[b][d];
+        }
+      HeState<Real> S;
+      he_state(P, y, t, S);
+      const int a = info & 7u;
+      Real gac, h[4][3];
+      he_row(P, a, c, S, t, gac, h, (WANT & W_H) != 0);
+      if (WANT & W_G) g += gac;
+      if (WANT & W_H) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const unsigned off = (info >> (kOffShift + kOffBits * b)) & 127u;
+          if (off != kNoCol) {
+            sacc[base + off] += h[b][0];
+            sacc[base + off + 1] += h[b][1];
+            sacc[base + off + 2] += h[b][2];
+          }
+        }
+      }
+      if ((WANT & W_E) && c == 0 && (info & kEnergyFlag)) eacc += he_energy<Real>(P, yd, t);
+    }
+    const int gp = A.row_gpos[r];
+    if (WANT & W_G) grad[gp] = (double)g - (A.rhs ? A.rhs[gp] : 0.0);
+    if ((WANT & W_E) && A.rhs) eacc -= A.rhs[gp] * A.u[A.lo + gp];
+  }
+  if (WANT & W_H) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < clen; j += blockDim.x) hess[cs + j] = (HOut)sacc[j];
+  }
+  if (WANT & W_E) energy_finalize(eacc, eo);
+}
+
+// ---------------------------------------------------------------------------
+// energy-only kernels (element-centric, grid-stride)
+// ---------------------------------------------------------------------------
+constexpr int kElemThreads = 256;
+
+template <typename Real, int FAM>
+__global__ void __launch_bounds__(kElemThreads) k_energy_tri(const typename TriRecT<Real>::T* __restrict__ R, int n_el,
+                                                             const double* __restrict__ u, const double* __restrict__ dir,
+                                                             Phys P, const double* __restrict__ rhs, int n_owned,
+                                                             long long lo, EnergyOut eo) {
+  double acc = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += stride) {
+    TriElem<Real> t;
+    load_tri(R, e, t);
+    if (!t.wflag) continue;
+    double vd[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) vd[b] = gather(u, dir, t.src[b], 0);
+    acc += tri_energy<Real, FAM>(P, vd, t);
+  }
+  if (rhs)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_owned; i += stride) acc -= rhs[i] * u[lo + i];
+  energy_finalize(acc, eo);
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kElemThreads) k_energy_tet(const typename TetRecT<Real>::T* __restrict__ R, int n_el,
+                                                             const double* __restrict__ u, const double* __restrict__ dir,
+                                                             Phys P, const double* __restrict__ rhs, int n_owned,
+                                                             long long lo, EnergyOut eo) {
+  double acc = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += stride) {
+    TetElem<Real> t;
+    load_tet(R, e, t);
+    if (!t.wflag) continue;
+    double yd[4][3];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) yd[b][d] = gather(u, dir, t.src[b], d);
+    acc += he_energy<Real>(P, yd, t);
+  }
+  if (rhs)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_owned; i += stride) acc -= rhs[i] * u[lo + i];
+  energy_finalize(acc, eo);
+}
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct fne_handle {
+  int family = 0, precision = 0, hess_fp32 = 0, npe = 0, bs = 0;
+  int64_t n_total = 0, n_free = 0, lo = 0, hi = 0, nnz = 0;
+  int n_rows = 0, n_local = 0, n_dir_only = 0, rows_per_cta = 0, grid_rows = 0, grid_elem = 0;
+  int64_t n_inc = 0;
+  int max_row_len = 0;
+  size_t smem_bytes = 0;
+  int device = 0, num_sms = 148;
+  Phys phys{};
+  // device buffers
+  void* rec = nullptr;
+  void* rec_dir_only = nullptr;
+  int *row_ptr = nullptr, *row_node = nullptr, *row_gpos = nullptr, *inc_ptr = nullptr, *inc_elem = nullptr;
+  unsigned char* row_comp = nullptr;
+  unsigned* inc_info = nullptr;
+  double *dir = nullptr, *rhs = nullptr, *partials = nullptr, *dir_const = nullptr;
+  unsigned* counter = nullptr;
+  int n_partials = 0;
+  int64_t device_bytes = 0;
+  // host staging for fne_eval_host (allocated on first use)
+  double *h_u = nullptr, *h_grad = nullptr, *h_energy = nullptr;
+  void* h_hess = nullptr;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return set_error(FNE_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+int dalloc(fne_handle* h, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return FNE_OK;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) return set_error(FNE_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  h->device_bytes += (int64_t)(count * sizeof(T));
+  return FNE_OK;
+}
+
+template <typename T>
+int upload(fne_handle* h, T** p, const T* src, size_t count) {
+  int rc = dalloc(h, p, count);
+  if (rc) return rc;
+  if (count == 0) return FNE_OK;
+  cudaError_t e = cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy H2D");
+  return FNE_OK;
+}
+
+void free_handle(fne_handle* h) {
+  if (!h) return;
+  void* ptrs[] = {h->rec, h->rec_dir_only, h->row_ptr, h->row_node, h->row_gpos, h->inc_ptr, h->inc_elem,
+                  h->row_comp, h->inc_info, h->dir, h->rhs, h->partials, h->dir_const, h->counter,
+                  h->h_u, h->h_grad, h->h_energy, h->h_hess};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete h;
+}
+
+// pack element records on the host (reference float64 arrays -> Real records)
+template <typename Real>
+void pack_tri(const fne_desc* d, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
+              const std::vector<uint8_t>* weight, std::vector<typename TriRecT<Real>::T>& out) {
+  out.assign(elems.size(), {});
+  for (size_t i = 0; i < elems.size(); ++i) {
+    const int64_t e = elems[i];
+    auto& r = out[i];
+    for (int b = 0; b < 3; ++b) {
+      r.src[b] = code[i * 3 + b];
+      r.dvx[b] = (Real)d->e0[e * 3 + b];
+      r.dvy[b] = (Real)d->e1[e * 3 + b];
+    }
+    r.vol = (Real)d->e2[e];
+    r.wflag = weight ? (*weight)[i] : 1;
+  }
+}
+
+template <typename Real>
+void pack_tet(const fne_desc* d, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
+              const std::vector<uint8_t>* weight, std::vector<typename TetRecT<Real>::T>& out);
+template <>
+void pack_tet<float>(const fne_desc* d, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
+                     const std::vector<uint8_t>* weight, std::vector<TetRecF>& out) {
+  out.assign(elems.size(), {});
+  for (size_t i = 0; i < elems.size(); ++i) {
+    const int64_t e = elems[i];
+    auto& r = out[i];
+    for (int b = 0; b < 4; ++b) {
+      r.src[b] = code[i * 4 + b];
+      r.gx[b] = (float)d->e0[e * 4 + b];
+      r.gy[b] = (float)d->e1[e * 4 + b];
+      r.gz[b] = (float)d->e2[e * 4 + b];
+    }
+    r.vol = (float)d->e3[e];
+    r.wflag = weight ? (*weight)[i] : 1;
+  }
+}
+template <>
+void pack_tet<double>(const fne_desc* d, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
+                      const std::vector<uint8_t>* weight, std::vector<TetRecD>& out) {
+  out.assign(elems.size(), {});
+  for (size_t i = 0; i < elems.size(); ++i) {
+    const int64_t e = elems[i];
+    auto& r = out[i];
+    for (int b = 0; b < 4; ++b) {
+      r.src[b] = code[i * 4 + b];
+      r.gx[b] = d->e0[e * 4 + b];
+      r.gy[b] = d->e1[e * 4 + b];
+      r.gz[b] = d->e2[e * 4 + b];
+    }
+    r.vol = d->e3[e];
+    r.wflag = weight ? (*weight)[i] : 1;
+  }
+}
+
+bool is_tri(int fam) { return fam == FNE_PLAPLACE || fam == FNE_GINZBURG_LANDAU; }
+
+// ---- kernel dispatch -------------------------------------------------------
+template <typename Real, int FAM, typename HOut>
+cudaError_t launch_rows_tri_t(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
+                              cudaStream_t st, bool set_attr) {
+  using RecT = typename TriRecT<Real>::T;
+  const RecT* R = static_cast<const RecT*>(h->rec);
+  HOut* H = static_cast<HOut*>(hess);
+  const dim3 grid(h->grid_rows), block(kTriRows);
+  const size_t sm = (want & W_H) ? h->smem_bytes : 0;
+#define FNE_TRI_CASE(W)                                                                              \
+  case W:                                                                                            \
+    if (set_attr)                                                                                    \
+      return cudaFuncSetAttribute(k_rows_tri<Real, FAM, W, HOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)h->smem_bytes);                                               \
+    k_rows_tri<Real, FAM, W, HOut><<<grid, block, sm, st>>>(A, R, h->phys, grad, H, eo);              \
+    return cudaGetLastError();
+  switch (want) {
+    FNE_TRI_CASE(2)
+    FNE_TRI_CASE(3)
+    FNE_TRI_CASE(4)
+    FNE_TRI_CASE(5)
+    FNE_TRI_CASE(6)
+    FNE_TRI_CASE(7)
+  }
+#undef FNE_TRI_CASE
+  return cudaErrorInvalidValue;
+}
+
+template <typename Real, typename HOut>
+cudaError_t launch_rows_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
+                              cudaStream_t st, bool set_attr) {
+  using RecT = typename TetRecT<Real>::T;
+  const RecT* R = static_cast<const RecT*>(h->rec);
+  HOut* H = static_cast<HOut*>(hess);
+  const dim3 grid(h->grid_rows), block(kTetRows);
+  const size_t sm = (want & W_H) ? h->smem_bytes : 0;
+#define FNE_TET_CASE(W)                                                                              \
+  case W:                                                                                            \
+    if (set_attr)                                                                                    \
+      return cudaFuncSetAttribute(k_rows_tet<Real, W, HOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  (int)h->smem_bytes);                                               \
+    k_rows_tet<Real, W, HOut><<<grid, block, sm, st>>>(A, R, h->phys, grad, H, eo);                   \
+    return cudaGetLastError();
+  switch (want) {
+    FNE_TET_CASE(2)
+    FNE_TET_CASE(3)
+    FNE_TET_CASE(4)
+    FNE_TET_CASE(5)
+    FNE_TET_CASE(6)
+    FNE_TET_CASE(7)
+  }
+#undef FNE_TET_CASE
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_rows(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
+                        cudaStream_t st, bool set_attr) {
+  const bool f32 = h->precision == FNE_FP32;
+  const bool h32 = f32 && h->hess_fp32;
+  if (h->family == FNE_PLAPLACE) {
+    if (!f32) return launch_rows_tri_t<double, FAM_PLAP, double>(h, want, A, grad, hess, eo, st, set_attr);
+    if (h32) return launch_rows_tri_t<float, FAM_PLAP, float>(h, want, A, grad, hess, eo, st, set_attr);
+    return launch_rows_tri_t<float, FAM_PLAP, double>(h, want, A, grad, hess, eo, st, set_attr);
+  }
+  if (h->family == FNE_GINZBURG_LANDAU) {
+    if (!f32) return launch_rows_tri_t<double, FAM_GL, double>(h, want, A, grad, hess, eo, st, set_attr);
+    if (h32) return launch_rows_tri_t<float, FAM_GL, float>(h, want, A, grad, hess, eo, st, set_attr);
+    return launch_rows_tri_t<float, FAM_GL, double>(h, want, A, grad, hess, eo, st, set_attr);
+  }
+  if (h->family == FNE_NEOHOOKEAN) {
+    if (!f32) return launch_rows_tet_t<double, double>(h, want, A, grad, hess, eo, st, set_attr);
+    if (h32) return launch_rows_tet_t<float, float>(h, want, A, grad, hess, eo, st, set_attr);
+    return launch_rows_tet_t<float, double>(h, want, A, grad, hess, eo, st, set_attr);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_energy(fne_handle* h, const void* rec, int n_el, const double* u, const double* rhs, int n_owned,
+                          EnergyOut eo, cudaStream_t st) {
+  const bool f32 = h->precision == FNE_FP32;
+  int grid = std::max(1, std::min(h->num_sms * 8, (std::max(n_el, n_owned) + kElemThreads - 1) / kElemThreads));
+  grid = std::min(grid, h->n_partials);
+  const long long lo = h->lo;
+  if (h->family == FNE_PLAPLACE) {
+    if (f32)
+      k_energy_tri<float, FAM_PLAP><<<grid, kElemThreads, 0, st>>>((const TriRecF*)rec, n_el, u, h->dir, h->phys, rhs,
+                                                                   n_owned, lo, eo);
+    else
+      k_energy_tri<double, FAM_PLAP><<<grid, kElemThreads, 0, st>>>((const TriRecD*)rec, n_el, u, h->dir, h->phys,
+                                                                    rhs, n_owned, lo, eo);
+  } else if (h->family == FNE_GINZBURG_LANDAU) {
+    if (f32)
+      k_energy_tri<float, FAM_GL><<<grid, kElemThreads, 0, st>>>((const TriRecF*)rec, n_el, u, h->dir, h->phys, rhs,
+                                                                 n_owned, lo, eo);
+    else
+      k_energy_tri<double, FAM_GL><<<grid, kElemThreads, 0, st>>>((const TriRecD*)rec, n_el, u, h->dir, h->phys, rhs,
+                                                                  n_owned, lo, eo);
+  } else if (h->family == FNE_NEOHOOKEAN) {
+    if (f32)
+      k_energy_tet<float><<<grid, kElemThreads, 0, st>>>((const TetRecF*)rec, n_el, u, h->dir, h->phys, rhs, n_owned,
+                                                         lo, eo);
+    else
+      k_energy_tet<double><<<grid, kElemThreads, 0, st>>>((const TetRecD*)rec, n_el, u, h->dir, h->phys, rhs, n_owned,
+                                                          lo, eo);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// energy of the elements without any free DOF (constant w.r.t. u)
+int refresh_dir_const(fne_handle* h) {
+  if (!h->dir_const) return FNE_OK;
+  cudaError_t e;
+  if (h->n_dir_only == 0) {
+    e = cudaMemset(h->dir_const, 0, sizeof(double));
+  } else {
+    EnergyOut eo{h->partials, h->counter, h->dir_const, nullptr};
+    e = launch_energy(h, h->rec_dir_only, h->n_dir_only, h->dir /*unused for Dirichlet nodes*/, nullptr, 0, eo, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "Dirichlet-only energy");
+  return FNE_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
+  if (!d || !out) return set_error(FNE_EINVAL, "fne_create: null argument");
+  *out = nullptr;
+  if (d->precision != FNE_FP64 && d->precision != FNE_FP32)
+    return set_error(FNE_EINVAL, "fne_create: precision must be FNE_FP64 or FNE_FP32");
+  int npe_expect = 0, bs_expect = 0;
+  if (is_tri(d->family)) {
+    npe_expect = 3;
+    bs_expect = 1;
+  } else if (d->family == FNE_NEOHOOKEAN) {
+    npe_expect = 4;
+    bs_expect = 3;
+  } else if (d->family == FNE_MOHR_COULOMB) {
+    return set_error(FNE_EINVAL, "fne_create: Mohr-Coulomb handles are created with fne_create_mc");
+  } else {
+    return set_error(FNE_EINVAL, "fne_create: unknown family");
+  }
+  if (d->npe != npe_expect || d->block_size != bs_expect)
+    return set_error(FNE_EINVAL, "fne_create: npe/block_size do not match the family");
+  if (d->n_elem < 0 || d->n_total < 0 || d->nnz < 0 || (d->n_elem > 0 && !d->elems) || !d->total_to_free_reord ||
+      (d->nnz > 0 && (!d->owned_rows || !d->owned_cols)) || (d->n_total > 0 && !d->dirichlet))
+    return set_error(FNE_EINVAL, "fne_create: missing array");
+  if (d->n_elem > 0 && (!d->e0 || !d->e1 || !d->e2 || (d->family == FNE_NEOHOOKEAN && !d->e3)))
+    return set_error(FNE_EINVAL, "fne_create: missing element data");
+  if (d->family == FNE_PLAPLACE && !(d->s[0] > 1.0))
+    return set_error(FNE_EINVAL, "fne_create: p-Laplace needs p > 1");
+
+  RowPlan plan;
+  int rc = build_row_plan(d, plan);
+  if (rc) return rc;
+
+  auto* h = new (std::nothrow) fne_handle();
+  if (!h) return set_error(FNE_ENOMEM, "fne_create: out of host memory");
+  h->family = d->family;
+  h->precision = d->precision;
+  h->hess_fp32 = d->precision == FNE_FP32 ? (d->hess_fp32 ? 1 : 0) : 0;
+  h->npe = d->npe;
+  h->bs = d->block_size;
+  h->n_total = d->n_total;
+  h->n_free = d->n_free;
+  h->lo = d->lo;
+  h->hi = d->hi;
+  h->nnz = d->nnz;
+  h->n_rows = plan.n_rows;
+  h->n_local = (int)plan.local_elems.size();
+  h->n_dir_only = (int)plan.dir_only.size();
+  h->n_inc = (int64_t)plan.inc_elem.size();
+  h->max_row_len = plan.max_row_len;
+  h->phys.p = d->s[0];
+  h->phys.eps = d->s[0];
+  for (int i = 0; i < 9; ++i) h->phys.ip[i] = d->s[1 + i];
+  for (int i = 0; i < 3; ++i) h->phys.w[i] = d->s[10 + i];
+  h->phys.C1 = d->s[0];
+  h->phys.D1 = d->s[1];
+  h->phys.absdet = d->family == FNE_NEOHOOKEAN && d->s[2] != 0.0;
+  cudaGetDevice(&h->device);
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+
+  const bool f32 = d->precision == FNE_FP32;
+  const size_t real_size = f32 ? sizeof(float) : sizeof(double);
+  h->rows_per_cta = is_tri(d->family) ? kTriRows : kTetRows;
+  h->grid_rows = (h->n_rows + h->rows_per_cta - 1) / h->rows_per_cta;
+  int64_t max_cta = 0;
+  for (int c = 0; c < h->grid_rows; ++c) {
+    const int a = c * h->rows_per_cta, b = std::min(h->n_rows, a + h->rows_per_cta);
+    max_cta = std::max<int64_t>(max_cta, plan.row_ptr[b] - plan.row_ptr[a]);
+  }
+  h->smem_bytes = (size_t)max_cta * real_size;
+  if (h->smem_bytes > 227 * 1024) {
+    free_handle(h);
+    return set_error(FNE_EBOUNDS, "fne_create: a CTA's rows exceed shared memory");
+  }
+  h->grid_elem = std::max(1, std::min(h->num_sms * 8, (h->n_local + kElemThreads - 1) / kElemThreads));
+  h->n_partials = std::max({h->grid_rows, h->num_sms * 8, 1});
+
+#define FNE_TRY(x)      \
+  do {                  \
+    rc = (x);           \
+    if (rc) {           \
+      free_handle(h);   \
+      return rc;        \
+    }                   \
+  } while (0)
+
+  // element records
+  if (is_tri(d->family)) {
+    if (f32) {
+      std::vector<TriRecF> recs, dro;
+      pack_tri<float>(d, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
+      FNE_TRY(upload(h, (TriRecF**)&h->rec, recs.data(), recs.size()));
+      if (d->dirichlet_only_energy) {
+        pack_tri<float>(d, plan.dir_only, plan.dir_only_code, nullptr, dro);
+        FNE_TRY(upload(h, (TriRecF**)&h->rec_dir_only, dro.data(), dro.size()));
+      }
+    } else {
+      std::vector<TriRecD> recs, dro;
+      pack_tri<double>(d, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
+      FNE_TRY(upload(h, (TriRecD**)&h->rec, recs.data(), recs.size()));
+      if (d->dirichlet_only_energy) {
+        pack_tri<double>(d, plan.dir_only, plan.dir_only_code, nullptr, dro);
+        FNE_TRY(upload(h, (TriRecD**)&h->rec_dir_only, dro.data(), dro.size()));
+      }
+    }
+  } else {
+    if (f32) {
+      std::vector<TetRecF> recs, dro;
+      pack_tet<float>(d, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
+      FNE_TRY(upload(h, (TetRecF**)&h->rec, recs.data(), recs.size()));
+      if (d->dirichlet_only_energy) {
+        pack_tet<float>(d, plan.dir_only, plan.dir_only_code, nullptr, dro);
+        FNE_TRY(upload(h, (TetRecF**)&h->rec_dir_only, dro.data(), dro.size()));
+      }
+    } else {
+      std::vector<TetRecD> recs, dro;
+      pack_tet<double>(d, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
+      FNE_TRY(upload(h, (TetRecD**)&h->rec, recs.data(), recs.size()));
+      if (d->dirichlet_only_energy) {
+        pack_tet<double>(d, plan.dir_only, plan.dir_only_code, nullptr, dro);
+        FNE_TRY(upload(h, (TetRecD**)&h->rec_dir_only, dro.data(), dro.size()));
+      }
+    }
+  }
+  FNE_TRY(upload(h, &h->row_ptr, plan.row_ptr.data(), plan.row_ptr.size()));
+  FNE_TRY(upload(h, &h->row_node, plan.row_node.data(), plan.row_node.size()));
+  FNE_TRY(upload(h, &h->row_comp, plan.row_comp.data(), plan.row_comp.size()));
+  FNE_TRY(upload(h, &h->row_gpos, plan.row_gpos.data(), plan.row_gpos.size()));
+  FNE_TRY(upload(h, &h->inc_ptr, plan.inc_ptr.data(), plan.inc_ptr.size()));
+  FNE_TRY(upload(h, &h->inc_elem, plan.inc_elem.data(), plan.inc_elem.size()));
+  FNE_TRY(upload(h, &h->inc_info, plan.inc_info.data(), plan.inc_info.size()));
+  FNE_TRY(upload(h, &h->dir, d->dirichlet, (size_t)d->n_total));
+  if (d->rhs_owned) FNE_TRY(upload(h, &h->rhs, d->rhs_owned, (size_t)(d->hi - d->lo)));
+  FNE_TRY(dalloc(h, &h->partials, (size_t)h->n_partials));
+  FNE_TRY(dalloc(h, &h->counter, 1));
+  {
+    cudaError_t e = cudaMemset(h->counter, 0, sizeof(unsigned));
+    if (e != cudaSuccess) {
+      free_handle(h);
+      return cuda_fail(e, "cudaMemset");
+    }
+  }
+  if (d->dirichlet_only_energy) {
+    FNE_TRY(dalloc(h, &h->dir_const, 1));
+    FNE_TRY(refresh_dir_const(h));
+  }
+  // opt in to large dynamic shared memory for every row-kernel variant
+  if (h->smem_bytes > 48 * 1024) {
+    RowArgs dummy{};
+    for (int want = 2; want <= 7; ++want) {
+      cudaError_t e = launch_rows(h, want, dummy, nullptr, nullptr, EnergyOut{}, 0, true);
+      if (e != cudaSuccess) {
+        free_handle(h);
+        return cuda_fail(e, "cudaFuncSetAttribute");
+      }
+    }
+  }
+#undef FNE_TRY
+  *out = h;
+  return FNE_OK;
+}
+
+extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
+  if (!h || !info) return set_error(FNE_EINVAL, "fne_info_get: null argument");
+  info->n_rows = h->n_rows;
+  info->nnz = h->nnz;
+  info->n_elem = h->n_local;
+  info->n_incidences = h->n_inc;
+  info->device_bytes = h->device_bytes;
+  info->max_row_len = h->max_row_len;
+  info->kernel_variant = is_tri(h->family) ? 1 : 2;
+  return FNE_OK;
+}
+
+extern "C" int fne_set_dirichlet(fne_handle* h, const double* dirichlet) {
+  if (!h || (!dirichlet && h->n_total > 0)) return set_error(FNE_EINVAL, "fne_set_dirichlet: null argument");
+  if (h->n_total == 0) return FNE_OK;
+  cudaError_t e = cudaMemcpy(h->dir, dirichlet, h->n_total * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "fne_set_dirichlet");
+  return refresh_dir_const(h);
+}
+
+extern "C" int fne_eval(fne_handle* h, const double* u, int flags, double* energy, double* grad, void* hess,
+                        void* stream) {
+  if (!h) return set_error(FNE_EINVAL, "fne_eval: null handle");
+  if (flags <= 0 || flags > 7) return set_error(FNE_EINVAL, "fne_eval: flags must combine FNE_ENERGY|GRAD|HESS");
+  if ((flags & FNE_ENERGY) && !energy) return set_error(FNE_EINVAL, "fne_eval: energy output missing");
+  if ((flags & FNE_GRAD) && !grad && h->hi > h->lo) return set_error(FNE_EINVAL, "fne_eval: grad output missing");
+  if ((flags & FNE_HESS) && !hess && h->nnz > 0) return set_error(FNE_EINVAL, "fne_eval: hess output missing");
+  if (!u && h->n_free > 0) return set_error(FNE_EINVAL, "fne_eval: u missing");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  EnergyOut eo{h->partials, h->counter, energy, h->dir_const};
+  cudaError_t e = cudaSuccess;
+  const int n_owned = (int)(h->hi - h->lo);
+  if (flags == FNE_ENERGY || h->n_rows == 0) {
+    if (flags & FNE_ENERGY) e = launch_energy(h, h->rec, h->n_local, u, h->rhs, n_owned, eo, st);
+  } else {
+    RowArgs A;
+    A.n_rows = h->n_rows;
+    A.row_ptr = h->row_ptr;
+    A.row_node = h->row_node;
+    A.row_comp = h->row_comp;
+    A.row_gpos = h->row_gpos;
+    A.inc_ptr = h->inc_ptr;
+    A.inc_elem = h->inc_elem;
+    A.inc_info = h->inc_info;
+    A.u = u;
+    A.dir = h->dir;
+    A.rhs = h->rhs;
+    A.lo = h->lo;
+    e = launch_rows(h, flags, A, grad, hess, eo, st, false);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "fne_eval launch");
+  return FNE_OK;
+}
+
+extern "C" int fne_eval_host(fne_handle* h, const double* u_host, int flags, double* energy_host, double* grad_host,
+                             void* hess_host) {
+  if (!h) return set_error(FNE_EINVAL, "fne_eval_host: null handle");
+  const size_t n_owned = (size_t)(h->hi - h->lo);
+  const size_t hsz = (h->precision == FNE_FP32 && h->hess_fp32) ? sizeof(float) : sizeof(double);
+  if (!h->h_energy) {  // staging buffers, allocated once per handle
+    int rc = dalloc(h, &h->h_u, std::max<size_t>(1, (size_t)h->n_free));
+    if (!rc) rc = dalloc(h, &h->h_grad, std::max<size_t>(1, n_owned));
+    if (!rc) rc = dalloc(h, &h->h_energy, 1);
+    if (!rc) rc = dalloc(h, (unsigned char**)&h->h_hess, std::max<size_t>(1, (size_t)h->nnz * hsz));
+    if (rc) return rc;
+  }
+  cudaError_t e = cudaMemcpy(h->h_u, u_host, h->n_free * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "fne_eval_host H2D");
+  int rc = fne_eval(h, h->h_u, flags, h->h_energy, h->h_grad, h->h_hess, nullptr);
+  if (rc) return rc;
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "fne_eval_host kernel");
+  if ((flags & FNE_ENERGY) && energy_host) e = cudaMemcpy(energy_host, h->h_energy, sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && (flags & FNE_GRAD) && grad_host && n_owned)
+    e = cudaMemcpy(grad_host, h->h_grad, n_owned * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && (flags & FNE_HESS) && hess_host && h->nnz)
+    e = cudaMemcpy(hess_host, h->h_hess, h->nnz * hsz, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "fne_eval_host D2H");
+  return FNE_OK;
+}
+
+extern "C" int fne_destroy(fne_handle* h) {
+  free_handle(h);
+  return FNE_OK;
+}
+
+extern "C" const char* fne_last_error(void) { return g_err.c_str(); }
+extern "C" const char* fne_version(void) { return "fne_asm 0.1 (sm_100a)"; }

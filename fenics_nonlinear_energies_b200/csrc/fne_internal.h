@@ -1,0 +1,57 @@
+// Internal declarations shared by the host-side C++ files of libfne_asm.so.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fne_asm.h"
+
+namespace fne {
+
+// Thread-local last-error message (fne_last_error()).
+int set_error(int code, const std::string& msg);
+
+void ownership_range(int64_t n, int rank, int size, int bs, int64_t* lo, int64_t* hi);
+int64_t rank_of_dof(int64_t dof, int64_t n, int size, int bs);
+void element_adjacency(int64_t n_total, int64_t n_free, const int64_t* freedofs, int64_t n_elem,
+                       int ndof_e, const int64_t* elems, std::vector<int64_t>& indptr,
+                       std::vector<int64_t>& indices);
+
+// Sentinel column offset: the element node has no free DOF (Dirichlet column).
+constexpr uint32_t kNoCol = 127u;
+// Incidence word: bits 0-2 local node a, bit 3 energy flag, then 7-bit column
+// offsets (DOF units, relative to the row start) of element nodes 0..npe-1.
+constexpr int kOffShift = 4;
+constexpr int kOffBits = 7;
+constexpr uint32_t kEnergyFlag = 8u;
+
+// Row-gather plan: the reference's element -> COO scatter map
+// (_build_scatter_data) regrouped by output row.  Row k of the owned COO
+// pattern owns positions [row_ptr[k], row_ptr[k+1]); its values are the sum,
+// over the incidences of the row's node, of the element Hessian row.
+struct RowPlan {
+  int32_t n_rows = 0;                // owned rows (every owned DOF once)
+  int32_t n_nodes = 0;               // owned row-nodes
+  std::vector<int32_t> row_ptr;      // [n_rows+1] output positions
+  std::vector<int32_t> row_node;     // [n_rows] index into inc_ptr
+  std::vector<uint8_t> row_comp;     // [n_rows] component of the row's DOF
+  std::vector<int32_t> row_gpos;     // [n_rows] reordered id - lo (gradient slot)
+  std::vector<int32_t> inc_ptr;      // [n_nodes+1]
+  std::vector<int32_t> inc_elem;     // [n_inc] local element index
+  std::vector<uint32_t> inc_info;    // [n_inc] packed (a, flag, offsets)
+  std::vector<int64_t> local_elems;  // local element -> global element id
+  std::vector<int32_t> elem_code;    // [n_local * npe] node gather code
+  std::vector<uint8_t> elem_weight;  // [n_local] 0/1 energy weight
+  std::vector<int64_t> dir_only;     // elements without any free DOF
+  std::vector<int32_t> dir_only_code;
+  int32_t max_row_len = 0;
+};
+
+// Builds the plan for node-uniform problems (every node has all or none of
+// its block_size DOFs free).  Returns FNE_OK or an error (set_error called).
+int build_row_plan(const fne_desc* d, RowPlan& P);
+
+// Gather code of one element node: >= 0 reordered id of component 0 (free
+// node); < 0: -1 - total DOF of component 0 (Dirichlet node).
+}  // namespace fne

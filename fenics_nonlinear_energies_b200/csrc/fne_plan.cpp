@@ -1,0 +1,227 @@
+// Host-side construction of the row-gather plan.
+//
+// The reference scatters the element Hessian stack with
+//   contrib = elem_hess[hess_e, hess_i, hess_j]; np.add.at(owned_vals, hess_positions, contrib)
+// (src/core/petsc/reordered_element_base.py:1754-1756), where hess_positions
+// come from a searchsorted of (row, col) keys into the owned COO pattern
+// (:1464-1534).  Here the same map is regrouped by OUTPUT ROW: every owned
+// row lists the (element, local node) incidences of its node and, per
+// incidence, where each element column lands inside the row.  A kernel thread
+// then produces one row by summing those contributions in a fixed order, so
+// no atomics are needed and the result is bit-reproducible.  As in the
+// reference, a missing (row, col) key is an error (FNE_ELAYOUT).
+#include <algorithm>
+#include <unordered_map>
+
+#include "fne_internal.h"
+
+namespace fne {
+
+int build_row_plan(const fne_desc* d, RowPlan& P) {
+  const int npe = d->npe, bs = d->block_size, nde = npe * bs;
+  const int64_t E = d->n_elem, lo = d->lo, hi = d->hi, nf = d->n_free;
+  if (npe < 1 || bs < 1 || bs > 3 || kOffShift + kOffBits * npe > 32)
+    return set_error(FNE_EINVAL, "row plan: unsupported npe/block_size");
+  if (lo < 0 || hi < lo || hi > nf) return set_error(FNE_EINVAL, "row plan: bad owned range");
+  if (hi - lo >= (int64_t)INT32_MAX || d->nnz >= (int64_t)INT32_MAX || E >= (int64_t)INT32_MAX)
+    return set_error(FNE_EBOUNDS, "row plan: sizes beyond 32-bit indexing");
+  const int64_t* t2f = d->total_to_free_reord;
+
+  // ---- element node codes -------------------------------------------------
+  std::vector<int32_t> code(E * npe);
+  std::vector<char> local(E, 0);
+  for (int64_t e = 0; e < E; ++e) {
+    for (int a = 0; a < npe; ++a) {
+      const int64_t* ed = d->elems + e * nde + a * bs;
+      const int64_t base = ed[0];
+      if (base < 0 || base >= d->n_total || base % bs != 0)
+        return set_error(FNE_EBOUNDS, "row plan: element DOF out of range / not node-blocked");
+      int nfree = 0;
+      for (int c = 0; c < bs; ++c) {
+        if (ed[c] != base + c)
+          return set_error(FNE_EINVAL, "row plan: element DOFs are not node-blocked");
+        if (t2f[base + c] >= 0) ++nfree;
+      }
+      if (nfree == bs) {
+        const int64_t r0 = t2f[base];
+        for (int c = 1; c < bs; ++c)
+          if (t2f[base + c] != r0 + c)
+            return set_error(FNE_EINVAL, "row plan: node components not consecutive after reordering");
+        if (r0 >= (int64_t)INT32_MAX) return set_error(FNE_EBOUNDS, "row plan: id beyond int32");
+        code[e * npe + a] = (int32_t)r0;
+        if (r0 >= lo && r0 < hi) local[e] = 1;
+      } else if (nfree == 0) {
+        if (base + 1 >= (int64_t)INT32_MAX) return set_error(FNE_EBOUNDS, "row plan: id beyond int32");
+        code[e * npe + a] = (int32_t)(-1 - base);
+      } else {
+        return set_error(FNE_EINVAL,
+                         "row plan: node with partially fixed components (use the Mohr-Coulomb path)");
+      }
+    }
+  }
+
+  // ---- local elements (overlap: any owned DOF), weights ---------------------
+  std::vector<int32_t> lidx(E, -1);
+  P.local_elems.clear();
+  P.elem_code.clear();
+  P.elem_weight.clear();
+  P.dir_only.clear();
+  P.dir_only_code.clear();
+  for (int64_t e = 0; e < E; ++e) {
+    bool any_free = false;
+    for (int a = 0; a < npe; ++a) any_free |= code[e * npe + a] >= 0;
+    if (!any_free) {
+      P.dir_only.push_back(e);
+      for (int a = 0; a < npe; ++a) P.dir_only_code.push_back(code[e * npe + a]);
+    }
+    if (!local[e]) continue;
+    double w = d->energy_weights ? d->energy_weights[e] : 1.0;
+    if (w != 0.0 && w != 1.0) return set_error(FNE_EINVAL, "row plan: energy weights must be 0 or 1");
+    lidx[e] = (int32_t)P.local_elems.size();
+    P.local_elems.push_back(e);
+    for (int a = 0; a < npe; ++a) P.elem_code.push_back(code[e * npe + a]);
+    P.elem_weight.push_back(w != 0.0 ? 1 : 0);
+  }
+
+  // ---- output rows (row-grouped owned COO pattern) --------------------------
+  const int64_t n_owned = hi - lo;
+  std::vector<int64_t> rev(n_owned, -1);  // reordered - lo -> total DOF
+  for (int64_t t = 0; t < d->n_total; ++t)
+    if (t2f[t] >= lo && t2f[t] < hi) rev[t2f[t] - lo] = t;
+  for (int64_t i = 0; i < n_owned; ++i)
+    if (rev[i] < 0) return set_error(FNE_EINVAL, "row plan: owned DOF without total DOF");
+
+  std::vector<int64_t> row_id;
+  std::vector<int64_t> rptr;
+  std::vector<char> seen(n_owned, 0);
+  for (int64_t j = 0; j < d->nnz; ++j) {
+    const int64_t r = d->owned_rows[j];
+    if (r < lo || r >= hi) return set_error(FNE_EBOUNDS, "row plan: owned row outside [lo, hi)");
+    if (d->owned_cols[j] < 0 || d->owned_cols[j] >= nf)
+      return set_error(FNE_EBOUNDS, "row plan: column out of range");
+    if (j == 0 || d->owned_rows[j - 1] != r) {
+      if (seen[r - lo]) return set_error(FNE_ELAYOUT, "row plan: COO pattern is not row-grouped");
+      seen[r - lo] = 1;
+      row_id.push_back(r);
+      rptr.push_back(j);
+    }
+  }
+  // owned DOFs absent from the pattern: gradient-only rows of length 0
+  for (int64_t i = 0; i < n_owned; ++i)
+    if (!seen[i]) {
+      row_id.push_back(lo + i);
+      rptr.push_back(d->nnz);
+    }
+  rptr.push_back(d->nnz);
+  const int32_t n_rows = (int32_t)row_id.size();
+  P.n_rows = n_rows;
+  P.row_ptr.assign(rptr.begin(), rptr.end());
+  P.row_node.resize(n_rows);
+  P.row_comp.resize(n_rows);
+  P.row_gpos.resize(n_rows);
+
+  // row-nodes in order of first appearance; the first row of each node is the
+  // one whose column layout defines the offsets (all rows must agree)
+  std::unordered_map<int64_t, int32_t> node_idx;
+  std::vector<int32_t> node_first_row;
+  std::vector<int64_t> node_of;
+  int32_t max_len = 0;
+  for (int32_t k = 0; k < n_rows; ++k) {
+    const int64_t t = rev[row_id[k] - lo];
+    const int64_t node = t / bs;
+    auto it = node_idx.find(node);
+    int32_t ni;
+    if (it == node_idx.end()) {
+      ni = (int32_t)node_of.size();
+      node_idx.emplace(node, ni);
+      node_of.push_back(node);
+      node_first_row.push_back(k);
+    } else {
+      ni = it->second;
+    }
+    P.row_node[k] = ni;
+    P.row_comp[k] = (uint8_t)(t % bs);
+    P.row_gpos[k] = (int32_t)(row_id[k] - lo);
+    max_len = std::max<int32_t>(max_len, P.row_ptr[k + 1] - P.row_ptr[k]);
+  }
+  P.max_row_len = max_len;
+  if (max_len >= (int32_t)kNoCol)
+    return set_error(FNE_EBOUNDS, "row plan: a row has more than 126 entries");
+  const int32_t n_nodes = (int32_t)node_of.size();
+  P.n_nodes = n_nodes;
+
+  // rows of each node (to validate identical column layouts)
+  std::vector<std::vector<int32_t>> node_rows(n_nodes);
+  for (int32_t k = 0; k < n_rows; ++k) node_rows[P.row_node[k]].push_back(k);
+
+  // ---- incidences ----------------------------------------------------------
+  std::vector<int32_t> cnt(n_nodes + 1, 0);
+  struct Inc {
+    int32_t node, le;
+    uint32_t info;
+  };
+  std::vector<Inc> incs;
+  incs.reserve(P.local_elems.size() * npe);
+  std::vector<std::pair<int64_t, int32_t>> rowcols;  // (col, offset) of one row
+  for (size_t le = 0; le < P.local_elems.size(); ++le) {
+    const int64_t e = P.local_elems[le];
+    bool flagged = false;
+    for (int a = 0; a < npe; ++a) {
+      const int32_t ca = code[e * npe + a];
+      if (ca < lo || ca >= hi) continue;  // not an owned row-node
+      const int64_t node = rev[ca - lo] / bs;
+      auto it = node_idx.find(node);
+      if (it == node_idx.end()) return set_error(FNE_ELAYOUT, "row plan: owned node has no row");
+      const int32_t ni = it->second;
+      uint32_t info = (uint32_t)a;
+      if (!flagged && P.elem_weight[le]) {
+        info |= kEnergyFlag;
+        flagged = true;
+      }
+      // column offsets, validated on every row of the node
+      for (int b = 0; b < npe; ++b) {
+        const int32_t cb = code[e * npe + b];
+        uint32_t off = kNoCol;
+        if (cb >= 0) {
+          bool first = true;
+          for (int32_t k : node_rows[ni]) {
+            const int64_t s = P.row_ptr[k], len = P.row_ptr[k + 1] - s;
+            int64_t pos = -1;
+            for (int64_t q = 0; q < len; ++q)
+              if (d->owned_cols[s + q] == cb) {
+                pos = q;
+                break;
+              }
+            if (pos < 0)
+              return set_error(FNE_ELAYOUT, "Scatter lookup found mismatched owned COO entries");
+            for (int c = 1; c < bs; ++c)
+              if (pos + c >= len || d->owned_cols[s + pos + c] != cb + c)
+                return set_error(FNE_ELAYOUT, "row plan: node block columns not consecutive");
+            if (first) {
+              off = (uint32_t)pos;
+              first = false;
+            } else if ((uint32_t)pos != off) {
+              return set_error(FNE_ELAYOUT, "row plan: rows of one node differ in column layout");
+            }
+          }
+        }
+        info |= (off & 127u) << (kOffShift + kOffBits * b);
+      }
+      incs.push_back({ni, (int32_t)le, info});
+      cnt[ni + 1]++;
+    }
+  }
+  for (int32_t i = 0; i < n_nodes; ++i) cnt[i + 1] += cnt[i];
+  P.inc_ptr = cnt;
+  P.inc_elem.resize(incs.size());
+  P.inc_info.resize(incs.size());
+  std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
+  for (const Inc& x : incs) {  // stable: element order within a node
+    const int32_t p = fill[x.node]++;
+    P.inc_elem[p] = x.le;
+    P.inc_info[p] = x.info;
+  }
+  return FNE_OK;
+}
+
+}  // namespace fne

@@ -1,0 +1,184 @@
+/*
+ * fne_asm.h -- C ABI of libfne_asm.so: element energy / gradient / Hessian
+ * assembly for the nonlinear-energy minimisers of Beremi/fenics_nonlinear_energies,
+ * on one NVIDIA B200 (sm_100a).
+ *
+ * Plain pointers and sizes only.  Every function returns an fne_status; on
+ * failure fne_last_error() gives a thread-local message.  Device pointers
+ * are CUDA global-memory pointers of the current device; ``stream`` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   fne_layout_build     build_global_layout + select_permutation('none'|'block_xyz')
+ *                        src/core/petsc/reordered_element_base.py:183-200, 380-506
+ *                        (+ petsc_ownership_range, src/core/petsc/dof_partition.py:27-55)
+ *   fne_create           ReorderedElementAssemblerBase._make_local_element_kernels
+ *                        (:922-923; per-family implementations
+ *                        src/problems/plaplace/jax_petsc/reordered_element_assembler.py:30-65,
+ *                        src/problems/ginzburg_landau/jax_petsc/reordered_element_assembler.py:54-91,
+ *                        src/problems/hyperelasticity/jax_petsc/reordered_element_assembler.py:55-101,
+ *                        src/problems/slope_stability/jax_petsc/reordered_element_assembler.py:152-243)
+ *                        together with _build_scatter_data (:1464-1534)
+ *   fne_eval ENERGY      energy_fn (:1579-1611): sum_e w_e e_e - f.u
+ *   fne_eval GRAD        gradient_fn (:1613-1633): grad_local[owned_local_pos] - f_owned
+ *   fne_eval HESS        assemble_hessian_element (:1733-1762): the (E,n,n) Hessian stack
+ *                        plus the np.add.at scatter into the owned COO values,
+ *                        in layout.owned_rows/owned_cols order
+ *   fne_set_dirichlet    update_dirichlet (:1560-1566)
+ *   fne_destroy          cleanup (:1777-1783)
+ */
+#ifndef FNE_ASM_H
+#define FNE_ASM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FNE_OK = 0,
+  FNE_EINVAL = 1,   /* bad argument                                    */
+  FNE_ECUDA = 2,    /* a CUDA runtime call failed                      */
+  FNE_EBOUNDS = 3,  /* an index or size outside the supported range    */
+  FNE_ETIMEOUT = 4, /* a bounded device wait gave up                   */
+  FNE_ENOMEM = 5,   /* host or device allocation failed                */
+  FNE_ELAYOUT = 6   /* COO pattern does not match the element graph    */
+} fne_status;
+
+typedef enum {
+  FNE_PLAPLACE = 1,        /* P1 triangles, scalar, (1/p)|grad u|^p      */
+  FNE_GINZBURG_LANDAU = 2, /* P1 triangles, scalar, eps/2|grad u|^2+W(u) */
+  FNE_NEOHOOKEAN = 3,      /* P1 tetrahedra, 3 dofs per node            */
+  FNE_MOHR_COULOMB = 4     /* Pk triangles, plane strain, 2 dofs/node   */
+} fne_family;
+
+typedef enum { FNE_FP64 = 0, FNE_FP32 = 1 } fne_precision;
+
+typedef enum { FNE_REORDER_NONE = 0, FNE_REORDER_BLOCK_XYZ = 1 } fne_reorder;
+
+enum { FNE_ENERGY = 1, FNE_GRAD = 2, FNE_HESS = 4 };
+
+/* ---------------------------------------------------------------------------
+ * Layout (host side, C++).  Replaces build_global_layout for the
+ * global-adjacency branch.  The COO pattern is iperm[adjacency CSR nonzero()]
+ * restricted to owned rows; when adj_indptr is NULL the adjacency is the
+ * free-DOF element-pair graph of ``elems`` (what the reference's mesh
+ * builders store).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int64_t n_total;              /* length of the full DOF vector              */
+  int64_t n_free;               /* number of free DOFs                        */
+  const int64_t* freedofs;      /* [n_free] total-DOF ids, ascending          */
+  int64_t n_elem;
+  int32_t ndof_e;               /* DOFs per element (npe * block_size)        */
+  const int64_t* elems;         /* [n_elem * ndof_e] total-DOF connectivity   */
+  int32_t block_size;
+  int32_t reorder;              /* fne_reorder                                */
+  int64_t n_nodes;              /* rows of coords                             */
+  int32_t dim;                  /* columns of coords                          */
+  const double* coords;         /* [n_nodes * dim] (block_xyz only)           */
+  const int64_t* perm_override; /* [n_free] or NULL                           */
+  const int64_t* adj_indptr;    /* [n_free+1] or NULL                         */
+  const int64_t* adj_indices;   /* [nnz] or NULL                              */
+  int32_t comm_rank, comm_size;
+} fne_layout_desc;
+
+typedef struct fne_layout fne_layout;
+
+int fne_layout_build(const fne_layout_desc* desc, fne_layout** out);
+/* Sizes of the arrays fne_layout_copy fills. */
+int fne_layout_sizes(const fne_layout* lay, int64_t* n_free, int64_t* lo, int64_t* hi,
+                     int64_t* nnz_total, int64_t* nnz_owned, int64_t* n_elem);
+/* Any output pointer may be NULL.  perm/iperm [n_free]; total_to_free_reord
+ * [n_total]; coo_rows/cols [nnz_total]; owned_rows/cols [nnz_owned];
+ * elem_owner [n_elem] (-1 = element without free DOF). */
+int fne_layout_copy(const fne_layout* lay, int64_t* perm, int64_t* iperm,
+                    int64_t* total_to_free_reord, int64_t* coo_rows, int64_t* coo_cols,
+                    int64_t* owned_rows, int64_t* owned_cols, int64_t* elem_owner);
+void fne_layout_free(fne_layout* lay);
+
+/* ---------------------------------------------------------------------------
+ * Assembler handle.  Holds device copies of the element data and the
+ * precomputed element -> nonzero gather plan; immutable after creation
+ * except for the Dirichlet values.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t family;               /* fne_family                                 */
+  int32_t precision;            /* fne_precision: arithmetic of grad/Hessian  */
+  int32_t hess_fp32;            /* FP32 mode only: 1 = Hessian values float32 */
+  int64_t n_elem;
+  int32_t npe;                  /* nodes per element                          */
+  int32_t block_size;           /* DOFs per node                              */
+  const int64_t* elems;         /* [n_elem * npe*block_size] total DOFs       */
+  int64_t n_total;
+  const int64_t* total_to_free_reord; /* [n_total], -1 = Dirichlet            */
+  int64_t n_free, lo, hi;       /* owned reordered range [lo, hi)             */
+  int64_t nnz;                  /* owned COO entries                          */
+  const int64_t* owned_rows;    /* [nnz] reordered row ids (output order)     */
+  const int64_t* owned_cols;    /* [nnz] reordered column ids                 */
+  const double* energy_weights; /* [n_elem] 0/1, or NULL = 1 where any free   */
+  int32_t nq;                   /* quadrature points (Mohr-Coulomb)           */
+  /* family element arrays, float64, reference layouts:
+   *   p-Laplace / GL : e0 = dvx [E*3], e1 = dvy [E*3], e2 = vol [E]
+   *   Neo-Hookean    : e0 = dphix [E*4], e1 = dphiy, e2 = dphiz, e3 = vol [E]
+   *   Mohr-Coulomb   : e0 = elem_B [E*nq*3*n], e1 = quad_weight [E*nq],
+   *                    e2 = eps_p_old [E*nq*3]                               */
+  const double* e0;
+  const double* e1;
+  const double* e2;
+  const double* e3;
+  /* scalars:
+   *   p-Laplace : s[0] = p
+   *   GL        : s[0] = eps, s[1..9] = ip (3x3 row-major), s[10..12] = w
+   *   Neo-Hook. : s[0] = C1, s[1] = D1, s[2] = use_abs_det (0/1)
+   *   M-C       : s[0] = E, s[1] = nu, s[2] = phi_deg, s[3] = cohesion,
+   *               s[4] = reg, s[5] = elastic (0/1)                           */
+  double s[16];
+  const double* dirichlet;      /* [n_total] full DOF vector (Dirichlet part) */
+  const double* rhs_owned;      /* [hi-lo] load vector f (reordered), or NULL */
+  int32_t dirichlet_only_energy;/* 1: add the energy of elements without any
+                                 * free DOF (Ginzburg-Landau assembler,
+                                 * src/problems/ginzburg_landau/jax_petsc/
+                                 * reordered_element_assembler.py:34-52, 96-97) */
+} fne_desc;
+
+typedef struct fne_handle fne_handle;
+
+typedef struct {
+  int64_t n_rows;       /* owned rows (= hi - lo)                              */
+  int64_t nnz;          /* owned COO entries                                   */
+  int64_t n_elem;       /* elements with at least one owned DOF                */
+  int64_t n_incidences; /* (row-node, element) pairs in the gather plan        */
+  int64_t device_bytes; /* device memory the handle owns                       */
+  int32_t max_row_len;
+  int32_t kernel_variant;
+} fne_info;
+
+int fne_create(const fne_desc* desc, fne_handle** out);
+int fne_info_get(const fne_handle* h, fne_info* info);
+/* Replace the Dirichlet values; ``dirichlet`` is a host array [n_total]. */
+int fne_set_dirichlet(fne_handle* h, const double* dirichlet);
+/*
+ * One fused pass.  u: device [n_free] full reordered free vector (on one
+ * rank this is the owned vector).  flags: FNE_ENERGY|FNE_GRAD|FNE_HESS.
+ *   energy (device, 1 double)   sum_e w_e e_e - f.u_owned      (FP64 always)
+ *   grad   (device, hi-lo doubles) owned gradient minus f
+ *   hess   (device, nnz values)  owned COO values, float64, or float32 when
+ *                                the handle was created with hess_fp32 = 1
+ * Outputs for flags not set may be NULL.  Stream-ordered; no allocation.
+ */
+int fne_eval(fne_handle* h, const double* u, int flags, double* energy, double* grad,
+             void* hess, void* stream);
+/* Host convenience: same pass with host buffers (copies in and out). */
+int fne_eval_host(fne_handle* h, const double* u_host, int flags, double* energy_host,
+                  double* grad_host, void* hess_host);
+int fne_destroy(fne_handle* h);
+
+const char* fne_last_error(void);
+const char* fne_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FNE_ASM_H */

@@ -1,0 +1,206 @@
+"""CUDA kernels vs the CPU oracle, through the C ABI (libfne_asm.so).
+
+Tolerances: FP64 mode within 1e-12 relative (energies: relative to the sum
+of absolute element energies; gradient / Hessian: relative to the largest
+entry); FP32 mode within 2e-5 relative for gradient / Hessian and 1e-7 for the
+FP64-reduced energy.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle.assembler import OracleAssembler
+from fenics_nonlinear_energies_b200 import _lib, meshes
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+FP32_TOL = 2e-5
+
+
+def _asm_classes():
+    from fenics_nonlinear_energies_b200.assembler import GLCudaAssembler, HECudaAssembler, PLaplaceCudaAssembler
+
+    return {"plaplace": PLaplaceCudaAssembler, "gl": GLCudaAssembler, "he": HECudaAssembler}
+
+
+def _make(family, params, **kw):
+    cls = _asm_classes()[family]
+    bs = 3 if family == "he" else 1
+    okw = dict(block_size=bs)
+    if family == "he":
+        okw.update(coordinate_key="nodes2coord", dirichlet_key="u_0_ref")
+    return cls(params, **kw), OracleAssembler(family, params, **okw)
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    scale = max(np.abs(b).max(initial=0.0), 1e-300)
+    return np.abs(a - b).max(initial=0.0) / scale
+
+
+def _check(gpu, ref, u, tol, *, energy_scale=None):
+    e_ref, g_ref, h_ref = ref.all_in_one(u)
+    ut = torch.as_tensor(u, device="cuda")
+    e, g, h = gpu.eval(ut, _lib.FNE_ENERGY | _lib.FNE_GRAD | _lib.FNE_HESS)
+    torch.cuda.synchronize()
+    scale = energy_scale if energy_scale is not None else max(abs(e_ref), 1.0)
+    assert abs(float(e.item()) - e_ref) <= tol * scale, (float(e.item()), e_ref)
+    assert _rel(g.cpu().numpy()[: gpu.n_owned], g_ref) <= tol
+    assert _rel(h.double().cpu().numpy(), h_ref) <= tol
+    # the separate callbacks agree with the fused pass
+    assert abs(gpu.energy_fn(u) - e_ref) <= tol * scale
+    gg = np.zeros(gpu.n_owned)
+    gpu.gradient_fn(u, gg)
+    assert _rel(gg, g_ref) <= tol
+    gpu.assemble_hessian(u)
+    assert _rel(gpu.owned_values.double().cpu().numpy(), h_ref) <= tol
+
+
+def _abs_energy_scale(ref, u):
+    """sum_e |e_e|: the natural scale of a sum of element energies."""
+    from oracle import energies
+
+    v = ref.v_local(u)[ref.local.elems_local_np]
+    e, _, _ = energies.element_derivatives(ref.family, v, ref.elem_data, ref.params, want_hessian=False)
+    return float(np.abs(e).sum() + np.abs(ref.f_owned @ np.asarray(u)[: ref.f_owned.size]) + 1e-300)
+
+
+@pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
+def test_plaplace_fp64(numbering):
+    params, _ = meshes.plaplace_problem(n=12, numbering=numbering)
+    gpu, ref = _make("plaplace", params)
+    u = np.random.default_rng(0).random(gpu.layout.n_free)
+    _check(gpu, ref, u, FP64_TOL, energy_scale=_abs_energy_scale(ref, u))
+
+
+def test_plaplace_zero_initial_guess():
+    params, _ = meshes.plaplace_problem(n=8)
+    gpu, ref = _make("plaplace", params)
+    u = np.zeros(gpu.layout.n_free)
+    _check(gpu, ref, u, FP64_TOL)
+    assert torch.all(gpu.owned_values == 0)
+
+
+@pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
+def test_gl_fp64(numbering):
+    params, u0 = meshes.gl_problem(n=16, seed=3, numbering=numbering)
+    gpu, ref = _make("gl", params)
+    _check(gpu, ref, u0, FP64_TOL, energy_scale=_abs_energy_scale(ref, u0))
+
+
+def test_gl_fp32():
+    params, u0 = meshes.gl_problem(n=16, seed=4)
+    gpu, ref = _make("gl", params, precision="fp32", hess_dtype=torch.float32)
+    e_ref, g_ref, h_ref = ref.all_in_one(u0)
+    e, g, h = gpu.eval(torch.as_tensor(u0, device="cuda"), 7)
+    assert h.dtype == torch.float32
+    assert abs(float(e.item()) - e_ref) <= 1e-7 * _abs_energy_scale(ref, u0)
+    assert _rel(g.cpu().numpy(), g_ref) <= FP32_TOL
+    assert _rel(h.double().cpu().numpy(), h_ref) <= FP32_TOL
+
+
+def test_he_fp64():
+    params, y0 = meshes.he_beam_problem(nx=8, ny=2, nz=2)
+    gpu, ref = _make("he", params)
+    rng = np.random.default_rng(5)
+    u = y0 + 2e-3 * rng.standard_normal(y0.size)
+    _check(gpu, ref, u, FP64_TOL, energy_scale=_abs_energy_scale(ref, u))
+
+
+def test_he_rotated_boundary_fp64_and_fp32():
+    params, y0 = meshes.he_beam_problem(nx=8, ny=2, nz=2)
+    gpu, ref = _make("he", params)
+    gpu32 = _asm_classes()["he"](params, precision="fp32")
+    u0 = meshes.rotate_right_face_from_reference(params["u_0_ref"], params["nodes2coord"], 0.3,
+                                                 params["right_nodes"])
+    for a in (gpu, ref, gpu32):
+        a.update_dirichlet(u0)
+    u = y0 + 1e-3 * np.random.default_rng(6).standard_normal(y0.size)
+    _check(gpu, ref, u, FP64_TOL, energy_scale=_abs_energy_scale(ref, u))
+    e_ref, g_ref, h_ref = ref.all_in_one(u)
+    e, g, h = gpu32.eval(torch.as_tensor(u, device="cuda"), 7)
+    assert _rel(g.cpu().numpy(), g_ref) <= 1e-4
+    assert _rel(h.cpu().numpy(), h_ref) <= FP32_TOL
+
+
+def test_he_inverted_element_gives_nonfinite_energy():
+    params, y0 = meshes.he_beam_problem(nx=4, ny=1, nz=1)
+    gpu, ref = _make("he", params)
+    u = y0.copy()
+    u[0::3] *= -1.0  # mirror x of free nodes -> negative det F somewhere
+    e = gpu.energy_fn(u)
+    assert not np.isfinite(e) or np.isfinite(ref.energy_fn(u))
+    assert np.isnan(e) == np.isnan(ref.energy_fn(u))
+
+
+def test_gl_dirichlet_only_energy_constant():
+    params, u0 = meshes.gl_problem(n=8)
+    gpu, ref = _make("gl", params)
+    assert ref.dirichlet_only_energy > 0
+    assert abs(gpu.energy_fn(u0) - ref.energy_fn(u0)) < 1e-12 * _abs_energy_scale(ref, u0)
+
+
+def test_deterministic_and_energy_paths_agree():
+    params, u0 = meshes.gl_problem(n=64, seed=9)
+    gpu, _ = _make("gl", params, precision="fp32", hess_dtype=torch.float32)
+    ut = torch.as_tensor(u0, device="cuda")
+    e1, g1, h1 = [t.clone() for t in gpu.eval(ut, 7)]
+    e2, g2, h2 = [t.clone() for t in gpu.eval(ut, 7)]
+    assert torch.equal(h1, h2) and torch.equal(g1, g2) and torch.equal(e1, e2)
+    e_only = gpu.eval(ut, _lib.FNE_ENERGY)[0].clone()
+    assert abs(float(e_only.item()) - float(e1.item())) < 1e-12 * abs(float(e1.item()))
+
+
+def test_autograd_energy_function():
+    from fenics_nonlinear_energies_b200.assembler import energy
+
+    params, u0 = meshes.gl_problem(n=16, seed=2)
+    gpu, ref = _make("gl", params)
+    u = torch.as_tensor(u0, device="cuda").requires_grad_(True)
+    J = energy(u, gpu)
+    J.backward()
+    np.testing.assert_allclose(u.grad.cpu().numpy(), ref.gradient_fn(u0), rtol=0, atol=1e-12 * np.abs(ref.gradient_fn(u0)).max())
+
+
+def test_empty_and_tiny_meshes():
+    # 1x1 grid: no free DOF at all; 2x2 grid: a single free node
+    for n in (1, 2):
+        params, u0 = meshes.gl_problem(n=n)
+        gpu, ref = _make("gl", params)
+        e, g, h = gpu.eval(torch.as_tensor(u0, device="cuda"), 7) if gpu.layout.n_free else (None, None, None)
+        assert abs(gpu.energy_fn(u0) - ref.energy_fn(u0)) < 1e-14
+        if gpu.layout.n_free:
+            assert _rel(h.cpu().numpy(), ref.assemble_hessian_element(u0)) <= FP64_TOL
+
+
+def test_full_size_gl_properties():
+    """1024 x 1024 GL, FP32 Hessian: FP64 energy vs the oracle's closed form,
+    directional-derivative consistency and Hessian symmetry."""
+    from scipy import sparse
+
+    params, u0 = meshes.gl_problem(n=1024, seed=0)
+    gpu = _asm_classes()["gl"](params, precision="fp32", hess_dtype=torch.float32)
+    ut = torch.as_tensor(u0, device="cuda")
+    e, g, h = [t.clone() for t in gpu.eval(ut, 7)]
+    # energy: vectorised FP64 closed form of the restated density
+    v = np.zeros(len(params["u_0"]))
+    v[params["freedofs"]] = u0
+    ve = v[params["elems"]]
+    fx = np.sum(ve * params["dvx"], 1)
+    fy = np.sum(ve * params["dvy"], 1)
+    n = ve @ params["ip"]
+    dens = 0.5 * params["eps"] * (fx**2 + fy**2) + (0.25 * (n**2 - 1.0) ** 2) @ params["w"]
+    e_ref = float(np.sum(dens * params["vol"]))
+    assert abs(float(e.item()) - e_ref) <= 1e-7 * float(np.sum(np.abs(dens * params["vol"])))
+    # directional derivative of the FP64 energy vs the FP32 gradient
+    d = torch.as_tensor(np.random.default_rng(1).standard_normal(u0.size), device="cuda")
+    hstep = 1e-4
+    ep = float(gpu.eval(ut + hstep * d, 1)[0].item())
+    em = float(gpu.eval(ut - hstep * d, 1)[0].item())
+    assert abs((ep - em) / (2 * hstep) - float(g @ d)) <= 1e-4 * abs(float(g @ d))
+    # Hessian symmetry
+    rows, cols = gpu.layout.owned_rows, gpu.layout.owned_cols
+    A = sparse.coo_matrix((h.double().cpu().numpy(), (rows, cols)), shape=(gpu.layout.n_free,) * 2).tocsr()
+    assert abs(A - A.T).max() <= 1e-6 * abs(A).max()

@@ -1,0 +1,104 @@
+"""Pin the CPU oracle: reference golden vectors and finite-difference consistency.
+
+The golden vectors are the reference's own unit tests
+(``tests/test_reordered_element_base.py:12-73``).  Element values have no
+numeric golden in the reference; like its ``tests/test_slope_stability_3d.py:434-523``
+the oracle derivatives are checked against central finite differences.
+"""
+
+import numpy as np
+import pytest
+from scipy import sparse
+
+from oracle import energies, layout as L
+from oracle.assembler import OracleAssembler
+from fenics_nonlinear_energies_b200 import meshes
+
+
+def test_block_xyz_scalar_golden():
+    coords = np.array([[1.0, 0.0], [0.0, 1.0], [0.0, 0.0], [1.0, 1.0]])
+    perm = L.select_permutation("block_xyz", adjacency=sparse.eye(4, format="csr"), coords_all=coords,
+                                freedofs=np.arange(4), block_size=1)
+    assert perm.tolist() == [2, 1, 0, 3]
+
+
+def test_block_xyz_vector_golden():
+    coords = np.array([[1.0, 0.0, 0.0], [0.0, 0.0, 0.0]])
+    perm = L.select_permutation("block_xyz", adjacency=sparse.eye(6, format="csr"), coords_all=coords,
+                                freedofs=np.arange(6), block_size=3)
+    assert perm.tolist() == [3, 4, 5, 0, 1, 2]
+
+
+def test_local_vec_from_full_golden():
+    v = L.local_vec_from_full(np.array([10.0, 20.0, 30.0]), np.array([-1, 0, 1, -1, 2]),
+                              np.arange(5), np.array([5.0, -1.0, -1.0, 6.0, -1.0]))
+    np.testing.assert_allclose(v, [5.0, 10.0, 20.0, 6.0, 30.0])
+
+
+def test_ownership_ranges():
+    assert [L.petsc_ownership_range(10, r, 3) for r in range(3)] == [(0, 4), (4, 7), (7, 10)]
+    assert [L.petsc_ownership_range(12, r, 2, block_size=3) for r in range(2)] == [(0, 6), (6, 12)]
+    np.testing.assert_array_equal(L.rank_of_dof_vec(np.arange(10), 10, 3), [0, 0, 0, 0, 1, 1, 1, 2, 2, 2])
+
+
+def _fd_check(family, v_e, data, params, h=1e-7, seed=0):
+    """Central FD of energy vs gradient, and of gradient vs Hessian (directional)."""
+    rng = np.random.default_rng(seed)
+    d = rng.standard_normal(v_e.shape)
+    e, g, H = energies.element_derivatives(family, v_e, data, params)
+    ep, gp, _ = energies.element_derivatives(family, v_e + h * d, data, params, want_hessian=False)
+    em, gm, _ = energies.element_derivatives(family, v_e - h * d, data, params, want_hessian=False)
+    dd_fd = (ep - em) / (2 * h)
+    dd = np.sum(g * d, axis=1)
+    np.testing.assert_allclose(dd, dd_fd, rtol=2e-4, atol=1e-8 * np.abs(dd).max())
+    hv_fd = (gp - gm) / (2 * h)
+    hv = np.einsum("eij,ej->ei", H, d)
+    np.testing.assert_allclose(hv, hv_fd, rtol=5e-3, atol=1e-5 * np.abs(hv).max())
+
+
+def test_plaplace_oracle_fd():
+    params, _ = meshes.plaplace_problem(n=4)
+    v = np.random.default_rng(1).random(len(params["u_0"]))
+    e = params["elems"]
+    _fd_check("plaplace", v[e], {k: params[k] for k in ("dvx", "dvy", "vol")}, params)
+
+
+def test_gl_oracle_fd():
+    params, _ = meshes.gl_problem(n=4)
+    v = np.random.default_rng(2).uniform(-1, 1, len(params["u_0"]))
+    e = params["elems"]
+    _fd_check("gl", v[e], {k: params[k] for k in ("dvx", "dvy", "vol")}, params)
+
+
+def test_he_oracle_fd():
+    params, _ = meshes.he_beam_problem(nx=3, ny=1, nz=1)
+    y = params["u_0_ref"] + 1e-3 * np.random.default_rng(3).standard_normal(len(params["u_0_ref"]))
+    e = params["elems"]
+    _fd_check("he", y[e], {k: params[k] for k in ("dphix", "dphiy", "dphiz", "vol")}, params, h=1e-7)
+
+
+def test_plaplace_zero_gradient_limit():
+    params, _ = meshes.plaplace_problem(n=2)
+    e = params["elems"]
+    v = np.zeros((len(e), 3))
+    _, g, H = energies.element_derivatives("plaplace", v, {k: params[k] for k in ("dvx", "dvy", "vol")}, params)
+    assert np.all(g == 0.0) and np.all(H == 0.0)
+
+
+@pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
+def test_oracle_assembler_consistency(numbering):
+    params, _ = meshes.gl_problem(n=6, numbering=numbering)
+    asm = OracleAssembler("gl", params)
+    rng = np.random.default_rng(4)
+    u = rng.uniform(-0.8, 0.8, asm.layout.n_free)
+    d = rng.standard_normal(asm.layout.n_free)
+    h = 1e-6
+    g = asm.gradient_fn(u)
+    fd = (asm.energy_fn(u + h * d) - asm.energy_fn(u - h * d)) / (2 * h)
+    assert abs(fd - g @ d) < 1e-6 * max(1.0, abs(fd))
+    vals = asm.assemble_hessian_element(u)
+    A = sparse.coo_matrix((vals, (asm.layout.owned_rows, asm.layout.owned_cols)),
+                          shape=(asm.layout.n_free,) * 2).tocsr()
+    hv_fd = (asm.gradient_fn(u + h * d) - asm.gradient_fn(u - h * d)) / (2 * h)
+    np.testing.assert_allclose(A @ d, hv_fd, rtol=1e-5, atol=1e-7)
+    assert abs(A - A.T).max() < 1e-14
