@@ -53,6 +53,7 @@ class Desc(C.Structure):
         ("e0", _f64p), ("e1", _f64p), ("e2", _f64p), ("e3", _f64p),
         ("s", C.c_double * 16),
         ("dirichlet", _f64p), ("rhs_owned", _f64p), ("dirichlet_only_energy", C.c_int32),
+        ("kernel_variant", C.c_int32),
     ]
 
 

@@ -51,7 +51,8 @@ class CudaElementAssemblerBase:
     local_elem_data_keys: tuple[str, ...] = ()
 
     def __init__(self, params, comm=None, adjacency=None, *, reorder_mode="block_xyz", perm_override=None,
-                 precision="fp64", hess_dtype=None, device=None, **_ignored_solver_kwargs):
+                 precision="fp64", hess_dtype=None, device=None, kernel_variant="auto",
+                 **_ignored_solver_kwargs):
         if not torch.cuda.is_available():
             raise RuntimeError("CudaElementAssemblerBase needs a CUDA device (no CPU fallback)")
         t_setup = time.perf_counter()
@@ -122,6 +123,7 @@ class CudaElementAssemblerBase:
             d.s[i] = float(v)
         d.nq = int(self._nq())
         d.dirichlet_only_energy = 1 if (self._adds_dirichlet_only_energy() and self.rank == 0) else 0
+        d.kernel_variant = {"auto": 0, "row_gather": 1, "incidence": 2}[kernel_variant]
         self._handle = _lib.C.c_void_p()
         check(lib.fne_create(_lib.C.byref(d), _lib.C.byref(self._handle)))
         del keep

@@ -51,55 +51,23 @@ struct Phys {
   int absdet;
 };
 
-// P1 triangle record.  FP32: 48 B (3 x 16 B loads); FP64: 80 B (5 x 16 B).
-struct __align__(16) TriRecF {
-  int src[3];
-  int wflag;
-  float dvx[3];
-  float vol;
-  float dvy[3];
-  float pad;
-};
-struct __align__(16) TriRecD {
-  int src[3];
-  int wflag;
-  double vol, dvx[3], dvy[3], pad;
-};
-// P1 tetrahedron record.  FP32: 80 B; FP64: 128 B.
-struct __align__(16) TetRecF {
-  int src[4];
-  float gx[4], gy[4], gz[4];
-  float vol;
-  int wflag;
-  float pad[2];
-};
-struct __align__(16) TetRecD {
-  int src[4];
-  double gx[4], gy[4], gz[4];
-  double vol;
-  int wflag;
-  int pad;
-};
-
-template <typename Real>
-struct TriRecT;
-template <>
-struct TriRecT<float> {
-  using T = TriRecF;
-};
-template <>
-struct TriRecT<double> {
-  using T = TriRecD;
+// Element records are stored as "chunk planes": plane k of an element record
+// is the 16-byte chunk  base[k * n + e], so a warp loading plane k of 32
+// consecutive elements reads 512 contiguous bytes.
+//   P1 triangle, FP32 (3 planes, 48 B): {src0,src1,src2,wflag} {dvx0,dvx1,dvx2,vol} {dvy0,dvy1,dvy2,-}
+//   P1 triangle, FP64 (5 planes, 80 B): {src0,src1,src2,wflag} {vol,dvx0} {dvx1,dvx2} {dvy0,dvy1} {dvy2,-}
+//   P1 tet, FP32 (5 planes, 80 B):  {src0..3} {gx0..3} {gy0..3} {gz0..3} {vol,wflag,-,-}
+//   P1 tet, FP64 (8 planes, 128 B): {src0..3} {gx0,gx1} {gx2,gx3} {gy..} {gy..} {gz..} {gz..} {vol,wflag}
+struct __align__(16) Chunk {
+  unsigned w[4];
 };
 template <typename Real>
-struct TetRecT;
-template <>
-struct TetRecT<float> {
-  using T = TetRecF;
+struct TriPlanes {
+  static constexpr int n = sizeof(Real) == 4 ? 3 : 5;
 };
-template <>
-struct TetRecT<double> {
-  using T = TetRecD;
+template <typename Real>
+struct TetPlanes {
+  static constexpr int n = sizeof(Real) == 4 ? 5 : 8;
 };
 
 template <typename Real>
@@ -116,33 +84,40 @@ struct TetElem {
   Real vol;
 };
 
-__device__ __forceinline__ void load_tri(const TriRecF* __restrict__ R, int e, TriElem<float>& t) {
-  const int4* p = reinterpret_cast<const int4*>(R + e);
-  const int4 c0 = __ldg(p);
-  const float4 c1 = __ldg(reinterpret_cast<const float4*>(p + 1));
-  const float4 c2 = __ldg(reinterpret_cast<const float4*>(p + 2));
+__device__ __forceinline__ int4 ldc_i(const Chunk* __restrict__ R, long long off) {
+  return __ldg(reinterpret_cast<const int4*>(R + off));
+}
+__device__ __forceinline__ float4 ldc_f(const Chunk* __restrict__ R, long long off) {
+  return __ldg(reinterpret_cast<const float4*>(R + off));
+}
+__device__ __forceinline__ double2 ldc_d(const Chunk* __restrict__ R, long long off) {
+  return __ldg(reinterpret_cast<const double2*>(R + off));
+}
+
+__device__ __forceinline__ void load_tri(const Chunk* __restrict__ R, int n, int e, TriElem<float>& t) {
+  const int4 c0 = ldc_i(R, e);
+  const float4 c1 = ldc_f(R, (long long)n + e);
+  const float4 c2 = ldc_f(R, 2LL * n + e);
   t.src[0] = c0.x; t.src[1] = c0.y; t.src[2] = c0.z; t.wflag = c0.w;
   t.dvx[0] = c1.x; t.dvx[1] = c1.y; t.dvx[2] = c1.z; t.vol = c1.w;
   t.dvy[0] = c2.x; t.dvy[1] = c2.y; t.dvy[2] = c2.z;
 }
-__device__ __forceinline__ void load_tri(const TriRecD* __restrict__ R, int e, TriElem<double>& t) {
-  const int4* p = reinterpret_cast<const int4*>(R + e);
-  const int4 c0 = __ldg(p);
-  const double2 d0 = __ldg(reinterpret_cast<const double2*>(p + 1));
-  const double2 d1 = __ldg(reinterpret_cast<const double2*>(p + 2));
-  const double2 d2 = __ldg(reinterpret_cast<const double2*>(p + 3));
-  const double2 d3 = __ldg(reinterpret_cast<const double2*>(p + 4));
+__device__ __forceinline__ void load_tri(const Chunk* __restrict__ R, int n, int e, TriElem<double>& t) {
+  const int4 c0 = ldc_i(R, e);
+  const double2 d0 = ldc_d(R, (long long)n + e);
+  const double2 d1 = ldc_d(R, 2LL * n + e);
+  const double2 d2 = ldc_d(R, 3LL * n + e);
+  const double2 d3 = ldc_d(R, 4LL * n + e);
   t.src[0] = c0.x; t.src[1] = c0.y; t.src[2] = c0.z; t.wflag = c0.w;
   t.vol = d0.x; t.dvx[0] = d0.y; t.dvx[1] = d1.x; t.dvx[2] = d1.y;
   t.dvy[0] = d2.x; t.dvy[1] = d2.y; t.dvy[2] = d3.x;
 }
-__device__ __forceinline__ void load_tet(const TetRecF* __restrict__ R, int e, TetElem<float>& t) {
-  const int4* p = reinterpret_cast<const int4*>(R + e);
-  const int4 c0 = __ldg(p);
-  const float4 x = __ldg(reinterpret_cast<const float4*>(p + 1));
-  const float4 y = __ldg(reinterpret_cast<const float4*>(p + 2));
-  const float4 z = __ldg(reinterpret_cast<const float4*>(p + 3));
-  const float4 v = __ldg(reinterpret_cast<const float4*>(p + 4));
+__device__ __forceinline__ void load_tet(const Chunk* __restrict__ R, int n, int e, TetElem<float>& t) {
+  const int4 c0 = ldc_i(R, e);
+  const float4 x = ldc_f(R, (long long)n + e);
+  const float4 y = ldc_f(R, 2LL * n + e);
+  const float4 z = ldc_f(R, 3LL * n + e);
+  const float4 v = ldc_f(R, 4LL * n + e);
   t.src[0] = c0.x; t.src[1] = c0.y; t.src[2] = c0.z; t.src[3] = c0.w;
   t.g[0][0] = x.x; t.g[1][0] = x.y; t.g[2][0] = x.z; t.g[3][0] = x.w;
   t.g[0][1] = y.x; t.g[1][1] = y.y; t.g[2][1] = y.z; t.g[3][1] = y.w;
@@ -150,19 +125,17 @@ __device__ __forceinline__ void load_tet(const TetRecF* __restrict__ R, int e, T
   t.vol = v.x;
   t.wflag = __float_as_int(v.y);
 }
-__device__ __forceinline__ void load_tet(const TetRecD* __restrict__ R, int e, TetElem<double>& t) {
-  const int4* p = reinterpret_cast<const int4*>(R + e);
-  const int4 c0 = __ldg(p);
+__device__ __forceinline__ void load_tet(const Chunk* __restrict__ R, int n, int e, TetElem<double>& t) {
+  const int4 c0 = ldc_i(R, e);
   t.src[0] = c0.x; t.src[1] = c0.y; t.src[2] = c0.z; t.src[3] = c0.w;
-  const double2* q = reinterpret_cast<const double2*>(p + 1);
   double2 a;
-  a = __ldg(q + 0); t.g[0][0] = a.x; t.g[1][0] = a.y;
-  a = __ldg(q + 1); t.g[2][0] = a.x; t.g[3][0] = a.y;
-  a = __ldg(q + 2); t.g[0][1] = a.x; t.g[1][1] = a.y;
-  a = __ldg(q + 3); t.g[2][1] = a.x; t.g[3][1] = a.y;
-  a = __ldg(q + 4); t.g[0][2] = a.x; t.g[1][2] = a.y;
-  a = __ldg(q + 5); t.g[2][2] = a.x; t.g[3][2] = a.y;
-  a = __ldg(q + 6); t.vol = a.x;
+  a = ldc_d(R, 1LL * n + e); t.g[0][0] = a.x; t.g[1][0] = a.y;
+  a = ldc_d(R, 2LL * n + e); t.g[2][0] = a.x; t.g[3][0] = a.y;
+  a = ldc_d(R, 3LL * n + e); t.g[0][1] = a.x; t.g[1][1] = a.y;
+  a = ldc_d(R, 4LL * n + e); t.g[2][1] = a.x; t.g[3][1] = a.y;
+  a = ldc_d(R, 5LL * n + e); t.g[0][2] = a.x; t.g[1][2] = a.y;
+  a = ldc_d(R, 6LL * n + e); t.g[2][2] = a.x; t.g[3][2] = a.y;
+  a = ldc_d(R, 7LL * n + e); t.vol = a.x;
   t.wflag = __double2loint(a.y);
 }
 
@@ -249,6 +222,73 @@ __device__ __forceinline__ double tri_energy(const Phys& P, const double v[3], c
       pot += 0.25 * m * m * P.w[q];
     }
     return (0.5 * P.eps * s + pot) * (double)t.vol;
+  }
+}
+
+// All three rows at once: gradient g[3] and the symmetric Hessian as its upper
+// triangle H = {H00, H01, H02, H11, H12, H22}.
+template <typename Real, int FAM>
+__device__ __forceinline__ void tri_full(const Phys& P, const Real v[3], const TriElem<Real>& t, Real g[3],
+                                         Real H[6]) {
+  const Real fx = v[0] * t.dvx[0] + v[1] * t.dvx[1] + v[2] * t.dvx[2];
+  const Real fy = v[0] * t.dvy[0] + v[1] * t.dvy[1] + v[2] * t.dvy[2];
+  Real G[3];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) G[b] = fx * t.dvx[b] + fy * t.dvy[b];
+  Real K[6];
+  K[0] = t.dvx[0] * t.dvx[0] + t.dvy[0] * t.dvy[0];
+  K[1] = t.dvx[0] * t.dvx[1] + t.dvy[0] * t.dvy[1];
+  K[2] = t.dvx[0] * t.dvx[2] + t.dvy[0] * t.dvy[2];
+  K[3] = t.dvx[1] * t.dvx[1] + t.dvy[1] * t.dvy[1];
+  K[4] = t.dvx[1] * t.dvx[2] + t.dvy[1] * t.dvy[2];
+  K[5] = t.dvx[2] * t.dvx[2] + t.dvy[2] * t.dvy[2];
+  if (FAM == FAM_PLAP) {
+    const Real s = fx * fx + fy * fy;
+    const Real p = (Real)P.p;
+    Real t1, t2;
+    if (s > Real(0)) {
+      if (P.p == 3.0) {
+        t1 = sqrt(s);
+        t2 = Real(1) / t1;
+      } else {
+        t1 = pow(s, p * Real(0.5) - Real(1));
+        t2 = (p - Real(2)) * pow(s, p * Real(0.5) - Real(2));
+      }
+    } else {
+      t1 = P.p == 2.0 ? Real(1) : (P.p > 2.0 ? Real(0) : Real(INFINITY));
+      t2 = Real(0);
+    }
+    const Real vt1 = t.vol * t1, vt2 = t.vol * t2;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) g[b] = vt1 * G[b];
+    H[0] = vt1 * K[0] + vt2 * G[0] * G[0];
+    H[1] = vt1 * K[1] + vt2 * G[0] * G[1];
+    H[2] = vt1 * K[2] + vt2 * G[0] * G[2];
+    H[3] = vt1 * K[3] + vt2 * G[1] * G[1];
+    H[4] = vt1 * K[4] + vt2 * G[1] * G[2];
+    H[5] = vt1 * K[5] + vt2 * G[2] * G[2];
+  } else {
+    const Real eps = (Real)P.eps;
+    Real ip[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) ip[k] = (Real)P.ip[k];
+    Real c1[3], c2[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const Real n = v[0] * ip[q] + v[1] * ip[3 + q] + v[2] * ip[6 + q];
+      c1[q] = (Real)P.w[q] * (n * n - Real(1)) * n;
+      c2[q] = (Real)P.w[q] * (Real(3) * n * n - Real(1));
+    }
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      g[b] = t.vol * (eps * G[b] + c1[0] * ip[3 * b] + c1[1] * ip[3 * b + 1] + c1[2] * ip[3 * b + 2]);
+    int m = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = a; b < 3; ++b, ++m)
+        H[m] = t.vol * (eps * K[m] + c2[0] * ip[3 * a] * ip[3 * b] + c2[1] * ip[3 * a + 1] * ip[3 * b + 1] +
+                        c2[2] * ip[3 * a + 2] * ip[3 * b + 2]);
   }
 }
 
@@ -407,8 +447,9 @@ __device__ void energy_finalize(double v, const EnergyOut& eo) {
   }
 }
 
+
 // ---------------------------------------------------------------------------
-// row-gather kernels
+// row-gather kernels (one thread per owned row; incidences recomputed)
 // ---------------------------------------------------------------------------
 struct RowArgs {
   int n_rows;
@@ -423,15 +464,16 @@ struct RowArgs {
   const double* __restrict__ dir;
   const double* __restrict__ rhs;  // may be null
   long long lo;
+  int nrec;                        // records (plane stride)
 };
 
 constexpr int kTriRows = 256;
 constexpr int kTetRows = 128;
 
 template <typename Real, int FAM, int WANT, typename HOut>
-__global__ void __launch_bounds__(kTriRows) k_rows_tri(RowArgs A, const typename TriRecT<Real>::T* __restrict__ R,
-                                                       Phys P, double* __restrict__ grad,
-                                                       HOut* __restrict__ hess, EnergyOut eo) {
+__global__ void __launch_bounds__(kTriRows) k_rows_tri(RowArgs A, const Chunk* __restrict__ R, Phys P,
+                                                       double* __restrict__ grad, HOut* __restrict__ hess,
+                                                       EnergyOut eo) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real* sacc = reinterpret_cast<Real*>(smem_raw);
   const int r0 = blockIdx.x * blockDim.x;
@@ -453,7 +495,7 @@ __global__ void __launch_bounds__(kTriRows) k_rows_tri(RowArgs A, const typename
       const int el = __ldg(A.inc_elem + i);
       const unsigned info = __ldg(A.inc_info + i);
       TriElem<Real> t;
-      load_tri(R, el, t);
+      load_tri(R, A.nrec, el, t);
       double vd[3];
 #pragma unroll
       for (int b = 0; b < 3; ++b) vd[b] = gather(A.u, A.dir, t.src[b], 0);
@@ -483,9 +525,9 @@ __global__ void __launch_bounds__(kTriRows) k_rows_tri(RowArgs A, const typename
 }
 
 template <typename Real, int WANT, typename HOut>
-__global__ void __launch_bounds__(kTetRows) k_rows_tet(RowArgs A, const typename TetRecT<Real>::T* __restrict__ R,
-                                                       Phys P, double* __restrict__ grad,
-                                                       HOut* __restrict__ hess, EnergyOut eo) {
+__global__ void __launch_bounds__(kTetRows) k_rows_tet(RowArgs A, const Chunk* __restrict__ R, Phys P,
+                                                       double* __restrict__ grad, HOut* __restrict__ hess,
+                                                       EnergyOut eo) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real* sacc = reinterpret_cast<Real*>(smem_raw);
   const int r0 = blockIdx.x * blockDim.x;
@@ -508,7 +550,7 @@ __global__ void __launch_bounds__(kTetRows) k_rows_tet(RowArgs A, const typename
       const int el = __ldg(A.inc_elem + i);
       const unsigned info = __ldg(A.inc_info + i);
       TetElem<Real> t;
-      load_tet(R, el, t);
+      load_tet(R, A.nrec, el, t);
       double yd[4][3];
       Real y[4][3];
 #pragma unroll
@@ -549,12 +591,101 @@ __global__ void __launch_bounds__(kTetRows) k_rows_tet(RowArgs A, const typename
 }
 
 // ---------------------------------------------------------------------------
+// Incidence-parallel kernel (P1 triangles): one thread per (row, element)
+// incidence.  Each thread runs one short chain of independent loads
+// (incidence word -> element record -> 3 nodal values), evaluates the
+// element's gradient entry and Hessian row for its local node, and the CTA
+// sums the incidences of each row in shared memory in rank order (round k
+// adds the k-th incidence of every row: no two writers per address, fixed
+// order).  The CTA's rows are one contiguous slice of the COO values, written
+// with coalesced stores.
+// ---------------------------------------------------------------------------
+struct IncArgs {
+  const int* __restrict__ cta_row;
+  const int* __restrict__ cta_inc;
+  const int* __restrict__ inc_elem;
+  const unsigned* __restrict__ inc_word;
+  const unsigned short* __restrict__ inc_rowl;
+  int max_rank;
+  int max_rows;
+  int max_len;
+};
+constexpr int kIncThreads = 512;
+
+template <typename Real, int FAM, int WANT, typename HOut>
+__global__ void __launch_bounds__(kIncThreads, 2) k_inc_tri(RowArgs A, IncArgs Q, const Chunk* __restrict__ R,
+                                                            Phys P, double* __restrict__ grad,
+                                                            HOut* __restrict__ hess, EnergyOut eo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int cta = blockIdx.x;
+  const int r0 = Q.cta_row[cta], r1 = Q.cta_row[cta + 1];
+  const int i0 = Q.cta_inc[cta], i1 = Q.cta_inc[cta + 1];
+  const int cs = A.row_ptr[r0];
+  const int clen = A.row_ptr[r1] - cs;
+  const int nrows = r1 - r0;
+  Real* sgrad = reinterpret_cast<Real*>(smem_raw);        // [max_rows]
+  Real* srow = sgrad + Q.max_rows;                         // [max_len]
+  int* sbase = reinterpret_cast<int*>(srow + Q.max_len);   // [max_rows] slice offset of each row
+  for (int k = threadIdx.x; k < nrows; k += blockDim.x) {
+    sbase[k] = A.row_ptr[r0 + k] - cs;
+    if (WANT & W_G) sgrad[k] = Real(0);
+  }
+  if (WANT & W_H)
+    for (int j = threadIdx.x; j < clen; j += blockDim.x) srow[j] = Real(0);
+  const int i = i0 + threadIdx.x;
+  const bool active = i < i1;
+  unsigned w = 0;
+  int rl = 0;
+  Real ga = Real(0), h[3] = {Real(0), Real(0), Real(0)};
+  double eacc = 0.0;
+  if (active) {
+    const int el = __ldg(Q.inc_elem + i);
+    w = __ldg(Q.inc_word + i);
+    rl = __ldg(Q.inc_rowl + i);
+    TriElem<Real> t;
+    load_tri(R, A.nrec, el, t);
+    double vd[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) vd[b] = gather(A.u, A.dir, t.src[b], 0);
+    const Real v[3] = {(Real)vd[0], (Real)vd[1], (Real)vd[2]};
+    tri_row<Real, FAM>(P, (int)(w & 3u), v, t, ga, h);
+    if ((WANT & W_E) && (w & 4u)) eacc = tri_energy<Real, FAM>(P, vd, t);
+  }
+  __syncthreads();
+  if (WANT & (W_G | W_H)) {
+    const int rank = (w >> 3) & 15u;
+    const int base = active ? sbase[rl] : 0;
+    for (int k = 0; k <= Q.max_rank; ++k) {
+      if (active && rank == k) {
+        if (WANT & W_G) sgrad[rl] += ga;
+        if (WANT & W_H) {
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const unsigned off = (w >> (7 + kOffBits * b)) & 127u;
+            if (off != kNoCol) srow[base + off] += h[b];
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int k = threadIdx.x; k < nrows; k += blockDim.x) {
+    const int gp = A.row_gpos[r0 + k];
+    if (WANT & W_G) grad[gp] = (double)sgrad[k] - (A.rhs ? A.rhs[gp] : 0.0);
+    if ((WANT & W_E) && A.rhs) eacc -= A.rhs[gp] * A.u[A.lo + gp];
+  }
+  if (WANT & W_H)
+    for (int j = threadIdx.x; j < clen; j += blockDim.x) hess[cs + j] = (HOut)srow[j];
+  if (WANT & W_E) energy_finalize(eacc, eo);
+}
+
+// ---------------------------------------------------------------------------
 // energy-only kernels (element-centric, grid-stride)
 // ---------------------------------------------------------------------------
 constexpr int kElemThreads = 256;
 
 template <typename Real, int FAM>
-__global__ void __launch_bounds__(kElemThreads) k_energy_tri(const typename TriRecT<Real>::T* __restrict__ R, int n_el,
+__global__ void __launch_bounds__(kElemThreads) k_energy_tri(const Chunk* __restrict__ R, int nrec, int n_el,
                                                              const double* __restrict__ u, const double* __restrict__ dir,
                                                              Phys P, const double* __restrict__ rhs, int n_owned,
                                                              long long lo, EnergyOut eo) {
@@ -562,7 +693,7 @@ __global__ void __launch_bounds__(kElemThreads) k_energy_tri(const typename TriR
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += stride) {
     TriElem<Real> t;
-    load_tri(R, e, t);
+    load_tri(R, nrec, e, t);
     if (!t.wflag) continue;
     double vd[3];
 #pragma unroll
@@ -575,7 +706,7 @@ __global__ void __launch_bounds__(kElemThreads) k_energy_tri(const typename TriR
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(kElemThreads) k_energy_tet(const typename TetRecT<Real>::T* __restrict__ R, int n_el,
+__global__ void __launch_bounds__(kElemThreads) k_energy_tet(const Chunk* __restrict__ R, int nrec, int n_el,
                                                              const double* __restrict__ u, const double* __restrict__ dir,
                                                              Phys P, const double* __restrict__ rhs, int n_owned,
                                                              long long lo, EnergyOut eo) {
@@ -583,7 +714,7 @@ __global__ void __launch_bounds__(kElemThreads) k_energy_tet(const typename TetR
   const int stride = gridDim.x * blockDim.x;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += stride) {
     TetElem<Real> t;
-    load_tet(R, e, t);
+    load_tet(R, nrec, e, t);
     if (!t.wflag) continue;
     double yd[4][3];
 #pragma unroll
@@ -603,23 +734,28 @@ __global__ void __launch_bounds__(kElemThreads) k_energy_tet(const typename TetR
 struct fne_handle {
   int family = 0, precision = 0, hess_fp32 = 0, npe = 0, bs = 0;
   int64_t n_total = 0, n_free = 0, lo = 0, hi = 0, nnz = 0;
-  int n_rows = 0, n_local = 0, n_dir_only = 0, rows_per_cta = 0, grid_rows = 0, grid_elem = 0;
+  int n_rows = 0, n_local = 0, n_dir_only = 0, rows_per_cta = 0, grid_rows = 0;
   int64_t n_inc = 0;
   int max_row_len = 0;
   size_t smem_bytes = 0;
   int device = 0, num_sms = 148;
+  bool use_inc = false;
+  int inc_max_rank = 0, inc_max_rows = 0, inc_max_len = 0;
   Phys phys{};
   // device buffers
-  void* rec = nullptr;
-  void* rec_dir_only = nullptr;
+  Chunk* rec = nullptr;
+  Chunk* rec_dir_only = nullptr;
   int *row_ptr = nullptr, *row_node = nullptr, *row_gpos = nullptr, *inc_ptr = nullptr, *inc_elem = nullptr;
   unsigned char* row_comp = nullptr;
   unsigned* inc_info = nullptr;
+  int *cta_row = nullptr, *cta_inc = nullptr, *inc_elem2 = nullptr;
+  unsigned* inc_word = nullptr;
+  unsigned short* inc_rowl = nullptr;
   double *dir = nullptr, *rhs = nullptr, *partials = nullptr, *dir_const = nullptr;
   unsigned* counter = nullptr;
   int n_partials = 0;
   int64_t device_bytes = 0;
-  // host staging for fne_eval_host (allocated on first use)
+  // device staging for fne_eval_host (allocated on first use)
   double *h_u = nullptr, *h_grad = nullptr, *h_energy = nullptr;
   void* h_hess = nullptr;
 };
@@ -653,66 +789,85 @@ int upload(fne_handle* h, T** p, const T* src, size_t count) {
 void free_handle(fne_handle* h) {
   if (!h) return;
   void* ptrs[] = {h->rec, h->rec_dir_only, h->row_ptr, h->row_node, h->row_gpos, h->inc_ptr, h->inc_elem,
-                  h->row_comp, h->inc_info, h->dir, h->rhs, h->partials, h->dir_const, h->counter,
-                  h->h_u, h->h_grad, h->h_energy, h->h_hess};
+                  h->row_comp, h->inc_info, h->cta_row, h->cta_inc, h->inc_elem2, h->inc_word, h->inc_rowl,
+                  h->dir, h->rhs, h->partials, h->dir_const, h->counter, h->h_u, h->h_grad, h->h_energy,
+                  h->h_hess};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
 }
 
-// pack element records on the host (reference float64 arrays -> Real records)
-template <typename Real>
-void pack_tri(const fne_desc* d, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
-              const std::vector<uint8_t>* weight, std::vector<typename TriRecT<Real>::T>& out) {
-  out.assign(elems.size(), {});
-  for (size_t i = 0; i < elems.size(); ++i) {
+// ---- packing of the reference's float64 arrays into chunk planes ----------
+inline void put_i(Chunk* R, size_t n, int plane, size_t e, int a, int b, int c, int d) {
+  int v[4] = {a, b, c, d};
+  std::memcpy(R[plane * n + e].w, v, 16);
+}
+inline void put_f(Chunk* R, size_t n, int plane, size_t e, float a, float b, float c, float d) {
+  float v[4] = {a, b, c, d};
+  std::memcpy(R[plane * n + e].w, v, 16);
+}
+inline void put_d(Chunk* R, size_t n, int plane, size_t e, double a, double b) {
+  double v[2] = {a, b};
+  std::memcpy(R[plane * n + e].w, v, 16);
+}
+inline double bits_as_double(int lo_word) {
+  int v[2] = {lo_word, 0};
+  double d;
+  std::memcpy(&d, v, 8);
+  return d;
+}
+
+void pack_tri(const fne_desc* d, bool f32, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
+              const std::vector<uint8_t>* weight, std::vector<Chunk>& out) {
+  const size_t n = elems.size();
+  out.assign(n * (f32 ? 3 : 5), Chunk{});
+  for (size_t i = 0; i < n; ++i) {
     const int64_t e = elems[i];
-    auto& r = out[i];
-    for (int b = 0; b < 3; ++b) {
-      r.src[b] = code[i * 3 + b];
-      r.dvx[b] = (Real)d->e0[e * 3 + b];
-      r.dvy[b] = (Real)d->e1[e * 3 + b];
+    const double* dx = d->e0 + e * 3;
+    const double* dy = d->e1 + e * 3;
+    const double vol = d->e2[e];
+    const int w = weight ? (*weight)[i] : 1;
+    put_i(out.data(), n, 0, i, code[i * 3], code[i * 3 + 1], code[i * 3 + 2], w);
+    if (f32) {
+      put_f(out.data(), n, 1, i, (float)dx[0], (float)dx[1], (float)dx[2], (float)vol);
+      put_f(out.data(), n, 2, i, (float)dy[0], (float)dy[1], (float)dy[2], 0.f);
+    } else {
+      put_d(out.data(), n, 1, i, vol, dx[0]);
+      put_d(out.data(), n, 2, i, dx[1], dx[2]);
+      put_d(out.data(), n, 3, i, dy[0], dy[1]);
+      put_d(out.data(), n, 4, i, dy[2], 0.0);
     }
-    r.vol = (Real)d->e2[e];
-    r.wflag = weight ? (*weight)[i] : 1;
   }
 }
 
-template <typename Real>
-void pack_tet(const fne_desc* d, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
-              const std::vector<uint8_t>* weight, std::vector<typename TetRecT<Real>::T>& out);
-template <>
-void pack_tet<float>(const fne_desc* d, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
-                     const std::vector<uint8_t>* weight, std::vector<TetRecF>& out) {
-  out.assign(elems.size(), {});
-  for (size_t i = 0; i < elems.size(); ++i) {
+void pack_tet(const fne_desc* d, bool f32, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
+              const std::vector<uint8_t>* weight, std::vector<Chunk>& out) {
+  const size_t n = elems.size();
+  out.assign(n * (f32 ? 5 : 8), Chunk{});
+  for (size_t i = 0; i < n; ++i) {
     const int64_t e = elems[i];
-    auto& r = out[i];
-    for (int b = 0; b < 4; ++b) {
-      r.src[b] = code[i * 4 + b];
-      r.gx[b] = (float)d->e0[e * 4 + b];
-      r.gy[b] = (float)d->e1[e * 4 + b];
-      r.gz[b] = (float)d->e2[e * 4 + b];
+    const double* gx = d->e0 + e * 4;
+    const double* gy = d->e1 + e * 4;
+    const double* gz = d->e2 + e * 4;
+    const double vol = d->e3[e];
+    const int w = weight ? (*weight)[i] : 1;
+    put_i(out.data(), n, 0, i, code[i * 4], code[i * 4 + 1], code[i * 4 + 2], code[i * 4 + 3]);
+    if (f32) {
+      float wf;
+      std::memcpy(&wf, &w, 4);
+      put_f(out.data(), n, 1, i, (float)gx[0], (float)gx[1], (float)gx[2], (float)gx[3]);
+      put_f(out.data(), n, 2, i, (float)gy[0], (float)gy[1], (float)gy[2], (float)gy[3]);
+      put_f(out.data(), n, 3, i, (float)gz[0], (float)gz[1], (float)gz[2], (float)gz[3]);
+      put_f(out.data(), n, 4, i, (float)vol, wf, 0.f, 0.f);
+    } else {
+      put_d(out.data(), n, 1, i, gx[0], gx[1]);
+      put_d(out.data(), n, 2, i, gx[2], gx[3]);
+      put_d(out.data(), n, 3, i, gy[0], gy[1]);
+      put_d(out.data(), n, 4, i, gy[2], gy[3]);
+      put_d(out.data(), n, 5, i, gz[0], gz[1]);
+      put_d(out.data(), n, 6, i, gz[2], gz[3]);
+      put_d(out.data(), n, 7, i, vol, bits_as_double(w));
     }
-    r.vol = (float)d->e3[e];
-    r.wflag = weight ? (*weight)[i] : 1;
-  }
-}
-template <>
-void pack_tet<double>(const fne_desc* d, const std::vector<int64_t>& elems, const std::vector<int32_t>& code,
-                      const std::vector<uint8_t>* weight, std::vector<TetRecD>& out) {
-  out.assign(elems.size(), {});
-  for (size_t i = 0; i < elems.size(); ++i) {
-    const int64_t e = elems[i];
-    auto& r = out[i];
-    for (int b = 0; b < 4; ++b) {
-      r.src[b] = code[i * 4 + b];
-      r.gx[b] = d->e0[e * 4 + b];
-      r.gy[b] = d->e1[e * 4 + b];
-      r.gz[b] = d->e2[e * 4 + b];
-    }
-    r.vol = d->e3[e];
-    r.wflag = weight ? (*weight)[i] : 1;
   }
 }
 
@@ -720,19 +875,24 @@ bool is_tri(int fam) { return fam == FNE_PLAPLACE || fam == FNE_GINZBURG_LANDAU;
 
 // ---- kernel dispatch -------------------------------------------------------
 template <typename Real, int FAM, typename HOut>
-cudaError_t launch_rows_tri_t(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
-                              cudaStream_t st, bool set_attr) {
-  using RecT = typename TriRecT<Real>::T;
-  const RecT* R = static_cast<const RecT*>(h->rec);
+cudaError_t launch_tri_t(fne_handle* h, int want, const RowArgs& A, const IncArgs& Q, double* grad, void* hess,
+                         EnergyOut eo, cudaStream_t st, bool set_attr) {
   HOut* H = static_cast<HOut*>(hess);
-  const dim3 grid(h->grid_rows), block(kTriRows);
-  const size_t sm = (want & W_H) ? h->smem_bytes : 0;
-#define FNE_TRI_CASE(W)                                                                              \
-  case W:                                                                                            \
-    if (set_attr)                                                                                    \
-      return cudaFuncSetAttribute(k_rows_tri<Real, FAM, W, HOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                  (int)h->smem_bytes);                                               \
-    k_rows_tri<Real, FAM, W, HOut><<<grid, block, sm, st>>>(A, R, h->phys, grad, H, eo);              \
+  const size_t sm = h->smem_bytes;
+  const dim3 grid(h->grid_rows);
+#define FNE_TRI_CASE(W)                                                                                        \
+  case W:                                                                                                      \
+    if (h->use_inc) {                                                                                          \
+      if (set_attr)                                                                                            \
+        return cudaFuncSetAttribute(k_inc_tri<Real, FAM, W, HOut>,                                            \
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                     \
+      k_inc_tri<Real, FAM, W, HOut><<<grid, kIncThreads, sm, st>>>(A, Q, h->rec, h->phys, grad, H, eo);        \
+    } else {                                                                                                   \
+      if (set_attr)                                                                                            \
+        return cudaFuncSetAttribute(k_rows_tri<Real, FAM, W, HOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                    (int)sm);                                                                  \
+      k_rows_tri<Real, FAM, W, HOut><<<grid, kTriRows, (W & W_H) ? sm : 0, st>>>(A, h->rec, h->phys, grad, H, eo); \
+    }                                                                                                          \
     return cudaGetLastError();
   switch (want) {
     FNE_TRI_CASE(2)
@@ -747,19 +907,17 @@ cudaError_t launch_rows_tri_t(fne_handle* h, int want, const RowArgs& A, double*
 }
 
 template <typename Real, typename HOut>
-cudaError_t launch_rows_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
-                              cudaStream_t st, bool set_attr) {
-  using RecT = typename TetRecT<Real>::T;
-  const RecT* R = static_cast<const RecT*>(h->rec);
+cudaError_t launch_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
+                         cudaStream_t st, bool set_attr) {
   HOut* H = static_cast<HOut*>(hess);
   const dim3 grid(h->grid_rows), block(kTetRows);
   const size_t sm = (want & W_H) ? h->smem_bytes : 0;
-#define FNE_TET_CASE(W)                                                                              \
-  case W:                                                                                            \
-    if (set_attr)                                                                                    \
-      return cudaFuncSetAttribute(k_rows_tet<Real, W, HOut>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                  (int)h->smem_bytes);                                               \
-    k_rows_tet<Real, W, HOut><<<grid, block, sm, st>>>(A, R, h->phys, grad, H, eo);                   \
+#define FNE_TET_CASE(W)                                                                                       \
+  case W:                                                                                                     \
+    if (set_attr)                                                                                             \
+      return cudaFuncSetAttribute(k_rows_tet<Real, W, HOut>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                  (int)h->smem_bytes);                                                        \
+    k_rows_tet<Real, W, HOut><<<grid, block, sm, st>>>(A, h->rec, h->phys, grad, H, eo);                       \
     return cudaGetLastError();
   switch (want) {
     FNE_TET_CASE(2)
@@ -773,29 +931,29 @@ cudaError_t launch_rows_tet_t(fne_handle* h, int want, const RowArgs& A, double*
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_rows(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
-                        cudaStream_t st, bool set_attr) {
+cudaError_t launch_rows(fne_handle* h, int want, const RowArgs& A, const IncArgs& Q, double* grad, void* hess,
+                        EnergyOut eo, cudaStream_t st, bool set_attr) {
   const bool f32 = h->precision == FNE_FP32;
   const bool h32 = f32 && h->hess_fp32;
   if (h->family == FNE_PLAPLACE) {
-    if (!f32) return launch_rows_tri_t<double, FAM_PLAP, double>(h, want, A, grad, hess, eo, st, set_attr);
-    if (h32) return launch_rows_tri_t<float, FAM_PLAP, float>(h, want, A, grad, hess, eo, st, set_attr);
-    return launch_rows_tri_t<float, FAM_PLAP, double>(h, want, A, grad, hess, eo, st, set_attr);
+    if (!f32) return launch_tri_t<double, FAM_PLAP, double>(h, want, A, Q, grad, hess, eo, st, set_attr);
+    if (h32) return launch_tri_t<float, FAM_PLAP, float>(h, want, A, Q, grad, hess, eo, st, set_attr);
+    return launch_tri_t<float, FAM_PLAP, double>(h, want, A, Q, grad, hess, eo, st, set_attr);
   }
   if (h->family == FNE_GINZBURG_LANDAU) {
-    if (!f32) return launch_rows_tri_t<double, FAM_GL, double>(h, want, A, grad, hess, eo, st, set_attr);
-    if (h32) return launch_rows_tri_t<float, FAM_GL, float>(h, want, A, grad, hess, eo, st, set_attr);
-    return launch_rows_tri_t<float, FAM_GL, double>(h, want, A, grad, hess, eo, st, set_attr);
+    if (!f32) return launch_tri_t<double, FAM_GL, double>(h, want, A, Q, grad, hess, eo, st, set_attr);
+    if (h32) return launch_tri_t<float, FAM_GL, float>(h, want, A, Q, grad, hess, eo, st, set_attr);
+    return launch_tri_t<float, FAM_GL, double>(h, want, A, Q, grad, hess, eo, st, set_attr);
   }
   if (h->family == FNE_NEOHOOKEAN) {
-    if (!f32) return launch_rows_tet_t<double, double>(h, want, A, grad, hess, eo, st, set_attr);
-    if (h32) return launch_rows_tet_t<float, float>(h, want, A, grad, hess, eo, st, set_attr);
-    return launch_rows_tet_t<float, double>(h, want, A, grad, hess, eo, st, set_attr);
+    if (!f32) return launch_tet_t<double, double>(h, want, A, grad, hess, eo, st, set_attr);
+    if (h32) return launch_tet_t<float, float>(h, want, A, grad, hess, eo, st, set_attr);
+    return launch_tet_t<float, double>(h, want, A, grad, hess, eo, st, set_attr);
   }
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_energy(fne_handle* h, const void* rec, int n_el, const double* u, const double* rhs, int n_owned,
+cudaError_t launch_energy(fne_handle* h, const Chunk* rec, int n_el, const double* u, const double* rhs, int n_owned,
                           EnergyOut eo, cudaStream_t st) {
   const bool f32 = h->precision == FNE_FP32;
   int grid = std::max(1, std::min(h->num_sms * 8, (std::max(n_el, n_owned) + kElemThreads - 1) / kElemThreads));
@@ -803,25 +961,23 @@ cudaError_t launch_energy(fne_handle* h, const void* rec, int n_el, const double
   const long long lo = h->lo;
   if (h->family == FNE_PLAPLACE) {
     if (f32)
-      k_energy_tri<float, FAM_PLAP><<<grid, kElemThreads, 0, st>>>((const TriRecF*)rec, n_el, u, h->dir, h->phys, rhs,
-                                                                   n_owned, lo, eo);
+      k_energy_tri<float, FAM_PLAP><<<grid, kElemThreads, 0, st>>>(rec, n_el, n_el, u, h->dir, h->phys, rhs, n_owned,
+                                                                   lo, eo);
     else
-      k_energy_tri<double, FAM_PLAP><<<grid, kElemThreads, 0, st>>>((const TriRecD*)rec, n_el, u, h->dir, h->phys,
-                                                                    rhs, n_owned, lo, eo);
+      k_energy_tri<double, FAM_PLAP><<<grid, kElemThreads, 0, st>>>(rec, n_el, n_el, u, h->dir, h->phys, rhs,
+                                                                    n_owned, lo, eo);
   } else if (h->family == FNE_GINZBURG_LANDAU) {
     if (f32)
-      k_energy_tri<float, FAM_GL><<<grid, kElemThreads, 0, st>>>((const TriRecF*)rec, n_el, u, h->dir, h->phys, rhs,
-                                                                 n_owned, lo, eo);
+      k_energy_tri<float, FAM_GL><<<grid, kElemThreads, 0, st>>>(rec, n_el, n_el, u, h->dir, h->phys, rhs, n_owned,
+                                                                 lo, eo);
     else
-      k_energy_tri<double, FAM_GL><<<grid, kElemThreads, 0, st>>>((const TriRecD*)rec, n_el, u, h->dir, h->phys, rhs,
-                                                                  n_owned, lo, eo);
+      k_energy_tri<double, FAM_GL><<<grid, kElemThreads, 0, st>>>(rec, n_el, n_el, u, h->dir, h->phys, rhs, n_owned,
+                                                                  lo, eo);
   } else if (h->family == FNE_NEOHOOKEAN) {
     if (f32)
-      k_energy_tet<float><<<grid, kElemThreads, 0, st>>>((const TetRecF*)rec, n_el, u, h->dir, h->phys, rhs, n_owned,
-                                                         lo, eo);
+      k_energy_tet<float><<<grid, kElemThreads, 0, st>>>(rec, n_el, n_el, u, h->dir, h->phys, rhs, n_owned, lo, eo);
     else
-      k_energy_tet<double><<<grid, kElemThreads, 0, st>>>((const TetRecD*)rec, n_el, u, h->dir, h->phys, rhs, n_owned,
-                                                          lo, eo);
+      k_energy_tet<double><<<grid, kElemThreads, 0, st>>>(rec, n_el, n_el, u, h->dir, h->phys, rhs, n_owned, lo, eo);
   } else {
     return cudaErrorInvalidValue;
   }
@@ -836,7 +992,8 @@ int refresh_dir_const(fne_handle* h) {
     e = cudaMemset(h->dir_const, 0, sizeof(double));
   } else {
     EnergyOut eo{h->partials, h->counter, h->dir_const, nullptr};
-    e = launch_energy(h, h->rec_dir_only, h->n_dir_only, h->dir /*unused for Dirichlet nodes*/, nullptr, 0, eo, 0);
+    // every node of these elements is a Dirichlet node: u is never read
+    e = launch_energy(h, h->rec_dir_only, h->n_dir_only, h->dir, nullptr, 0, eo, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
   }
   if (e != cudaSuccess) return cuda_fail(e, "Dirichlet-only energy");
@@ -878,12 +1035,20 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   RowPlan plan;
   int rc = build_row_plan(d, plan);
   if (rc) return rc;
+  const bool f32 = d->precision == FNE_FP32;
+  const size_t real_size = f32 ? sizeof(float) : sizeof(double);
+
+  // incidence-parallel plan for triangles (else the row-gather kernel)
+  IncPlan inc;
+  bool use_inc = false;
+  if (is_tri(d->family) && plan.n_rows > 0 && d->kernel_variant == 2)
+    use_inc = build_inc_plan(plan, kIncThreads, inc);
 
   auto* h = new (std::nothrow) fne_handle();
   if (!h) return set_error(FNE_ENOMEM, "fne_create: out of host memory");
   h->family = d->family;
   h->precision = d->precision;
-  h->hess_fp32 = d->precision == FNE_FP32 ? (d->hess_fp32 ? 1 : 0) : 0;
+  h->hess_fp32 = f32 ? (d->hess_fp32 ? 1 : 0) : 0;
   h->npe = d->npe;
   h->bs = d->block_size;
   h->n_total = d->n_total;
@@ -896,6 +1061,7 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   h->n_dir_only = (int)plan.dir_only.size();
   h->n_inc = (int64_t)plan.inc_elem.size();
   h->max_row_len = plan.max_row_len;
+  h->use_inc = use_inc;
   h->phys.p = d->s[0];
   h->phys.eps = d->s[0];
   for (int i = 0; i < 9; ++i) h->phys.ip[i] = d->s[1 + i];
@@ -906,21 +1072,26 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
 
-  const bool f32 = d->precision == FNE_FP32;
-  const size_t real_size = f32 ? sizeof(float) : sizeof(double);
-  h->rows_per_cta = is_tri(d->family) ? kTriRows : kTetRows;
-  h->grid_rows = (h->n_rows + h->rows_per_cta - 1) / h->rows_per_cta;
-  int64_t max_cta = 0;
-  for (int c = 0; c < h->grid_rows; ++c) {
-    const int a = c * h->rows_per_cta, b = std::min(h->n_rows, a + h->rows_per_cta);
-    max_cta = std::max<int64_t>(max_cta, plan.row_ptr[b] - plan.row_ptr[a]);
+  if (use_inc) {
+    h->grid_rows = inc.n_cta;
+    h->inc_max_rank = inc.max_rank;
+    h->inc_max_rows = std::max(1, inc.max_rows);
+    h->inc_max_len = inc.max_len;
+    h->smem_bytes = (size_t)h->inc_max_rows * (sizeof(int) + real_size) + (size_t)inc.max_len * real_size;
+  } else {
+    h->rows_per_cta = is_tri(d->family) ? kTriRows : kTetRows;
+    h->grid_rows = (h->n_rows + h->rows_per_cta - 1) / h->rows_per_cta;
+    int64_t max_cta = 0;
+    for (int c = 0; c < h->grid_rows; ++c) {
+      const int a = c * h->rows_per_cta, b = std::min(h->n_rows, a + h->rows_per_cta);
+      max_cta = std::max<int64_t>(max_cta, plan.row_ptr[b] - plan.row_ptr[a]);
+    }
+    h->smem_bytes = (size_t)max_cta * real_size;
   }
-  h->smem_bytes = (size_t)max_cta * real_size;
   if (h->smem_bytes > 227 * 1024) {
     free_handle(h);
     return set_error(FNE_EBOUNDS, "fne_create: a CTA's rows exceed shared memory");
   }
-  h->grid_elem = std::max(1, std::min(h->num_sms * 8, (h->n_local + kElemThreads - 1) / kElemThreads));
   h->n_partials = std::max({h->grid_rows, h->num_sms * 8, 1});
 
 #define FNE_TRY(x)      \
@@ -932,51 +1103,33 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     }                   \
   } while (0)
 
-  // element records
-  if (is_tri(d->family)) {
-    if (f32) {
-      std::vector<TriRecF> recs, dro;
-      pack_tri<float>(d, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
-      FNE_TRY(upload(h, (TriRecF**)&h->rec, recs.data(), recs.size()));
-      if (d->dirichlet_only_energy) {
-        pack_tri<float>(d, plan.dir_only, plan.dir_only_code, nullptr, dro);
-        FNE_TRY(upload(h, (TriRecF**)&h->rec_dir_only, dro.data(), dro.size()));
-      }
+  {
+    std::vector<Chunk> recs, dro;
+    if (is_tri(d->family)) {
+      pack_tri(d, f32, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
+      if (d->dirichlet_only_energy) pack_tri(d, f32, plan.dir_only, plan.dir_only_code, nullptr, dro);
     } else {
-      std::vector<TriRecD> recs, dro;
-      pack_tri<double>(d, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
-      FNE_TRY(upload(h, (TriRecD**)&h->rec, recs.data(), recs.size()));
-      if (d->dirichlet_only_energy) {
-        pack_tri<double>(d, plan.dir_only, plan.dir_only_code, nullptr, dro);
-        FNE_TRY(upload(h, (TriRecD**)&h->rec_dir_only, dro.data(), dro.size()));
-      }
+      pack_tet(d, f32, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
+      if (d->dirichlet_only_energy) pack_tet(d, f32, plan.dir_only, plan.dir_only_code, nullptr, dro);
     }
-  } else {
-    if (f32) {
-      std::vector<TetRecF> recs, dro;
-      pack_tet<float>(d, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
-      FNE_TRY(upload(h, (TetRecF**)&h->rec, recs.data(), recs.size()));
-      if (d->dirichlet_only_energy) {
-        pack_tet<float>(d, plan.dir_only, plan.dir_only_code, nullptr, dro);
-        FNE_TRY(upload(h, (TetRecF**)&h->rec_dir_only, dro.data(), dro.size()));
-      }
-    } else {
-      std::vector<TetRecD> recs, dro;
-      pack_tet<double>(d, plan.local_elems, plan.elem_code, &plan.elem_weight, recs);
-      FNE_TRY(upload(h, (TetRecD**)&h->rec, recs.data(), recs.size()));
-      if (d->dirichlet_only_energy) {
-        pack_tet<double>(d, plan.dir_only, plan.dir_only_code, nullptr, dro);
-        FNE_TRY(upload(h, (TetRecD**)&h->rec_dir_only, dro.data(), dro.size()));
-      }
-    }
+    FNE_TRY(upload(h, &h->rec, recs.data(), recs.size()));
+    FNE_TRY(upload(h, &h->rec_dir_only, dro.data(), dro.size()));
   }
   FNE_TRY(upload(h, &h->row_ptr, plan.row_ptr.data(), plan.row_ptr.size()));
   FNE_TRY(upload(h, &h->row_node, plan.row_node.data(), plan.row_node.size()));
   FNE_TRY(upload(h, &h->row_comp, plan.row_comp.data(), plan.row_comp.size()));
   FNE_TRY(upload(h, &h->row_gpos, plan.row_gpos.data(), plan.row_gpos.size()));
   FNE_TRY(upload(h, &h->inc_ptr, plan.inc_ptr.data(), plan.inc_ptr.size()));
-  FNE_TRY(upload(h, &h->inc_elem, plan.inc_elem.data(), plan.inc_elem.size()));
-  FNE_TRY(upload(h, &h->inc_info, plan.inc_info.data(), plan.inc_info.size()));
+  if (use_inc) {
+    FNE_TRY(upload(h, &h->cta_row, inc.cta_row.data(), inc.cta_row.size()));
+    FNE_TRY(upload(h, &h->cta_inc, inc.cta_inc.data(), inc.cta_inc.size()));
+    FNE_TRY(upload(h, &h->inc_elem2, inc.inc_elem.data(), inc.inc_elem.size()));
+    FNE_TRY(upload(h, &h->inc_word, inc.inc_word.data(), inc.inc_word.size()));
+    FNE_TRY(upload(h, &h->inc_rowl, inc.inc_rowl.data(), inc.inc_rowl.size()));
+  } else {
+    FNE_TRY(upload(h, &h->inc_elem, plan.inc_elem.data(), plan.inc_elem.size()));
+    FNE_TRY(upload(h, &h->inc_info, plan.inc_info.data(), plan.inc_info.size()));
+  }
   FNE_TRY(upload(h, &h->dir, d->dirichlet, (size_t)d->n_total));
   if (d->rhs_owned) FNE_TRY(upload(h, &h->rhs, d->rhs_owned, (size_t)(d->hi - d->lo)));
   FNE_TRY(dalloc(h, &h->partials, (size_t)h->n_partials));
@@ -992,11 +1145,11 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     FNE_TRY(dalloc(h, &h->dir_const, 1));
     FNE_TRY(refresh_dir_const(h));
   }
-  // opt in to large dynamic shared memory for every row-kernel variant
   if (h->smem_bytes > 48 * 1024) {
-    RowArgs dummy{};
+    RowArgs ra{};
+    IncArgs pa{};
     for (int want = 2; want <= 7; ++want) {
-      cudaError_t e = launch_rows(h, want, dummy, nullptr, nullptr, EnergyOut{}, 0, true);
+      cudaError_t e = launch_rows(h, want, ra, pa, nullptr, nullptr, EnergyOut{}, 0, true);
       if (e != cudaSuccess) {
         free_handle(h);
         return cuda_fail(e, "cudaFuncSetAttribute");
@@ -1016,7 +1169,7 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   info->n_incidences = h->n_inc;
   info->device_bytes = h->device_bytes;
   info->max_row_len = h->max_row_len;
-  info->kernel_variant = is_tri(h->family) ? 1 : 2;
+  info->kernel_variant = is_tri(h->family) ? (h->use_inc ? 3 : 1) : 2;
   return FNE_OK;
 }
 
@@ -1056,7 +1209,10 @@ extern "C" int fne_eval(fne_handle* h, const double* u, int flags, double* energ
     A.dir = h->dir;
     A.rhs = h->rhs;
     A.lo = h->lo;
-    e = launch_rows(h, flags, A, grad, hess, eo, st, false);
+    A.nrec = h->n_local;
+    IncArgs Q{h->cta_row, h->cta_inc, h->inc_elem2, h->inc_word, h->inc_rowl, h->inc_max_rank, h->inc_max_rows,
+              h->inc_max_len};
+    e = launch_rows(h, flags, A, Q, grad, hess, eo, st, false);
   }
   if (e != cudaSuccess) return cuda_fail(e, "fne_eval launch");
   return FNE_OK;
@@ -1074,7 +1230,8 @@ extern "C" int fne_eval_host(fne_handle* h, const double* u_host, int flags, dou
     if (!rc) rc = dalloc(h, (unsigned char**)&h->h_hess, std::max<size_t>(1, (size_t)h->nnz * hsz));
     if (rc) return rc;
   }
-  cudaError_t e = cudaMemcpy(h->h_u, u_host, h->n_free * sizeof(double), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaSuccess;
+  if (h->n_free) e = cudaMemcpy(h->h_u, u_host, h->n_free * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "fne_eval_host H2D");
   int rc = fne_eval(h, h->h_u, flags, h->h_energy, h->h_grad, h->h_hess, nullptr);
   if (rc) return rc;
@@ -1095,4 +1252,4 @@ extern "C" int fne_destroy(fne_handle* h) {
 }
 
 extern "C" const char* fne_last_error(void) { return g_err.c_str(); }
-extern "C" const char* fne_version(void) { return "fne_asm 0.1 (sm_100a)"; }
+extern "C" const char* fne_version(void) { return "fne_asm 0.2 (sm_100a)"; }

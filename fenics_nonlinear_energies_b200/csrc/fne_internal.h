@@ -52,6 +52,28 @@ struct RowPlan {
 // its block_size DOFs free).  Returns FNE_OK or an error (set_error called).
 int build_row_plan(const fne_desc* d, RowPlan& P);
 
+// Incidence-parallel plan (scalar P1 triangles): one thread per
+// (row, element) incidence.  CTA c owns rows [cta_row[c], cta_row[c+1]) and
+// their incidences [cta_inc[c], cta_inc[c+1]) (at most `threads` of them).
+// inc_word: bits 0-1 local node a, bit 2 energy flag, bits 3-6 rank of the
+// incidence within its row, then 7-bit column offsets of element nodes 0..2
+// (127 = Dirichlet column).  inc_rowl: row index within the CTA.
+struct IncPlan {
+  int32_t n_cta = 0;
+  int32_t max_rank = 0;       // largest rank (incidences per row - 1)
+  int32_t max_rows = 0;       // most rows of one CTA
+  int32_t max_len = 0;        // largest output slice of one CTA
+  std::vector<int32_t> cta_row, cta_inc;
+  std::vector<int32_t> inc_elem;
+  std::vector<uint32_t> inc_word;
+  std::vector<uint16_t> inc_rowl;
+};
+
+// Sorts P's local elements by the first row that needs them (locality),
+// permuting the element arrays and P.inc_elem, and builds Q.  Returns false
+// when the mesh does not fit the packed format.
+bool build_inc_plan(RowPlan& P, int threads, IncPlan& Q);
+
 // Gather code of one element node: >= 0 reordered id of component 0 (free
 // node); < 0: -1 - total DOF of component 0 (Dirichlet node).
 }  // namespace fne

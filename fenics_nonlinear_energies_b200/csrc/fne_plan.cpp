@@ -225,3 +225,82 @@ int build_row_plan(const fne_desc* d, RowPlan& P) {
 }
 
 }  // namespace fne
+
+namespace fne {
+
+bool build_inc_plan(RowPlan& P, int threads, IncPlan& Q) {
+  const int32_t n_local = (int32_t)P.local_elems.size();
+  const int npe = n_local ? (int)(P.elem_code.size() / n_local) : 3;
+  if (npe != 3) return false;
+  const int32_t n_rows = P.n_rows;
+  // locality: sort elements by the first row (output order) that needs them
+  std::vector<int32_t> first(n_local, INT32_MAX);
+  for (int32_t k = 0; k < n_rows; ++k) {
+    const int32_t nd = P.row_node[k];
+    for (int32_t i = P.inc_ptr[nd]; i < P.inc_ptr[nd + 1]; ++i)
+      first[P.inc_elem[i]] = std::min(first[P.inc_elem[i]], k);
+  }
+  std::vector<int32_t> order(n_local);
+  for (int32_t i = 0; i < n_local; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return first[a] < first[b]; });
+  std::vector<int32_t> newidx(n_local);
+  for (int32_t i = 0; i < n_local; ++i) newidx[order[i]] = i;
+  {
+    std::vector<int64_t> le(n_local);
+    std::vector<int32_t> code(P.elem_code.size());
+    std::vector<uint8_t> w(n_local);
+    for (int32_t i = 0; i < n_local; ++i) {
+      le[i] = P.local_elems[order[i]];
+      w[i] = P.elem_weight[order[i]];
+      for (int a = 0; a < npe; ++a) code[(size_t)i * npe + a] = P.elem_code[(size_t)order[i] * npe + a];
+    }
+    P.local_elems.swap(le);
+    P.elem_code.swap(code);
+    P.elem_weight.swap(w);
+    for (auto& e : P.inc_elem) e = newidx[e];
+  }
+  // CTAs: greedy runs of whole rows with at most `threads` incidences
+  Q.cta_row.assign(1, 0);
+  Q.cta_inc.assign(1, 0);
+  Q.inc_elem.clear();
+  Q.inc_word.clear();
+  Q.inc_rowl.clear();
+  Q.max_rank = 0;
+  Q.max_rows = 0;
+  Q.max_len = 0;
+  int32_t cnt = 0, rows_in = 0, row0 = 0;
+  for (int32_t k = 0; k < n_rows; ++k) {
+    const int32_t nd = P.row_node[k];
+    const int32_t m = P.inc_ptr[nd + 1] - P.inc_ptr[nd];
+    if (m > threads || m > 16) return false;
+    if (cnt + m > threads || rows_in == 65535) {
+      Q.cta_row.push_back(k);
+      Q.cta_inc.push_back((int32_t)Q.inc_elem.size());
+      Q.max_rows = std::max(Q.max_rows, rows_in);
+      Q.max_len = std::max(Q.max_len, P.row_ptr[k] - P.row_ptr[row0]);
+      cnt = 0;
+      rows_in = 0;
+      row0 = k;
+    }
+    for (int32_t j = 0; j < m; ++j) {
+      const int32_t i = P.inc_ptr[nd] + j;
+      const uint32_t info = P.inc_info[i];
+      uint32_t w = (info & 3u) | ((info & kEnergyFlag) ? 4u : 0u) | ((uint32_t)j << 3);
+      w |= ((info >> kOffShift) & ((1u << (3 * kOffBits)) - 1u)) << 7;
+      Q.inc_elem.push_back(P.inc_elem[i]);
+      Q.inc_word.push_back(w);
+      Q.inc_rowl.push_back((uint16_t)rows_in);
+    }
+    Q.max_rank = std::max(Q.max_rank, m - 1);
+    cnt += m;
+    ++rows_in;
+  }
+  Q.cta_row.push_back(n_rows);
+  Q.cta_inc.push_back((int32_t)Q.inc_elem.size());
+  Q.max_rows = std::max(Q.max_rows, rows_in);
+  Q.max_len = std::max(Q.max_len, P.row_ptr[n_rows] - P.row_ptr[row0]);
+  Q.n_cta = (int32_t)Q.cta_row.size() - 1;
+  return true;
+}
+
+}  // namespace fne

@@ -141,6 +141,7 @@ typedef struct {
                                  * free DOF (Ginzburg-Landau assembler,
                                  * src/problems/ginzburg_landau/jax_petsc/
                                  * reordered_element_assembler.py:34-52, 96-97) */
+  int32_t kernel_variant;       /* 0 = automatic; 1 = row-gather; 2 = incidence-parallel */
 } fne_desc;
 
 typedef struct fne_handle fne_handle;

@@ -67,10 +67,11 @@ def _abs_energy_scale(ref, u):
     return float(np.abs(e).sum() + np.abs(ref.f_owned @ np.asarray(u)[: ref.f_owned.size]) + 1e-300)
 
 
+@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence"])
 @pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
-def test_plaplace_fp64(numbering):
-    params, _ = meshes.plaplace_problem(n=12, numbering=numbering)
-    gpu, ref = _make("plaplace", params)
+def test_plaplace_fp64(numbering, variant):
+    params, _ = meshes.plaplace_problem(n=40, numbering=numbering)
+    gpu, ref = _make("plaplace", params, kernel_variant=variant)
     u = np.random.default_rng(0).random(gpu.layout.n_free)
     _check(gpu, ref, u, FP64_TOL, energy_scale=_abs_energy_scale(ref, u))
 
@@ -83,16 +84,18 @@ def test_plaplace_zero_initial_guess():
     assert torch.all(gpu.owned_values == 0)
 
 
+@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence"])
 @pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
-def test_gl_fp64(numbering):
+def test_gl_fp64(numbering, variant):
     params, u0 = meshes.gl_problem(n=16, seed=3, numbering=numbering)
-    gpu, ref = _make("gl", params)
+    gpu, ref = _make("gl", params, kernel_variant=variant)
     _check(gpu, ref, u0, FP64_TOL, energy_scale=_abs_energy_scale(ref, u0))
 
 
-def test_gl_fp32():
-    params, u0 = meshes.gl_problem(n=16, seed=4)
-    gpu, ref = _make("gl", params, precision="fp32", hess_dtype=torch.float32)
+@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence"])
+def test_gl_fp32(variant):
+    params, u0 = meshes.gl_problem(n=40, seed=4)
+    gpu, ref = _make("gl", params, precision="fp32", hess_dtype=torch.float32, kernel_variant=variant)
     e_ref, g_ref, h_ref = ref.all_in_one(u0)
     e, g, h = gpu.eval(torch.as_tensor(u0, device="cuda"), 7)
     assert h.dtype == torch.float32
