@@ -290,7 +290,9 @@ def run(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": f"{peak_kind} burst copy",
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": "k_rows_tri<float, GL, E|G|H, float>"},
+                         "kernel": {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri",
+                                    4: "k_sweep_tri"}.get(asm.info["kernel_variant"], "?")
+                                   + "<float, GL, E|G|H, float>"},
             "e2e": {"value": e2e_value, "unit": "elements/s",
                     "h2d_bytes_per_step": int(u0.nbytes),
                     "d2h_bytes_per_step": int(8 + host_g.numel() * 8 + host_h.numel() * 4)},

@@ -49,7 +49,22 @@ struct Phys {
   double w[3];    // GL quadrature weights
   double C1, D1;  // Neo-Hookean
   int absdet;
+  int p_is3;      // p == 3 (sqrt fast path)
+  // float copies: FP32 kernels never convert parameters per element
+  float pf, epsf, ipf[9], wf[3], C1f, D1f;
 };
+
+// parameter in the kernel's arithmetic type, without a per-use conversion
+template <typename Real>
+__device__ __forceinline__ Real prm(double d, float f);
+template <>
+__device__ __forceinline__ float prm<float>(double, float f) {
+  return f;
+}
+template <>
+__device__ __forceinline__ double prm<double>(double d, float) {
+  return d;
+}
 
 // Element records are stored as "chunk planes": plane k of an element record
 // is the 16-byte chunk  base[k * n + e], so a warp loading plane k of 32
@@ -144,6 +159,7 @@ __device__ __forceinline__ double gather(const double* __restrict__ u, const dou
   return code >= 0 ? __ldg(u + code + c) : __ldg(dir + (-1 - code) + c);
 }
 
+
 // ---------------------------------------------------------------------------
 // physics: p-Laplace, Ginzburg-Landau (P1 triangles, scalar)
 // ---------------------------------------------------------------------------
@@ -167,10 +183,10 @@ __device__ __forceinline__ void tri_row(const Phys& P, int a, const Real v[3], c
   const Real dya = a == 0 ? t.dvy[0] : (a == 1 ? t.dvy[1] : t.dvy[2]);
   if (FAM == FAM_PLAP) {
     const Real s = fx * fx + fy * fy;
-    const Real p = (Real)P.p;
+    const Real p = prm<Real>(P.p, P.pf);
     Real t1, t2;
     if (s > Real(0)) {
-      if (P.p == 3.0) {
+      if (P.p_is3) {
         t1 = sqrt(s);
         t2 = Real(1) / t1;
       } else {
@@ -187,20 +203,20 @@ __device__ __forceinline__ void tri_row(const Phys& P, int a, const Real v[3], c
     for (int b = 0; b < 3; ++b)
       h[b] = t.vol * (t1 * (dxa * t.dvx[b] + dya * t.dvy[b]) + t2 * Ga * (fx * t.dvx[b] + fy * t.dvy[b]));
   } else {
-    const Real eps = (Real)P.eps;
+    const Real eps = prm<Real>(P.eps, P.epsf);
     Real ipa[3], n[3], c1[3], c2[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      n[q] = v[0] * (Real)P.ip[q] + v[1] * (Real)P.ip[3 + q] + v[2] * (Real)P.ip[6 + q];
-      ipa[q] = (Real)(a == 0 ? P.ip[q] : (a == 1 ? P.ip[3 + q] : P.ip[6 + q]));
-      c1[q] = (Real)P.w[q] * (n[q] * n[q] - Real(1)) * n[q];
-      c2[q] = (Real)P.w[q] * (Real(3) * n[q] * n[q] - Real(1)) * ipa[q];
+      n[q] = v[0] * prm<Real>(P.ip[q], P.ipf[q]) + v[1] * prm<Real>(P.ip[3 + q], P.ipf[3 + q]) + v[2] * prm<Real>(P.ip[6 + q], P.ipf[6 + q]);
+      ipa[q] = a == 0 ? prm<Real>(P.ip[q], P.ipf[q]) : (a == 1 ? prm<Real>(P.ip[3 + q], P.ipf[3 + q]) : prm<Real>(P.ip[6 + q], P.ipf[6 + q]));
+      c1[q] = prm<Real>(P.w[q], P.wf[q]) * (n[q] * n[q] - Real(1)) * n[q];
+      c2[q] = prm<Real>(P.w[q], P.wf[q]) * (Real(3) * n[q] * n[q] - Real(1)) * ipa[q];
     }
     ga = t.vol * (eps * (fx * dxa + fy * dya) + c1[0] * ipa[0] + c1[1] * ipa[1] + c1[2] * ipa[2]);
 #pragma unroll
     for (int b = 0; b < 3; ++b)
-      h[b] = t.vol * (eps * (dxa * t.dvx[b] + dya * t.dvy[b]) + c2[0] * (Real)P.ip[3 * b] +
-                      c2[1] * (Real)P.ip[3 * b + 1] + c2[2] * (Real)P.ip[3 * b + 2]);
+      h[b] = t.vol * (eps * (dxa * t.dvx[b] + dya * t.dvy[b]) + c2[0] * prm<Real>(P.ip[3 * b], P.ipf[3 * b]) +
+                      c2[1] * prm<Real>(P.ip[3 * b + 1], P.ipf[3 * b + 1]) + c2[2] * prm<Real>(P.ip[3 * b + 2], P.ipf[3 * b + 2]));
   }
 }
 
@@ -244,10 +260,10 @@ __device__ __forceinline__ void tri_full(const Phys& P, const Real v[3], const T
   K[5] = t.dvx[2] * t.dvx[2] + t.dvy[2] * t.dvy[2];
   if (FAM == FAM_PLAP) {
     const Real s = fx * fx + fy * fy;
-    const Real p = (Real)P.p;
+    const Real p = prm<Real>(P.p, P.pf);
     Real t1, t2;
     if (s > Real(0)) {
-      if (P.p == 3.0) {
+      if (P.p_is3) {
         t1 = sqrt(s);
         t2 = Real(1) / t1;
       } else {
@@ -268,16 +284,16 @@ __device__ __forceinline__ void tri_full(const Phys& P, const Real v[3], const T
     H[4] = vt1 * K[4] + vt2 * G[1] * G[2];
     H[5] = vt1 * K[5] + vt2 * G[2] * G[2];
   } else {
-    const Real eps = (Real)P.eps;
+    const Real eps = prm<Real>(P.eps, P.epsf);
     Real ip[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) ip[k] = (Real)P.ip[k];
+    for (int k = 0; k < 9; ++k) ip[k] = prm<Real>(P.ip[k], P.ipf[k]);
     Real c1[3], c2[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const Real n = v[0] * ip[q] + v[1] * ip[3 + q] + v[2] * ip[6 + q];
-      c1[q] = (Real)P.w[q] * (n * n - Real(1)) * n;
-      c2[q] = (Real)P.w[q] * (Real(3) * n * n - Real(1));
+      c1[q] = prm<Real>(P.w[q], P.wf[q]) * (n * n - Real(1)) * n;
+      c2[q] = prm<Real>(P.w[q], P.wf[q]) * (Real(3) * n * n - Real(1));
     }
 #pragma unroll
     for (int b = 0; b < 3; ++b)
@@ -289,6 +305,29 @@ __device__ __forceinline__ void tri_full(const Phys& P, const Real v[3], const T
       for (int b = a; b < 3; ++b, ++m)
         H[m] = t.vol * (eps * K[m] + c2[0] * ip[3 * a] * ip[3 * b] + c2[1] * ip[3 * a + 1] * ip[3 * b + 1] +
                         c2[2] * ip[3 * a + 2] * ip[3 * b + 2]);
+  }
+}
+
+// Element energy in the kernel's arithmetic type (FP32 mode: FP32 element
+// energies, reduced in FP64 by the caller).
+template <typename Real, int FAM>
+__device__ __forceinline__ double tri_energy_r(const Phys& P, const Real v[3], const TriElem<Real>& t) {
+  const Real fx = v[0] * t.dvx[0] + v[1] * t.dvx[1] + v[2] * t.dvx[2];
+  const Real fy = v[0] * t.dvy[0] + v[1] * t.dvy[1] + v[2] * t.dvy[2];
+  const Real s = fx * fx + fy * fy;
+  if (FAM == FAM_PLAP) {
+    const Real ps = P.p_is3 ? s * sqrt(s) : pow(s, Real(0.5) * prm<Real>(P.p, P.pf));
+    return (double)(ps * t.vol / prm<Real>(P.p, P.pf));
+  } else {
+    Real pot = Real(0);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const Real n = v[0] * prm<Real>(P.ip[q], P.ipf[q]) + v[1] * prm<Real>(P.ip[3 + q], P.ipf[3 + q]) +
+                     v[2] * prm<Real>(P.ip[6 + q], P.ipf[6 + q]);
+      const Real m = n * n - Real(1);
+      pot += m * m * prm<Real>(P.w[q], P.wf[q]);
+    }
+    return (double)((Real(0.5) * prm<Real>(P.eps, P.epsf) * s + Real(0.25) * pot) * t.vol);
   }
 }
 
@@ -325,7 +364,7 @@ __device__ __forceinline__ void he_state(const Phys& P, const Real y[4][3], cons
   S.cof[2][1] = F[0][2] * F[1][0] - F[0][0] * F[1][2];
   S.cof[2][2] = F[0][0] * F[1][1] - F[0][1] * F[1][0];
   S.J = F[0][0] * S.cof[0][0] + F[0][1] * S.cof[0][1] + F[0][2] * S.cof[0][2];
-  const Real C1 = (Real)P.C1, D1 = (Real)P.D1;
+  const Real C1 = prm<Real>(P.C1, P.C1f), D1 = prm<Real>(P.D1, P.D1f);
   const Real sg = P.absdet ? (S.J > Real(0) ? Real(1) : (S.J < Real(0) ? Real(-1) : Real(0))) : Real(1);
   const Real iJ = Real(1) / S.J;
   S.c2 = Real(2) * C1 * iJ * iJ + Real(2) * D1;
@@ -340,7 +379,7 @@ __device__ __forceinline__ void he_row(const Phys& P, int a, int c, const HeStat
 #pragma unroll
   for (int j = 0; j < 3; ++j)
     ga[j] = a == 0 ? t.g[0][j] : (a == 1 ? t.g[1][j] : (a == 2 ? t.g[2][j] : t.g[3][j]));
-  const Real C1 = (Real)P.C1;
+  const Real C1 = prm<Real>(P.C1, P.C1f);
   const Real Fc0 = c == 0 ? S.F[0][0] : (c == 1 ? S.F[1][0] : S.F[2][0]);
   const Real Fc1 = c == 0 ? S.F[0][1] : (c == 1 ? S.F[1][1] : S.F[2][1]);
   const Real Fc2 = c == 0 ? S.F[0][2] : (c == 1 ? S.F[1][2] : S.F[2][2]);
@@ -680,6 +719,227 @@ __global__ void __launch_bounds__(kIncThreads, 2) k_inc_tri(RowArgs A, IncArgs Q
 }
 
 // ---------------------------------------------------------------------------
+// Banded-sweep kernel (P1 triangles): CTA s owns the row segment
+// [seg_row[s], seg_row[s+1]) and sweeps the elements that feed it in order of
+// their first row, in batches of NB: every element is evaluated once (plus the
+// few "pre" elements shared with the previous segment), the records are read
+// with coalesced 16-byte loads and the next batch's records are in flight
+// while the current batch is reduced.  Row sums live in a shared-memory ring
+// window over the COO positions; after each batch the rows that no later
+// element can touch are streamed out (contiguous, coalesced) and their window
+// slots cleared.  Each row entry of a batch is summed by one thread in a
+// fixed order: no atomics, bit-reproducible.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int sym_index(int a, int b) {  // upper-triangle slot of (a, b)
+  const int lo = min(a, b), hi = max(a, b);
+  return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
+}
+
+struct SweepArgs {
+  const int* __restrict__ seg_row;
+  const int* __restrict__ seg_elem;
+  const int* __restrict__ seg_batch;
+  const int* __restrict__ batch_done;
+  const int* __restrict__ ent_ptr;
+  const int* __restrict__ inc_base;
+  const int* __restrict__ ent_row;
+  const int* __restrict__ ent_pos;
+  const unsigned* __restrict__ ent_meta;
+  const unsigned* __restrict__ inc_word;
+  int win_mask;
+  int rwin_mask;
+  int gpos_identity;
+};
+
+// Per-thread prefetch state of one batch: the element it evaluates and the
+// row entry it reduces (first kPfWords incidence words in registers).
+constexpr int kPfWords = 4;
+template <typename Real>
+struct SweepPf {
+  TriElem<Real> t;
+  Real v[3];
+  int row, pos;
+  unsigned meta;
+  unsigned w[kPfWords];
+  bool elem_ok, ent_ok;
+};
+
+// level-1 loads of batch b: element record and row-entry header
+template <typename Real>
+__device__ __forceinline__ void sweep_load1(const SweepArgs& S, const Chunk* __restrict__ R, int nrec, int e,
+                                            bool elem_ok, int ent, bool ent_ok, SweepPf<Real>& f) {
+  f.elem_ok = elem_ok;
+  f.ent_ok = ent_ok;
+  if (elem_ok) load_tri(R, nrec, e, f.t);
+  if (ent_ok) {
+    f.row = __ldg(S.ent_row + ent);
+    f.pos = __ldg(S.ent_pos + ent);
+    f.meta = __ldg(S.ent_meta + ent);
+  }
+}
+// level-2 loads of batch b: nodal values and incidence words
+template <typename Real>
+__device__ __forceinline__ void sweep_load2(const SweepArgs& S, const double* __restrict__ u,
+                                            const double* __restrict__ dir, int ibase, SweepPf<Real>& f) {
+  if (f.elem_ok) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f.v[k] = (Real)gather(u, dir, f.t.src[k], 0);
+  }
+  if (f.ent_ok) {
+    const unsigned* __restrict__ iw = S.inc_word + ibase + (f.meta & 0xffffu);
+    const int cnt = f.meta >> 16;
+#pragma unroll
+    for (int k = 0; k < kPfWords; ++k) f.w[k] = k < cnt ? __ldg(iw + k) : 0u;
+  }
+}
+
+template <typename Real, int WANT, int NB>
+__device__ __forceinline__ void sweep_reduce_word(unsigned w, int pos0, const Real* sH, const Real* sG, Real* swin,
+                                                  int win_mask, Real& gs) {
+  const int j = w & 511u;
+  const int a = (w >> 9) & 3u;
+  if (WANT & W_G) gs += sG[a * NB + j];
+  if (WANT & W_H) {
+    const Real* hrow = sH + 3 * a * NB + j;  // row a of the element Hessian
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb) {
+      const unsigned off = (w >> (11 + kOffBits * bb)) & 127u;
+      if (off != kNoCol) swin[(pos0 + (int)off) & win_mask] += hrow[bb * NB];
+    }
+  }
+}
+
+template <typename Real, int FAM, int WANT, typename HOut, int NB>
+__global__ void __launch_bounds__(NB, 2) k_sweep_tri(RowArgs A, SweepArgs S, const Chunk* __restrict__ R, Phys P,
+                                                     double* __restrict__ grad, HOut* __restrict__ hess,
+                                                     EnergyOut eo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* sH = reinterpret_cast<Real*>(smem_raw);  // [9][NB] element Hessians, row-major 3x3
+  Real* sG = sH + 9 * NB;                         // [3][NB]
+  Real* swin = sG + 3 * NB;                       // [win_mask + 1]
+  Real* sgw = swin + (S.win_mask + 1);            // [rwin_mask + 1]
+  const int seg = blockIdx.x;
+  const int R0 = S.seg_row[seg], R1 = S.seg_row[seg + 1];
+  const int p_lo = S.seg_elem[3 * seg], o_lo = S.seg_elem[3 * seg + 1], o_hi = S.seg_elem[3 * seg + 2];
+  const int b0 = S.seg_batch[seg], b1 = S.seg_batch[seg + 1];
+  if (WANT & W_H)
+    for (int j = threadIdx.x; j <= S.win_mask; j += NB) swin[j] = Real(0);
+  if (WANT & W_G)
+    for (int j = threadIdx.x; j <= S.rwin_mask; j += NB) sgw[j] = Real(0);
+  double eacc = 0.0;
+  int done = R0;
+  int p_done = A.row_ptr[R0];
+  // batch b0 (prologue)
+  SweepPf<Real> cur, nxt;
+  int c_eb = 0, c_ee = 0, c_ib = 0, c_bd = R0, c_p1 = p_done;
+  if (b0 < b1) {
+    c_eb = S.ent_ptr[b0];
+    c_ee = S.ent_ptr[b0 + 1];
+    c_ib = S.inc_base[b0];
+    c_bd = S.batch_done[b0];
+    c_p1 = A.row_ptr[c_bd];
+    const int e = p_lo + threadIdx.x;
+    sweep_load1(S, R, A.nrec, e, e < o_hi, c_eb + threadIdx.x, c_eb + (int)threadIdx.x < c_ee, cur);
+    sweep_load2(S, A.u, A.dir, c_ib, cur);
+  }
+  for (int b = b0; b < b1; ++b) {
+    const int e = p_lo + (b - b0) * NB + threadIdx.x;
+    // (1) level-1 loads of batch b+1 while batch b is processed
+    const bool has_next = b + 1 < b1;
+    int n_eb = 0, n_ee = 0, n_ib = 0, n_bd = c_bd, n_p1 = c_p1;
+    if (has_next) {
+      n_eb = S.ent_ptr[b + 1];
+      n_ee = S.ent_ptr[b + 2];
+      n_ib = S.inc_base[b + 1];
+      n_bd = S.batch_done[b + 1];
+    }
+    sweep_load1(S, R, A.nrec, e + NB, has_next && e + NB < o_hi, n_eb + threadIdx.x,
+                has_next && n_eb + (int)threadIdx.x < n_ee, nxt);
+    // (2) phase A: element gradient / Hessian of batch b into shared memory
+    if (cur.elem_ok) {
+      Real g[3], H[6];
+      tri_full<Real, FAM>(P, cur.v, cur.t, g, H);
+      if (WANT & W_H) {
+        Real* hs = sH + threadIdx.x;
+        hs[0 * NB] = H[0]; hs[1 * NB] = H[1]; hs[2 * NB] = H[2];
+        hs[3 * NB] = H[1]; hs[4 * NB] = H[3]; hs[5 * NB] = H[4];
+        hs[6 * NB] = H[2]; hs[7 * NB] = H[4]; hs[8 * NB] = H[5];
+      }
+      if (WANT & W_G) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) sG[k * NB + threadIdx.x] = g[k];
+      }
+      if ((WANT & W_E) && e >= o_lo && cur.t.wflag) eacc += tri_energy_r<Real, FAM>(P, cur.v, cur.t);
+    }
+    // (3) level-2 loads of batch b+1
+    if (has_next) {
+      sweep_load2(S, A.u, A.dir, n_ib, nxt);
+      n_p1 = A.row_ptr[n_bd];
+    }
+    __syncthreads();
+    // (4) phase B: row entries of batch b (prefetched entry + rare overflow entries)
+    if (cur.ent_ok) {
+      const int cnt = cur.meta >> 16;
+      Real gs = Real(0);
+#pragma unroll
+      for (int k = 0; k < kPfWords; ++k)
+        if (k < cnt) sweep_reduce_word<Real, WANT, NB>(cur.w[k], cur.pos, sH, sG, swin, S.win_mask, gs);
+      for (int k = kPfWords; k < cnt; ++k)
+        sweep_reduce_word<Real, WANT, NB>(__ldg(S.inc_word + c_ib + (cur.meta & 0xffffu) + k), cur.pos, sH, sG,
+                                          swin, S.win_mask, gs);
+      if (WANT & W_G) sgw[cur.row & S.rwin_mask] += gs;
+    }
+    for (int ent = c_eb + NB + threadIdx.x; ent < c_ee; ent += NB) {
+      const int r = __ldg(S.ent_row + ent);
+      const int pos0 = __ldg(S.ent_pos + ent);
+      const unsigned meta = __ldg(S.ent_meta + ent);
+      const unsigned* __restrict__ iw = S.inc_word + c_ib + (meta & 0xffffu);
+      Real gs = Real(0);
+      for (int k = 0; k < (int)(meta >> 16); ++k)
+        sweep_reduce_word<Real, WANT, NB>(__ldg(iw + k), pos0, sH, sG, swin, S.win_mask, gs);
+      if (WANT & W_G) sgw[r & S.rwin_mask] += gs;
+    }
+    __syncthreads();
+    // (5) phase C: stream out the rows that are now final
+    if (c_bd > done) {
+      if (WANT & W_H)
+        for (int q = p_done + threadIdx.x; q < c_p1; q += NB) {
+          hess[q] = (HOut)swin[q & S.win_mask];
+          swin[q & S.win_mask] = Real(0);
+        }
+      for (int r = done + threadIdx.x; r < c_bd; r += NB) {
+        const int gp = S.gpos_identity ? r : A.row_gpos[r];
+        if (WANT & W_G) {
+          grad[gp] = (double)sgw[r & S.rwin_mask] - (A.rhs ? A.rhs[gp] : 0.0);
+          sgw[r & S.rwin_mask] = Real(0);
+        }
+        if ((WANT & W_E) && A.rhs) eacc -= A.rhs[gp] * A.u[A.lo + gp];
+      }
+      done = c_bd;
+      p_done = c_p1;
+    }
+    cur = nxt;
+    c_eb = n_eb;
+    c_ee = n_ee;
+    c_ib = n_ib;
+    c_bd = n_bd;
+    c_p1 = n_p1;
+  }
+  if (done < R1) {  // rows no element of the segment touches (gradient-only rows)
+    __syncthreads();
+    const int p1 = A.row_ptr[R1];
+    if (WANT & W_H)
+      for (int q = p_done + threadIdx.x; q < p1; q += NB) hess[q] = (HOut)swin[q & S.win_mask];
+    for (int r = done + threadIdx.x; r < R1; r += NB) {
+      const int gp = S.gpos_identity ? r : A.row_gpos[r];
+      if (WANT & W_G) grad[gp] = (double)sgw[r & S.rwin_mask] - (A.rhs ? A.rhs[gp] : 0.0);
+      if ((WANT & W_E) && A.rhs) eacc -= A.rhs[gp] * A.u[A.lo + gp];
+    }
+  }
+  if (WANT & W_E) energy_finalize(eacc, eo);
+}
+
+// ---------------------------------------------------------------------------
 // energy-only kernels (element-centric, grid-stride)
 // ---------------------------------------------------------------------------
 constexpr int kElemThreads = 256;
@@ -740,6 +1000,12 @@ struct fne_handle {
   size_t smem_bytes = 0;
   int device = 0, num_sms = 148;
   bool use_inc = false;
+  bool use_sweep = false;
+  int sweep_nb = 0, sweep_win_mask = 0, sweep_rwin_mask = 0;
+  int *sw_seg_row = nullptr, *sw_seg_elem = nullptr, *sw_seg_batch = nullptr, *sw_batch_done = nullptr,
+      *sw_ent_ptr = nullptr, *sw_inc_base = nullptr, *sw_ent_row = nullptr, *sw_ent_pos = nullptr;
+  int sw_gpos_identity = 0;
+  unsigned *sw_ent_meta = nullptr, *sw_inc_word = nullptr;
   int inc_max_rank = 0, inc_max_rows = 0, inc_max_len = 0;
   Phys phys{};
   // device buffers
@@ -790,6 +1056,8 @@ void free_handle(fne_handle* h) {
   if (!h) return;
   void* ptrs[] = {h->rec, h->rec_dir_only, h->row_ptr, h->row_node, h->row_gpos, h->inc_ptr, h->inc_elem,
                   h->row_comp, h->inc_info, h->cta_row, h->cta_inc, h->inc_elem2, h->inc_word, h->inc_rowl,
+                  h->sw_seg_row, h->sw_seg_elem, h->sw_seg_batch, h->sw_batch_done, h->sw_ent_ptr, h->sw_inc_base,
+                  h->sw_ent_row, h->sw_ent_pos, h->sw_ent_meta, h->sw_inc_word,
                   h->dir, h->rhs, h->partials, h->dir_const, h->counter, h->h_u, h->h_grad, h->h_energy,
                   h->h_hess};
   for (void* p : ptrs)
@@ -875,14 +1143,20 @@ bool is_tri(int fam) { return fam == FNE_PLAPLACE || fam == FNE_GINZBURG_LANDAU;
 
 // ---- kernel dispatch -------------------------------------------------------
 template <typename Real, int FAM, typename HOut>
-cudaError_t launch_tri_t(fne_handle* h, int want, const RowArgs& A, const IncArgs& Q, double* grad, void* hess,
-                         EnergyOut eo, cudaStream_t st, bool set_attr) {
+cudaError_t launch_tri_t(fne_handle* h, int want, const RowArgs& A, const IncArgs& Q, const SweepArgs& SW,
+                         double* grad, void* hess, EnergyOut eo, cudaStream_t st, bool set_attr) {
   HOut* H = static_cast<HOut*>(hess);
   const size_t sm = h->smem_bytes;
   const dim3 grid(h->grid_rows);
+  constexpr int NBS = sizeof(Real) == 4 ? 512 : 256;
 #define FNE_TRI_CASE(W)                                                                                        \
   case W:                                                                                                      \
-    if (h->use_inc) {                                                                                          \
+    if (h->use_sweep) {                                                                                        \
+      if (set_attr)                                                                                            \
+        return cudaFuncSetAttribute(k_sweep_tri<Real, FAM, W, HOut, NBS>,                                     \
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                     \
+      k_sweep_tri<Real, FAM, W, HOut, NBS><<<grid, NBS, sm, st>>>(A, SW, h->rec, h->phys, grad, H, eo);       \
+    } else if (h->use_inc) {                                                                                          \
       if (set_attr)                                                                                            \
         return cudaFuncSetAttribute(k_inc_tri<Real, FAM, W, HOut>,                                            \
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                     \
@@ -931,19 +1205,19 @@ cudaError_t launch_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_rows(fne_handle* h, int want, const RowArgs& A, const IncArgs& Q, double* grad, void* hess,
-                        EnergyOut eo, cudaStream_t st, bool set_attr) {
+cudaError_t launch_rows(fne_handle* h, int want, const RowArgs& A, const IncArgs& Q, const SweepArgs& SW,
+                        double* grad, void* hess, EnergyOut eo, cudaStream_t st, bool set_attr) {
   const bool f32 = h->precision == FNE_FP32;
   const bool h32 = f32 && h->hess_fp32;
   if (h->family == FNE_PLAPLACE) {
-    if (!f32) return launch_tri_t<double, FAM_PLAP, double>(h, want, A, Q, grad, hess, eo, st, set_attr);
-    if (h32) return launch_tri_t<float, FAM_PLAP, float>(h, want, A, Q, grad, hess, eo, st, set_attr);
-    return launch_tri_t<float, FAM_PLAP, double>(h, want, A, Q, grad, hess, eo, st, set_attr);
+    if (!f32) return launch_tri_t<double, FAM_PLAP, double>(h, want, A, Q, SW, grad, hess, eo, st, set_attr);
+    if (h32) return launch_tri_t<float, FAM_PLAP, float>(h, want, A, Q, SW, grad, hess, eo, st, set_attr);
+    return launch_tri_t<float, FAM_PLAP, double>(h, want, A, Q, SW, grad, hess, eo, st, set_attr);
   }
   if (h->family == FNE_GINZBURG_LANDAU) {
-    if (!f32) return launch_tri_t<double, FAM_GL, double>(h, want, A, Q, grad, hess, eo, st, set_attr);
-    if (h32) return launch_tri_t<float, FAM_GL, float>(h, want, A, Q, grad, hess, eo, st, set_attr);
-    return launch_tri_t<float, FAM_GL, double>(h, want, A, Q, grad, hess, eo, st, set_attr);
+    if (!f32) return launch_tri_t<double, FAM_GL, double>(h, want, A, Q, SW, grad, hess, eo, st, set_attr);
+    if (h32) return launch_tri_t<float, FAM_GL, float>(h, want, A, Q, SW, grad, hess, eo, st, set_attr);
+    return launch_tri_t<float, FAM_GL, double>(h, want, A, Q, SW, grad, hess, eo, st, set_attr);
   }
   if (h->family == FNE_NEOHOOKEAN) {
     if (!f32) return launch_tet_t<double, double>(h, want, A, grad, hess, eo, st, set_attr);
@@ -1038,11 +1312,30 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   const bool f32 = d->precision == FNE_FP32;
   const size_t real_size = f32 ? sizeof(float) : sizeof(double);
 
-  // incidence-parallel plan for triangles (else the row-gather kernel)
+  int dev_id = 0, n_sms = 148, smem_optin = 227 * 1024;
+  cudaGetDevice(&dev_id);
+  cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, dev_id);
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev_id);
+  if (smem_optin <= 0) smem_optin = 227 * 1024;
+  // banded sweep for triangles (default), incidence-parallel on request,
+  // else the row-gather kernel
   IncPlan inc;
-  bool use_inc = false;
+  SweepPlan sweep;
+  bool use_inc = false, use_sweep = false;
+  const int sweep_nb = f32 ? 512 : 256;
   if (is_tri(d->family) && plan.n_rows > 0 && d->kernel_variant == 2)
     use_inc = build_inc_plan(plan, kIncThreads, inc);
+  if (is_tri(d->family) && plan.n_rows > 0 && d->kernel_variant == 0) {
+    // shared memory per CTA: 12*nb element quantities + entry window + row window,
+    // sized so that two CTAs fit on one SM
+    const int64_t budget = std::min<int64_t>(smem_optin, (228 * 1024) / 2 - 1024) / (int64_t)real_size;
+    const int64_t avail = budget - 12 * (int64_t)sweep_nb;
+    const int n_seg = (int)std::max<int64_t>(
+        1, std::min<int64_t>(2 * n_sms, (int64_t)plan.local_elems.size() / (4 * sweep_nb)));
+    if (avail > 0)
+      use_sweep = build_sweep_plan(plan, sweep_nb, n_seg, (int)(avail * 3 / 4), (int)(avail / 4), sweep);
+    if (use_sweep && 12 * (int64_t)sweep_nb + sweep.win_entries + sweep.win_rows > budget) use_sweep = false;
+  }
 
   auto* h = new (std::nothrow) fne_handle();
   if (!h) return set_error(FNE_ENOMEM, "fne_create: out of host memory");
@@ -1062,6 +1355,7 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   h->n_inc = (int64_t)plan.inc_elem.size();
   h->max_row_len = plan.max_row_len;
   h->use_inc = use_inc;
+  h->use_sweep = use_sweep;
   h->phys.p = d->s[0];
   h->phys.eps = d->s[0];
   for (int i = 0; i < 9; ++i) h->phys.ip[i] = d->s[1 + i];
@@ -1069,10 +1363,23 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   h->phys.C1 = d->s[0];
   h->phys.D1 = d->s[1];
   h->phys.absdet = d->family == FNE_NEOHOOKEAN && d->s[2] != 0.0;
+  h->phys.p_is3 = d->family == FNE_PLAPLACE && d->s[0] == 3.0;
+  h->phys.pf = (float)h->phys.p;
+  h->phys.epsf = (float)h->phys.eps;
+  for (int i = 0; i < 9; ++i) h->phys.ipf[i] = (float)h->phys.ip[i];
+  for (int i = 0; i < 3; ++i) h->phys.wf[i] = (float)h->phys.w[i];
+  h->phys.C1f = (float)h->phys.C1;
+  h->phys.D1f = (float)h->phys.D1;
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
 
-  if (use_inc) {
+  if (use_sweep) {
+    h->grid_rows = sweep.n_seg;
+    h->sweep_nb = sweep.nb;
+    h->sweep_win_mask = sweep.win_entries - 1;
+    h->sweep_rwin_mask = sweep.win_rows - 1;
+    h->smem_bytes = ((size_t)12 * sweep.nb + sweep.win_entries + sweep.win_rows) * real_size;
+  } else if (use_inc) {
     h->grid_rows = inc.n_cta;
     h->inc_max_rank = inc.max_rank;
     h->inc_max_rows = std::max(1, inc.max_rows);
@@ -1120,7 +1427,19 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   FNE_TRY(upload(h, &h->row_comp, plan.row_comp.data(), plan.row_comp.size()));
   FNE_TRY(upload(h, &h->row_gpos, plan.row_gpos.data(), plan.row_gpos.size()));
   FNE_TRY(upload(h, &h->inc_ptr, plan.inc_ptr.data(), plan.inc_ptr.size()));
-  if (use_inc) {
+  if (use_sweep) {
+    FNE_TRY(upload(h, &h->sw_seg_row, sweep.seg_row.data(), sweep.seg_row.size()));
+    FNE_TRY(upload(h, &h->sw_seg_elem, sweep.seg_elem.data(), sweep.seg_elem.size()));
+    FNE_TRY(upload(h, &h->sw_seg_batch, sweep.seg_batch.data(), sweep.seg_batch.size()));
+    FNE_TRY(upload(h, &h->sw_batch_done, sweep.batch_done.data(), sweep.batch_done.size()));
+    FNE_TRY(upload(h, &h->sw_ent_ptr, sweep.ent_ptr.data(), sweep.ent_ptr.size()));
+    FNE_TRY(upload(h, &h->sw_inc_base, sweep.inc_base.data(), sweep.inc_base.size()));
+    FNE_TRY(upload(h, &h->sw_ent_row, sweep.ent_row.data(), sweep.ent_row.size()));
+    FNE_TRY(upload(h, &h->sw_ent_pos, sweep.ent_pos.data(), sweep.ent_pos.size()));
+    h->sw_gpos_identity = sweep.gpos_identity ? 1 : 0;
+    FNE_TRY(upload(h, &h->sw_ent_meta, sweep.ent_meta.data(), sweep.ent_meta.size()));
+    FNE_TRY(upload(h, &h->sw_inc_word, sweep.inc_word.data(), sweep.inc_word.size()));
+  } else if (use_inc) {
     FNE_TRY(upload(h, &h->cta_row, inc.cta_row.data(), inc.cta_row.size()));
     FNE_TRY(upload(h, &h->cta_inc, inc.cta_inc.data(), inc.cta_inc.size()));
     FNE_TRY(upload(h, &h->inc_elem2, inc.inc_elem.data(), inc.inc_elem.size()));
@@ -1148,8 +1467,9 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   if (h->smem_bytes > 48 * 1024) {
     RowArgs ra{};
     IncArgs pa{};
+    SweepArgs sa{};
     for (int want = 2; want <= 7; ++want) {
-      cudaError_t e = launch_rows(h, want, ra, pa, nullptr, nullptr, EnergyOut{}, 0, true);
+      cudaError_t e = launch_rows(h, want, ra, pa, sa, nullptr, nullptr, EnergyOut{}, 0, true);
       if (e != cudaSuccess) {
         free_handle(h);
         return cuda_fail(e, "cudaFuncSetAttribute");
@@ -1169,7 +1489,7 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   info->n_incidences = h->n_inc;
   info->device_bytes = h->device_bytes;
   info->max_row_len = h->max_row_len;
-  info->kernel_variant = is_tri(h->family) ? (h->use_inc ? 3 : 1) : 2;
+  info->kernel_variant = is_tri(h->family) ? (h->use_sweep ? 4 : (h->use_inc ? 3 : 1)) : 2;
   return FNE_OK;
 }
 
@@ -1212,7 +1532,11 @@ extern "C" int fne_eval(fne_handle* h, const double* u, int flags, double* energ
     A.nrec = h->n_local;
     IncArgs Q{h->cta_row, h->cta_inc, h->inc_elem2, h->inc_word, h->inc_rowl, h->inc_max_rank, h->inc_max_rows,
               h->inc_max_len};
-    e = launch_rows(h, flags, A, Q, grad, hess, eo, st, false);
+    SweepArgs SW{h->sw_seg_row,  h->sw_seg_elem,  h->sw_seg_batch,  h->sw_batch_done,
+                 h->sw_ent_ptr,  h->sw_inc_base,  h->sw_ent_row,    h->sw_ent_pos,
+                 h->sw_ent_meta, h->sw_inc_word,  h->sweep_win_mask, h->sweep_rwin_mask,
+                 h->sw_gpos_identity};
+    e = launch_rows(h, flags, A, Q, SW, grad, hess, eo, st, false);
   }
   if (e != cudaSuccess) return cuda_fail(e, "fne_eval launch");
   return FNE_OK;

@@ -74,6 +74,40 @@ struct IncPlan {
 // when the mesh does not fit the packed format.
 bool build_inc_plan(RowPlan& P, int threads, IncPlan& Q);
 
+// Banded-sweep plan (scalar P1 triangles).  Elements are sorted by the
+// first output row f(e) that needs them.  CTA s sweeps the row segment
+// [seg_row[s], seg_row[s+1]): it evaluates the elements [seg_elem[3s],
+// seg_elem[3s+2]) in batches of `nb` (the first ones, below seg_elem[3s+1],
+// only feed rows of the segment; the energy is counted for
+// [seg_elem[3s+1], seg_elem[3s+2])).  After batch b every row below
+// batch_done[b] is final and is streamed out of the shared-memory ring
+// window.  Batch b's row entries ent_ptr[b]..: ent_row = row, ent_meta = first
+// incidence (relative to inc_base[b], bits 0-15) | count << 16; incidence
+// word: bits 0-8 batch-local element (nb <= 512), 9-10 local node a, then
+// 7-bit column offsets of element nodes 0..2 from bit 11 (127 = Dirichlet).
+struct SweepPlan {
+  int32_t nb = 0;                       // elements per batch (= threads)
+  int32_t n_seg = 0;
+  int32_t win_entries = 0;              // ring window size (power of two)
+  int32_t win_rows = 0;                 // ring window for gradient rows (power of two)
+  std::vector<int32_t> seg_row;         // [n_seg+1]
+  std::vector<int32_t> seg_elem;        // [3*n_seg] (pre start, own start, own end)
+  std::vector<int32_t> seg_batch;       // [n_seg+1]
+  std::vector<int32_t> batch_done;      // [n_batch]
+  std::vector<int32_t> ent_ptr;         // [n_batch+1]
+  std::vector<int32_t> inc_base;        // [n_batch]
+  std::vector<int32_t> ent_row;         // [n_ent]
+  std::vector<int32_t> ent_pos;         // [n_ent] COO position of the row's first entry
+  std::vector<uint32_t> ent_meta;       // [n_ent]
+  bool gpos_identity = false;           // gradient slot of row k is k
+  std::vector<uint32_t> inc_word;       // [n_inc_sweep]
+};
+
+// Sorts P's local elements by first row (permuting element arrays and
+// P.inc_elem) and builds Q with n_seg segments.  Returns false when the mesh
+// does not fit (window larger than max_win_entries, rows longer than 126...).
+bool build_sweep_plan(RowPlan& P, int nb, int n_seg, int max_win_entries, int max_win_rows, SweepPlan& Q);
+
 // Gather code of one element node: >= 0 reordered id of component 0 (free
 // node); < 0: -1 - total DOF of component 0 (Dirichlet node).
 }  // namespace fne

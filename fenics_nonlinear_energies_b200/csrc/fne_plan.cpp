@@ -304,3 +304,160 @@ bool build_inc_plan(RowPlan& P, int threads, IncPlan& Q) {
 }
 
 }  // namespace fne
+
+namespace fne {
+
+static int32_t next_pow2(int64_t x) {
+  int64_t p = 1;
+  while (p < x) p <<= 1;
+  return (int32_t)p;
+}
+
+bool build_sweep_plan(RowPlan& P, int nb, int n_seg, int max_win_entries, int max_win_rows, SweepPlan& Q) {
+  const int32_t n_local = (int32_t)P.local_elems.size();
+  const int npe = n_local ? (int)(P.elem_code.size() / n_local) : 3;
+  if (npe != 3 || nb > 512 || n_local == 0) return false;
+  const int32_t n_rows = P.n_rows;
+  // first / last row of every element
+  std::vector<int32_t> first(n_local, INT32_MAX), last(n_local, -1);
+  for (int32_t k = 0; k < n_rows; ++k) {
+    const int32_t nd = P.row_node[k];
+    for (int32_t i = P.inc_ptr[nd]; i < P.inc_ptr[nd + 1]; ++i) {
+      first[P.inc_elem[i]] = std::min(first[P.inc_elem[i]], k);
+      last[P.inc_elem[i]] = std::max(last[P.inc_elem[i]], k);
+    }
+  }
+  std::vector<int32_t> order(n_local);
+  for (int32_t i = 0; i < n_local; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return first[a] < first[b]; });
+  std::vector<int32_t> newidx(n_local);
+  for (int32_t i = 0; i < n_local; ++i) newidx[order[i]] = i;
+  {
+    std::vector<int64_t> le(n_local);
+    std::vector<int32_t> code(P.elem_code.size());
+    std::vector<uint8_t> w(n_local);
+    std::vector<int32_t> f2(n_local), l2(n_local);
+    for (int32_t i = 0; i < n_local; ++i) {
+      le[i] = P.local_elems[order[i]];
+      w[i] = P.elem_weight[order[i]];
+      f2[i] = first[order[i]];
+      l2[i] = last[order[i]];
+      for (int a = 0; a < npe; ++a) code[(size_t)i * npe + a] = P.elem_code[(size_t)order[i] * npe + a];
+    }
+    P.local_elems.swap(le);
+    P.elem_code.swap(code);
+    P.elem_weight.swap(w);
+    first.swap(f2);
+    last.swap(l2);
+    for (auto& e : P.inc_elem) e = newidx[e];
+  }
+  // incidences of every row sorted by (new) element index
+  std::vector<int32_t> rinc_ptr(n_rows + 1, 0);
+  for (int32_t k = 0; k < n_rows; ++k) rinc_ptr[k + 1] = rinc_ptr[k] + (P.inc_ptr[P.row_node[k] + 1] - P.inc_ptr[P.row_node[k]]);
+  std::vector<std::pair<int32_t, uint32_t>> rinc(rinc_ptr[n_rows]);  // (element, info)
+  for (int32_t k = 0; k < n_rows; ++k) {
+    const int32_t nd = P.row_node[k];
+    int32_t q = rinc_ptr[k];
+    for (int32_t i = P.inc_ptr[nd]; i < P.inc_ptr[nd + 1]; ++i) rinc[q++] = {P.inc_elem[i], P.inc_info[i]};
+    std::sort(rinc.begin() + rinc_ptr[k], rinc.begin() + rinc_ptr[k + 1]);
+  }
+  // segments: balance the elements each CTA evaluates (own + pre)
+  n_seg = std::max(1, std::min(n_seg, n_rows));
+  Q.nb = nb;
+  Q.seg_row.assign(1, 0);
+  {
+    // cumulative own-element count by first row
+    std::vector<int64_t> cum(n_rows + 1, 0);
+    for (int32_t i = 0; i < n_local; ++i)
+      if (first[i] < n_rows) cum[first[i] + 1]++;
+    for (int32_t k = 0; k < n_rows; ++k) cum[k + 1] += cum[k];
+    for (int s = 1; s < n_seg; ++s) {
+      const int64_t target = (int64_t)n_local * s / n_seg;
+      int32_t r = (int32_t)(std::lower_bound(cum.begin(), cum.end(), target) - cum.begin());
+      r = std::max(r, Q.seg_row.back() + 1);
+      if (r >= n_rows) break;
+      Q.seg_row.push_back(r);
+    }
+    Q.seg_row.push_back(n_rows);
+  }
+  Q.n_seg = (int32_t)Q.seg_row.size() - 1;
+  Q.seg_elem.assign(3 * (size_t)Q.n_seg, 0);
+  Q.seg_batch.assign(1, 0);
+  Q.batch_done.clear();
+  Q.ent_ptr.assign(1, 0);
+  Q.inc_base.clear();
+  Q.ent_row.clear();
+  Q.ent_pos.clear();
+  Q.ent_meta.clear();
+  Q.inc_word.clear();
+  int64_t need_entries = 1, need_rows = 1;
+  std::vector<std::vector<std::pair<int32_t, int32_t>>> per_batch;  // (row, rinc index) lists
+  for (int32_t s = 0; s < Q.n_seg; ++s) {
+    const int32_t R0 = Q.seg_row[s], R1 = Q.seg_row[s + 1];
+    const int32_t o_lo = (int32_t)(std::lower_bound(first.begin(), first.end(), R0) - first.begin());
+    const int32_t o_hi = (int32_t)(std::lower_bound(first.begin(), first.end(), R1) - first.begin());
+    // pre elements: smallest element index touching a row of the segment
+    int32_t p_lo = o_lo;
+    for (int32_t k = R0; k < R1; ++k)
+      if (rinc_ptr[k + 1] > rinc_ptr[k]) p_lo = std::min(p_lo, rinc[rinc_ptr[k]].first);
+    Q.seg_elem[3 * s] = p_lo;
+    Q.seg_elem[3 * s + 1] = o_lo;
+    Q.seg_elem[3 * s + 2] = o_hi;
+    const int32_t nbat = (o_hi - p_lo + nb - 1) / nb;
+    per_batch.assign(nbat, {});
+    for (int32_t k = R0; k < R1; ++k)
+      for (int32_t q = rinc_ptr[k]; q < rinc_ptr[k + 1]; ++q) {
+        const int32_t e = rinc[q].first;
+        if (e < p_lo || e >= o_hi) return false;  // cannot happen for a consistent plan
+        per_batch[(e - p_lo) / nb].push_back({k, q});
+      }
+    int32_t done = R0, maxrow = R0 - 1;
+    for (int32_t b = 0; b < nbat; ++b) {
+      const int32_t e0 = p_lo + b * nb;
+      auto& lst = per_batch[b];  // already grouped by row (rows ascending, incidences ascending)
+      Q.inc_base.push_back((int32_t)Q.inc_word.size());
+      const int32_t base = (int32_t)Q.inc_word.size();
+      for (size_t x = 0; x < lst.size();) {
+        const int32_t row = lst[x].first;
+        size_t y = x;
+        const int32_t start = (int32_t)Q.inc_word.size() - base;
+        while (y < lst.size() && lst[y].first == row) {
+          const int32_t e = rinc[lst[y].second].first;
+          const uint32_t info = rinc[lst[y].second].second;
+          uint32_t w = (uint32_t)(e - e0) | ((info & 3u) << 9);
+          w |= ((info >> kOffShift) & ((1u << (3 * kOffBits)) - 1u)) << 11;
+          Q.inc_word.push_back(w);
+          ++y;
+        }
+        const int32_t cnt = (int32_t)(y - x);
+        if (start >= 65536 || cnt > 255) return false;
+        Q.ent_row.push_back(row);
+        Q.ent_pos.push_back(P.row_ptr[row]);
+        Q.ent_meta.push_back((uint32_t)start | ((uint32_t)cnt << 16));
+        maxrow = std::max(maxrow, row);
+        x = y;
+      }
+      Q.ent_ptr.push_back((int32_t)Q.ent_row.size());
+      // live window after this batch: positions [row_ptr[done], row_ptr[maxrow + 1])
+      if (maxrow >= done) {
+        need_entries = std::max<int64_t>(need_entries, (int64_t)P.row_ptr[maxrow + 1] - P.row_ptr[done]);
+        need_rows = std::max<int64_t>(need_rows, (int64_t)maxrow + 1 - done);
+      }
+      const int32_t nxt = (b + 1 < nbat) ? first[e0 + nb] : R1;
+      done = std::max(done, std::min(std::max(nxt, R0), R1));
+      Q.batch_done.push_back(done);
+    }
+    Q.seg_batch.push_back((int32_t)Q.batch_done.size());
+  }
+  Q.gpos_identity = true;
+  for (int32_t k = 0; k < n_rows; ++k)
+    if (P.row_gpos[k] != k) {
+      Q.gpos_identity = false;
+      break;
+    }
+  Q.win_entries = next_pow2(need_entries);
+  Q.win_rows = next_pow2(need_rows);
+  return Q.win_entries <= max_win_entries && Q.win_rows <= max_win_rows;
+}
+
+}  // namespace fne

@@ -153,7 +153,8 @@ def test_deterministic_and_energy_paths_agree():
     e2, g2, h2 = [t.clone() for t in gpu.eval(ut, 7)]
     assert torch.equal(h1, h2) and torch.equal(g1, g2) and torch.equal(e1, e2)
     e_only = gpu.eval(ut, _lib.FNE_ENERGY)[0].clone()
-    assert abs(float(e_only.item()) - float(e1.item())) < 1e-12 * abs(float(e1.item()))
+    # the fused pass sums FP32 element energies in FP64; the energy-only pass is FP64 throughout
+    assert abs(float(e_only.item()) - float(e1.item())) < 1e-6 * abs(float(e1.item()))
 
 
 def test_autograd_energy_function():
