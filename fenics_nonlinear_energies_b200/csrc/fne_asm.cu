@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "fne_internal.h"
@@ -986,6 +987,122 @@ __global__ void __launch_bounds__(kElemThreads) k_energy_tet(const Chunk* __rest
   if (rhs)
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_owned; i += stride) acc -= rhs[i] * u[lo + i];
   energy_finalize(acc, eo);
+}
+
+// ---------------------------------------------------------------------------
+// No-allocation energy entry point (fne_energy_p1tri_noalloc).
+//
+// Same FP64 energy reduction as k_energy_tri, reading the caller's float64
+// element arrays directly.  Its scratch (the per-CTA partial sums and the
+// last-CTA ticket) is this file-scope device array instead of handle-owned
+// memory, so the entry point never allocates.  Host code must not use the
+// symbol itself as a device pointer: the device address is obtained once per
+// device with cudaGetSymbolAddress (noalloc_scratch below).
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxCtas = 1024;  // grid cap = number of partial sums
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxCtas + 1];  // + ticket slot
+
+__global__ void __launch_bounds__(256) k_energy_tri_soa(int fam, int n_el, const int* __restrict__ codes,
+                                                        const double* __restrict__ dvx,
+                                                        const double* __restrict__ dvy,
+                                                        const double* __restrict__ vol,
+                                                        const double* __restrict__ weights,
+                                                        const double* __restrict__ u,
+                                                        const double* __restrict__ dir, Phys P,
+                                                        const double* __restrict__ rhs, int n_owned, long long lo,
+                                                        EnergyOut eo) {
+  double acc = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += stride) {
+    const double w = weights ? weights[e] : 1.0;
+    if (w == 0.0) continue;
+    TriElem<double> t;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      t.src[k] = codes[3 * e + k];
+      t.dvx[k] = dvx[3 * e + k];
+      t.dvy[k] = dvy[3 * e + k];
+    }
+    t.vol = vol[e];
+    t.wflag = 1;
+    double vd[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) vd[k] = gather(u, dir, t.src[k], 0);
+    acc += w * (fam == FAM_PLAP ? tri_energy<double, FAM_PLAP>(P, vd, t) : tri_energy<double, FAM_GL>(P, vd, t));
+  }
+  if (rhs)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_owned; i += stride) acc -= rhs[i] * u[lo + i];
+  energy_finalize(acc, eo);
+}
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up once
+// per device; the first call on a device performs the lookup).
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(FNE_EBOUNDS, "device ordinal beyond 63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(FNE_ECUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return FNE_OK;
+}
+}  // namespace
+
+extern "C" int fne_energy_p1tri_noalloc(int32_t family, int64_t n_elem, const int32_t* codes, const double* dvx,
+                                        const double* dvy, const double* vol, const double* weights,
+                                        const double* u, const double* dirichlet, const double* params,
+                                        const double* rhs, int64_t n_owned, int64_t lo, double* energy,
+                                        void* stream) {
+  if (family != FNE_PLAPLACE && family != FNE_GINZBURG_LANDAU)
+    return set_error(FNE_EINVAL, "fne_energy_p1tri_noalloc: family must be FNE_PLAPLACE or FNE_GINZBURG_LANDAU");
+  if (n_elem < 0 || n_elem > (int64_t)INT32_MAX || n_owned < 0 || n_owned > (int64_t)INT32_MAX)
+    return set_error(FNE_EBOUNDS,
+                     "fne_energy_p1tri_noalloc: n_elem and n_owned must be in [0, 2^31-1] (32-bit indexing)");
+  if (!energy || !params || (n_elem > 0 && (!codes || !dvx || !dvy || !vol)) || (rhs && n_owned > 0 && !u))
+    return set_error(FNE_EINVAL, "fne_energy_p1tri_noalloc: missing array");
+  if (family == FNE_PLAPLACE && !(params[0] > 1.0))
+    return set_error(FNE_EINVAL, "fne_energy_p1tri_noalloc: p-Laplace needs p > 1");
+  double* scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  Phys P{};
+  P.p = params[0];
+  P.eps = params[0];
+  if (family == FNE_GINZBURG_LANDAU) {
+    for (int i = 0; i < 9; ++i) P.ip[i] = params[1 + i];
+    for (int i = 0; i < 3; ++i) P.w[i] = params[10 + i];
+  }
+  P.p_is3 = family == FNE_PLAPLACE && params[0] == 3.0;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t work = std::max<int64_t>(n_elem, n_owned);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)kNoAllocMaxCtas, (int64_t)sms * 8,
+                                                                (work + 255) / 256}));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned* ticket = reinterpret_cast<unsigned*>(scratch + kNoAllocMaxCtas);
+  cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), st);  // the ticket must start at zero
+  if (e != cudaSuccess)
+    return set_error(FNE_ECUDA, std::string("fne_energy_p1tri_noalloc memset: ") + cudaGetErrorString(e));
+  EnergyOut eo{scratch, ticket, energy, nullptr};
+  k_energy_tri_soa<<<grid, 256, 0, st>>>(family == FNE_PLAPLACE ? FAM_PLAP : FAM_GL, (int)n_elem, codes, dvx, dvy,
+                                         vol, weights, u, dirichlet, P, rhs, (int)n_owned, (long long)lo, eo);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_error(FNE_ECUDA, std::string("fne_energy_p1tri_noalloc launch: ") + cudaGetErrorString(e));
+  return FNE_OK;
 }
 
 // ---------------------------------------------------------------------------

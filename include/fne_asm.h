@@ -176,6 +176,35 @@ int fne_eval_host(fne_handle* h, const double* u_host, int flags, double* energy
                   double* grad_host, void* hess_host);
 int fne_destroy(fne_handle* h);
 
+/*
+ * No counterpart in the reference.  FP64 energy of P1-triangle p-Laplace /
+ * Ginzburg-Landau elements WITHOUT any device allocation: for callers whose
+ * device memory belongs to someone else -- a framework whose caching
+ * allocator already holds the GPU's memory, or a solver that forbids
+ * allocation once it is set up -- and who therefore cannot let a library
+ * call cudaMalloc (fne_create allocates the element records and its scratch).
+ * The caller passes every input and the output as device arrays:
+ *   codes   [n_elem*3] int32 gather codes: >= 0 index into u, < 0 the
+ *           Dirichlet entry -1-code of ``dirichlet``
+ *   dvx, dvy [n_elem*3], vol [n_elem] float64 (the reference's element arrays)
+ *   weights [n_elem] 0/1 energy weights, or NULL (all 1)
+ *   params  HOST array laid out like fne_desc.s (p; or eps, ip[9], w[3])
+ *   rhs     [n_owned] load vector or NULL; subtracts rhs . u[lo:lo+n_owned]
+ *   energy  device double receiving sum_e w_e e_e - rhs.u
+ * Scratch: a fixed device array inside libfne_asm.so (1024 FP64 partial sums
+ * and a ticket, ~8 KB per GPU, held until the process exits); the grid is
+ * capped at 1024 CTAs, so any n_elem up to 2^31-1 fits and larger sizes are
+ * rejected with FNE_EBOUNDS.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.  No
+ * cudaMalloc, cudaFree or allocating library routine is called.
+ */
+int fne_energy_p1tri_noalloc(int32_t family, int64_t n_elem, const int32_t* codes, const double* dvx,
+                             const double* dvy, const double* vol, const double* weights, const double* u,
+                             const double* dirichlet, const double* params, const double* rhs,
+                             int64_t n_owned, int64_t lo, double* energy, void* stream);
+
 const char* fne_last_error(void);
 const char* fne_version(void);
 
