@@ -116,6 +116,8 @@ class CudaElementAssemblerBase:
             r, d.rhs_owned = _lib.f64(rhs)
             keep.append(r)
         for slot, arr in zip(("e0", "e1", "e2", "e3"), self._element_arrays()):
+            if arr is None:
+                continue
             a, p = _lib.f64(arr)
             keep.append(a)
             setattr(d, slot, p)
@@ -341,6 +343,49 @@ class HECudaAssembler(CudaElementAssemblerBase):
 
     def _scalars(self):
         return [float(self.params["C1"]), float(self.params["D1"]), 1.0 if self.use_abs_det else 0.0]
+
+
+class SlopeStabilityCudaAssembler(CudaElementAssemblerBase):
+    """``SlopeStabilityReorderedElementAssembler``
+    (slope_stability/jax_petsc/reordered_element_assembler.py:75-243), plane-strain
+    Mohr-Coulomb (``constitutive_mode="mc"``) or linear elastic (``"elastic"``).
+
+    The element operators are passed in affine form (inverse Jacobian,
+    ``|det J|`` and the reference-element basis gradients at the quadrature
+    points) instead of the reference's stored ``elem_B``; for straight-sided
+    triangles both give the same strains.  The load vector is the gravity
+    ``force`` restricted to the owned DOFs.
+    """
+
+    family = _lib.FNE_MOHR_COULOMB
+    block_size = 2
+    coordinate_key, dirichlet_key = "nodes", "u_0"
+
+    def __init__(self, params, comm=None, adjacency=None, *, constitutive_mode="mc", **kw):
+        self.constitutive_mode = str(constitutive_mode)
+        if self.constitutive_mode not in ("mc", "elastic"):
+            raise ValueError(f"Unsupported constitutive_mode {constitutive_mode!r}")
+        self.npe = int(np.asarray(params["elems_scalar"]).shape[1])
+        super().__init__(params, comm, adjacency, **kw)
+
+    def _element_arrays(self):
+        p = self.params
+        epsp = np.asarray(p["eps_p_old"], dtype=np.float64)
+        tables = np.concatenate((np.ravel(p["dhat1"]), np.ravel(p["dhat2"]), np.ravel(p["quad_w"])))
+        return [np.asarray(p["inv_jac"]), np.asarray(p["det_j"]), epsp if np.any(epsp) else None, tables]
+
+    def _nq(self):
+        return int(np.asarray(self.params["quad_w"]).size)
+
+    def _scalars(self):
+        p = self.params
+        return [float(p["E"]), float(p["nu"]), float(p["phi_deg"]), float(p["cohesion"]),
+                float(p.get("reg", 1.0e-12)), 1.0 if self.constitutive_mode == "elastic" else 0.0]
+
+    def _build_rhs_owned(self):
+        force = np.asarray(self.params["force"], dtype=np.float64)
+        free = np.asarray(self.params["freedofs"], dtype=np.int64)
+        return np.ascontiguousarray(force[free][self.layout.perm][self.layout.lo: self.layout.hi])
 
 
 class EnergyFunction(torch.autograd.Function):

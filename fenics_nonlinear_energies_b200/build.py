@@ -38,7 +38,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if not force and not needs_build():
         return LIB
     cmd = [
-        _nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3",
+        _nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-Xptxas=-warn-spills",
         "-shared", "-o", str(LIB), *map(str, sources()),
     ]
     if verbose:

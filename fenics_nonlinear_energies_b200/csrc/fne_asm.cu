@@ -1109,6 +1109,7 @@ extern "C" int fne_energy_p1tri_noalloc(int32_t family, int64_t n_elem, const in
 // handle
 // ---------------------------------------------------------------------------
 struct fne_handle {
+  McHandle* mc = nullptr;  // Mohr-Coulomb handles delegate to fne_mc.cu
   int family = 0, precision = 0, hess_fp32 = 0, npe = 0, bs = 0;
   int64_t n_total = 0, n_free = 0, lo = 0, hi = 0, nnz = 0;
   int n_rows = 0, n_local = 0, n_dir_only = 0, rows_per_cta = 0, grid_rows = 0;
@@ -1171,6 +1172,7 @@ int upload(fne_handle* h, T** p, const T* src, size_t count) {
 
 void free_handle(fne_handle* h) {
   if (!h) return;
+  if (h->mc) mc_destroy(h->mc);
   void* ptrs[] = {h->rec, h->rec_dir_only, h->row_ptr, h->row_node, h->row_gpos, h->inc_ptr, h->inc_elem,
                   h->row_comp, h->inc_info, h->cta_row, h->cta_inc, h->inc_elem2, h->inc_word, h->inc_rowl,
                   h->sw_seg_row, h->sw_seg_elem, h->sw_seg_batch, h->sw_batch_done, h->sw_ent_ptr, h->sw_inc_base,
@@ -1409,7 +1411,28 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     npe_expect = 4;
     bs_expect = 3;
   } else if (d->family == FNE_MOHR_COULOMB) {
-    return set_error(FNE_EINVAL, "fne_create: Mohr-Coulomb handles are created with fne_create_mc");
+    if (d->n_elem < 0 || d->n_total < 0 || d->nnz < 0 || (d->n_elem > 0 && !d->elems) || !d->total_to_free_reord ||
+        (d->nnz > 0 && (!d->owned_rows || !d->owned_cols)) || (d->n_total > 0 && !d->dirichlet))
+      return set_error(FNE_EINVAL, "fne_create: missing array");
+    McHandle* mc = nullptr;
+    int rc = mc_create(d, &mc);
+    if (rc) return rc;
+    auto* h = new (std::nothrow) fne_handle();
+    if (!h) {
+      mc_destroy(mc);
+      return set_error(FNE_ENOMEM, "fne_create: out of host memory");
+    }
+    h->mc = mc;
+    h->family = d->family;
+    h->precision = d->precision;
+    h->hess_fp32 = d->precision == FNE_FP32 && d->hess_fp32;
+    h->n_total = d->n_total;
+    h->n_free = d->n_free;
+    h->lo = d->lo;
+    h->hi = d->hi;
+    h->nnz = d->nnz;
+    *out = h;
+    return FNE_OK;
   } else {
     return set_error(FNE_EINVAL, "fne_create: unknown family");
   }
@@ -1600,6 +1623,10 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
 
 extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   if (!h || !info) return set_error(FNE_EINVAL, "fne_info_get: null argument");
+  if (h->mc) {
+    mc_info(h->mc, info);
+    return FNE_OK;
+  }
   info->n_rows = h->n_rows;
   info->nnz = h->nnz;
   info->n_elem = h->n_local;
@@ -1613,6 +1640,7 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
 extern "C" int fne_set_dirichlet(fne_handle* h, const double* dirichlet) {
   if (!h || (!dirichlet && h->n_total > 0)) return set_error(FNE_EINVAL, "fne_set_dirichlet: null argument");
   if (h->n_total == 0) return FNE_OK;
+  if (h->mc) return mc_set_dirichlet(h->mc, dirichlet);
   cudaError_t e = cudaMemcpy(h->dir, dirichlet, h->n_total * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "fne_set_dirichlet");
   return refresh_dir_const(h);
@@ -1626,6 +1654,7 @@ extern "C" int fne_eval(fne_handle* h, const double* u, int flags, double* energ
   if ((flags & FNE_GRAD) && !grad && h->hi > h->lo) return set_error(FNE_EINVAL, "fne_eval: grad output missing");
   if ((flags & FNE_HESS) && !hess && h->nnz > 0) return set_error(FNE_EINVAL, "fne_eval: hess output missing");
   if (!u && h->n_free > 0) return set_error(FNE_EINVAL, "fne_eval: u missing");
+  if (h->mc) return mc_eval(h->mc, u, flags, energy, grad, hess, stream);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   EnergyOut eo{h->partials, h->counter, energy, h->dir_const};
   cudaError_t e = cudaSuccess;

@@ -108,6 +108,14 @@ struct SweepPlan {
 // does not fit (window larger than max_win_entries, rows longer than 126...).
 bool build_sweep_plan(RowPlan& P, int nb, int n_seg, int max_win_entries, int max_win_rows, SweepPlan& Q);
 
+// Mohr-Coulomb (plane strain, Pk triangles) handle, csrc/fne_mc.cu.
+struct McHandle;
+int mc_create(const fne_desc* d, McHandle** out);
+int mc_eval(McHandle* h, const double* u, int flags, double* energy, double* grad, void* hess, void* stream);
+int mc_set_dirichlet(McHandle* h, const double* dirichlet);
+void mc_info(const McHandle* h, fne_info* info);
+void mc_destroy(McHandle* h);
+
 // Gather code of one element node: >= 0 reordered id of component 0 (free
 // node); < 0: -1 - total DOF of component 0 (Dirichlet node).
 }  // namespace fne

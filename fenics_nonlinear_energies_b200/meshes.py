@@ -207,3 +207,217 @@ def rotate_right_face_from_reference(u0_reference, nodes2coord, angle, right_nod
     out[3 * rn + 1] = ca * y0 + sa * z0
     out[3 * rn + 2] = -sa * y0 + ca * z0
     return out
+
+
+# ---------------------------------------------------------------------------
+# Plane-strain slope (Mohr-Coulomb): P1 macro mesh -> same-mesh Pk Lagrange
+# ---------------------------------------------------------------------------
+SLOPE_LEVEL_TO_H = {1: 4.0, 2: 2.0, 3: 1.0, 4: 0.5, 5: 0.25, 6: 0.125, 7: 0.0625}
+SLOPE_GEOMETRY = {"x1": 15.0, "x2": 10.0, "x3": 15.0, "y1": 10.0, "y2": 10.0}
+
+# 7-point degree-5 rule on the reference triangle (area 1/2) with the
+# 13-digit constants the reference's P2 slope operators use
+# (src/problems/slope_stability/support/mesh.py:151-190).
+P2_QUAD_XI = np.array([
+    [0.1012865073235, 0.7974269853531, 0.1012865073235, 0.4701420641051, 0.4701420641051, 0.0597158717898,
+     1.0 / 3.0],
+    [0.1012865073235, 0.1012865073235, 0.7974269853531, 0.0597158717898, 0.4701420641051, 0.4701420641051,
+     1.0 / 3.0]])
+P2_QUAD_W = np.array([0.1259391805448, 0.1259391805448, 0.1259391805448, 0.1323941527885, 0.1323941527885,
+                      0.1323941527885, 0.225]) / 2.0
+
+
+def slope_counts(h, x1=15.0, x2=10.0, x3=15.0, y1=10.0, y2=10.0):
+    """Cell counts of the homogeneous slope grid for mesh size ``h``."""
+    nx12 = int(round((x1 + x2) / h))
+    nx3 = int(round(x3 / h))
+    ny1 = int(round(y1 / h))
+    ny2 = int(round(y2 / h))
+    return nx12, nx3, ny1, ny2
+
+
+def slope_macro_mesh(h, x1=15.0, x2=10.0, x3=15.0, y1=10.0, y2=10.0):
+    """Vertices and P1 triangles of the 2-D slope: a full block ``[0, x1+x2+x3] x [0, y1]``
+    under a trapezoid whose right edge runs from ``(x1+x2, y1)`` to ``(x1, y1+y2)``.
+    Every cell is split into ``(ll, lr, ul)`` and ``(ur, ul, lr)``; lower block first."""
+    nx12, nx3, ny1, ny2 = slope_counts(h, x1, x2, x3, y1, y2)
+    nx = nx12 + nx3
+    cx = np.concatenate((np.linspace(0.0, x1 + x2, nx12 + 1), np.linspace(x1 + x2, x1 + x2 + x3, nx3 + 1)[1:]))
+    cy = np.concatenate((np.linspace(0.0, y1, ny1 + 1), np.linspace(y1, y1 + y2, ny2 + 1)[1:]))
+    ids = {}
+    pts = []
+    for j in range(ny1 + 1):
+        for i in range(nx + 1):
+            ids[(i, j)] = len(pts)
+            pts.append((cx[i], cy[j]))
+    for j in range(ny1 + 1, ny1 + ny2 + 1):
+        xmax = x1 + x2 * (y1 + y2 - cy[j]) / y2
+        lx = np.linspace(0.0, xmax, nx12 + 1)
+        for i in range(nx12 + 1):
+            ids[(i, j)] = len(pts)
+            pts.append((lx[i], cy[j]))
+    tris = []
+    for (j0, j1, ni) in ((0, ny1, nx), (ny1, ny1 + ny2, nx12)):
+        for j in range(j0, j1):
+            for i in range(ni):
+                ll, lr, ul, ur = ids[(i, j)], ids[(i + 1, j)], ids[(i, j + 1)], ids[(i + 1, j + 1)]
+                tris.append((ll, lr, ul))
+                tris.append((ur, ul, lr))
+    return np.asarray(pts, dtype=np.float64), np.asarray(tris, dtype=np.int64)
+
+
+def lagrange_points(degree):
+    """Equispaced Lagrange points on the reference triangle, ordered vertices,
+    then edges (edge 0 = v1-v2, edge 1 = v0-v2, edge 2 = v0-v1, each from its
+    first to its second vertex), then interior points (x fastest)."""
+    k = int(degree)
+    v = [(0.0, 0.0), (1.0, 0.0), (0.0, 1.0)]
+    pts = list(v)
+    for (a, b) in ((1, 2), (0, 2), (0, 1)):
+        for t in range(1, k):
+            s = t / k
+            pts.append((v[a][0] + s * (v[b][0] - v[a][0]), v[a][1] + s * (v[b][1] - v[a][1])))
+    for j in range(1, k):
+        for i in range(1, k - j):
+            pts.append((i / k, j / k))
+    return np.asarray(pts, dtype=np.float64)
+
+
+def lagrange_tabulate(degree, xi):
+    """Values and reference gradients of the equispaced Lagrange basis at ``xi`` (2, nq)."""
+    pts = lagrange_points(degree)
+    k = int(degree)
+    mons = [(i, j) for j in range(k + 1) for i in range(k + 1 - j)]
+    V = np.array([[x ** i * y ** j for (i, j) in mons] for (x, y) in pts])
+    coef = np.linalg.inv(V)  # column a = monomial coefficients of basis a
+    x, y = xi[0], xi[1]
+    M = np.array([x ** i * y ** j for (i, j) in mons])
+    Mx = np.array([i * x ** max(i - 1, 0) * y ** j if i > 0 else 0 * x for (i, j) in mons])
+    My = np.array([j * x ** i * y ** max(j - 1, 0) if j > 0 else 0 * y for (i, j) in mons])
+    return coef.T @ M, coef.T @ Mx, coef.T @ My
+
+
+def gauss_jacobi_triangle(n):
+    """Collapsed (Duffy) Gauss-Jacobi rule with ``n*n`` points, exact to degree 2n-1
+    on the reference triangle (area 1/2)."""
+    from scipy.special import roots_jacobi
+
+    a, wa = roots_jacobi(n, 1.0, 0.0)   # weight (1 - t) on [-1, 1]
+    b, wb = roots_jacobi(n, 0.0, 0.0)
+    s = (a + 1.0) / 2.0                  # collapsed coordinate
+    t = (b + 1.0) / 2.0
+    X, Y, W = [], [], []
+    for i in range(n):
+        for j in range(n):
+            X.append(t[j] * (1.0 - s[i]))
+            Y.append(s[i])
+            W.append(wa[i] * wb[j] / 8.0)
+    return np.array([X, Y]), np.array(W)
+
+
+def slope_quadrature(degree):
+    if degree == 2:
+        return P2_QUAD_XI.copy(), P2_QUAD_W.copy()
+    if degree == 1:
+        return np.array([[1.0 / 3.0], [1.0 / 3.0]]), np.array([0.5])
+    return gauss_jacobi_triangle(degree + 1)  # degree 2*deg+1 exactness
+
+
+def same_mesh_lagrange(macro_nodes, macro_elems, degree, decimals=12):
+    """Pk nodes on every macro triangle, shared nodes merged by rounded coordinates
+    in element order (the numbering rule of the reference's same-mesh builder)."""
+    ref = lagrange_points(degree)
+    lookup = {}
+    coords = []
+    elems = np.zeros((macro_elems.shape[0], ref.shape[0]), dtype=np.int64)
+    v = macro_nodes[macro_elems]
+    for e in range(macro_elems.shape[0]):
+        p0, p1, p2 = v[e, 0], v[e, 1], v[e, 2]
+        for a, (xi, eta) in enumerate(ref):
+            p = (1.0 - xi - eta) * p0 + xi * p1 + eta * p2
+            key = (round(float(p[0]), decimals), round(float(p[1]), decimals))
+            nid = lookup.get(key)
+            if nid is None:
+                nid = len(coords)
+                lookup[key] = nid
+                coords.append(p)
+            elems[e, a] = nid
+    return np.asarray(coords, dtype=np.float64), elems
+
+
+def affine_triangle_geometry(nodes, elems_scalar):
+    """Inverse Jacobian (row-major ``[dxi/dx, dxi/dy, deta/dx, deta/dy]``) and
+    ``|det J|`` of the affine map of every triangle (vertices = first 3 nodes)."""
+    v = nodes[elems_scalar[:, :3]]
+    j11 = v[:, 1, 0] - v[:, 0, 0]
+    j12 = v[:, 1, 1] - v[:, 0, 1]
+    j21 = v[:, 2, 0] - v[:, 0, 0]
+    j22 = v[:, 2, 1] - v[:, 0, 1]
+    det = j11 * j22 - j12 * j21
+    # grads = inv @ [dhat1; dhat2] with inv = [[j22, -j12], [-j21, j11]] / det
+    inv = np.stack((j22 / det, -j12 / det, -j21 / det, j11 / det), axis=1)
+    return inv, np.abs(det)
+
+
+def davis_b_reduction(c0, phi_deg, psi_deg, lam):
+    """Davis-B strength reduction: reduced cohesion and friction angle (degrees)."""
+    if lam <= 0.0:
+        raise ValueError("lambda must be positive")
+    phi, psi = math.radians(phi_deg), math.radians(psi_deg)
+    c01 = c0 / lam
+    phi1 = math.atan(math.tan(phi) / lam)
+    psi1 = math.atan(math.tan(psi) / lam)
+    beta = math.cos(phi1) * math.cos(psi1) / (1.0 - math.sin(phi1) * math.sin(psi1))
+    return beta * c01, math.degrees(math.atan(beta * math.tan(phi1)))
+
+
+def slope_problem(*, level=None, h=None, degree=4, E=2.0e4, nu=0.49, c0=6.0, phi_deg=45.0, psi_deg=0.0,
+                  gamma=20.0, lam=1.0, with_elem_B=False):
+    """Homogeneous slope, plane strain, Pk same-mesh elements, Davis-B reduced strength."""
+    if h is None:
+        h = SLOPE_LEVEL_TO_H[int(level)]
+    macro_nodes, macro_elems = slope_macro_mesh(h)
+    nodes, es = same_mesh_lagrange(macro_nodes, macro_elems, degree)
+    xi, wq = slope_quadrature(degree)
+    hatp, dh1, dh2 = lagrange_tabulate(degree, xi)      # (n_p, nq)
+    inv, det = affine_triangle_geometry(nodes, es)
+    n_nodes = nodes.shape[0]
+    xmax = float(np.max(nodes[:, 0])) - 1.0e-9
+    q_mask = np.zeros((n_nodes, 2), dtype=bool)
+    q_mask[:, 0] = (nodes[:, 0] > 0.0) & (nodes[:, 1] > 0.0) & (nodes[:, 0] < xmax)
+    q_mask[:, 1] = nodes[:, 1] > 0.0
+    freedofs = np.arange(2 * n_nodes, dtype=np.int64).reshape(n_nodes, 2)[q_mask]
+    qw = det[:, None] * wq[None, :]                       # (E, nq)
+    # gravity load f_a = sum_q w_q phi_a(q) (0, -gamma)
+    force = np.zeros(2 * n_nodes)
+    np.add.at(force, 2 * es + 1, -gamma * (qw @ hatp.T))
+    coh, phi = davis_b_reduction(c0, phi_deg, psi_deg, lam)
+    params = {
+        "nodes": nodes, "elems_scalar": es, "elems": expand_connectivity_to_dofs(es, 2),
+        "freedofs": freedofs, "q_mask": q_mask, "u_0": np.zeros(2 * n_nodes), "force": force,
+        "inv_jac": inv, "det_j": det, "quad_xi": xi, "quad_w": wq,
+        "dhat1": dh1.T.copy(), "dhat2": dh2.T.copy(), "hatp": hatp.T.copy(),   # (nq, n_p)
+        "quad_weight": qw, "eps_p_old": np.zeros((es.shape[0], wq.size, 3)),
+        "E": float(E), "nu": float(nu), "phi_deg": float(phi), "cohesion": float(coh),
+        "c0": float(c0), "phi0_deg": float(phi_deg), "psi_deg": float(psi_deg), "gamma": float(gamma),
+        "lambda": float(lam), "reg": 1.0e-12, "degree": int(degree), "h": float(h),
+    }
+    if with_elem_B:
+        params["elem_B"] = slope_elem_B(params)
+    return params
+
+
+def slope_elem_B(params):
+    """Reference-layout strain operators ``elem_B (E, nq, 3, 2 n_p)``:
+    rows (eps_xx, eps_yy, gamma_xy), interleaved (u_x, u_y) per node."""
+    inv = params["inv_jac"]
+    d1, d2 = params["dhat1"], params["dhat2"]            # (nq, n_p)
+    gx = inv[:, 0, None, None] * d1[None] + inv[:, 1, None, None] * d2[None]
+    gy = inv[:, 2, None, None] * d1[None] + inv[:, 3, None, None] * d2[None]
+    E, nq, n_p = gx.shape
+    B = np.zeros((E, nq, 3, 2 * n_p))
+    B[:, :, 0, 0::2] = gx
+    B[:, :, 1, 1::2] = gy
+    B[:, :, 2, 0::2] = gy
+    B[:, :, 2, 1::2] = gx
+    return B

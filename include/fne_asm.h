@@ -119,11 +119,17 @@ typedef struct {
   const int64_t* owned_cols;    /* [nnz] reordered column ids                 */
   const double* energy_weights; /* [n_elem] 0/1, or NULL = 1 where any free   */
   int32_t nq;                   /* quadrature points (Mohr-Coulomb)           */
-  /* family element arrays, float64, reference layouts:
+  /* family element arrays, float64:
    *   p-Laplace / GL : e0 = dvx [E*3], e1 = dvy [E*3], e2 = vol [E]
    *   Neo-Hookean    : e0 = dphix [E*4], e1 = dphiy, e2 = dphiz, e3 = vol [E]
-   *   Mohr-Coulomb   : e0 = elem_B [E*nq*3*n], e1 = quad_weight [E*nq],
-   *                    e2 = eps_p_old [E*nq*3]                               */
+   *   Mohr-Coulomb   : affine form of the reference's elem_B / quad_weight
+   *                    (elem_B[e,q] = rows (xx, yy, xy) of the basis
+   *                    gradients J_e^-T grad(phi_a)(xi_q); quad_weight[e,q]
+   *                    = |det J_e| w_q):
+   *                    e0 = J_e^-1 row-major [E*4], e1 = |det J_e| [E],
+   *                    e2 = eps_p_old [E*nq*3] or NULL (zero),
+   *                    e3 = reference tables [dhat1 (nq*np) | dhat2 (nq*np) | w (nq)],
+   *                    npe = np (3, 6 or 15), block_size = 2, nq = 1, 7 or 25 */
   const double* e0;
   const double* e1;
   const double* e2;

@@ -93,8 +93,14 @@ def mc_elastic_tensors(E, nu):
 
 
 def mc_energy_density(strain, eps_p_old, E, nu, phi_deg, cohesion, reg):
-    """``jax_energy.py:45-108`` for ONE quadrature point.  ``lax.cond`` becomes a
-    select on both branches (which is what ``vmap`` of ``lax.cond`` does)."""
+    """``jax_energy.py:45-108`` for ONE quadrature point.
+
+    ``lax.cond`` under ``vmap`` becomes a select over both branches; the
+    plastic branch is evaluated on safe inputs where the elastic branch is
+    selected (and vice versa for the line/apex choice), so the autodiff of the
+    branch that is NOT taken cannot inject ``0 * NaN`` (the isotropic trial
+    stress makes ``atan2(0, 0)`` non-differentiable).
+    """
     C, S = mc_elastic_tensors(E, nu)
     eps_e = strain - eps_p_old
     sig_tr = C @ eps_e
@@ -109,6 +115,7 @@ def mc_energy_density(strain, eps_p_old, E, nu, phi_deg, cohesion, reg):
     beta = 1.0 - math.sin(phi)
     kappa = 2.0 * cohesion * math.cos(phi)
     f_tr = alpha * s1 - beta * s2 - kappa
+    elastic = f_tr <= 0.0
 
     psi_el = sig_tr @ eps_e - 0.5 * sig_tr @ (S @ sig_tr)
 
@@ -127,12 +134,15 @@ def mc_energy_density(strain, eps_p_old, E, nu, phi_deg, cohesion, reg):
     s2p = torch.where(line, s2_line, torch.full_like(s2_line, s_apex))
     mp = 0.5 * (s1p + s2p)
     rp = 0.5 * (s1p - s2p)
-    two_theta = torch.atan2(2.0 * txy, sxx - syy)
+    # direction of the trial stress; (1, 0) stands in where the branch is unused
+    dd = torch.where(elastic, torch.ones_like(d), sxx - syy)
+    tt = torch.where(elastic, torch.zeros_like(txy), 2.0 * txy)
+    two_theta = torch.atan2(tt, dd)
     sig = torch.stack(
         (mp + rp * torch.cos(two_theta), mp - rp * torch.cos(two_theta), rp * torch.sin(two_theta))
     )
     psi_pl = sig @ eps_e - 0.5 * sig @ (S @ sig)
-    return torch.where(f_tr <= 0.0, psi_el, psi_pl)
+    return torch.where(elastic, psi_el, psi_pl)
 
 
 def mc_elastic_density(strain, eps_p_old, E, nu):

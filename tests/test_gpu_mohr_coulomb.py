@@ -1,0 +1,108 @@
+"""Plane-strain Mohr-Coulomb kernels (P2 / P4 slope) vs the CPU oracle, through the C ABI.
+
+FP64 mode within 1e-12 relative (energies vs the sum of |element energy|,
+gradient / Hessian vs the largest entry); FP32 mode within 2e-5.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle.assembler import OracleAssembler
+from fenics_nonlinear_energies_b200 import _lib, meshes
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.abs(a - b).max(initial=0.0) / max(np.abs(b).max(initial=0.0), 1e-300)
+
+
+def _pair(params, **kw):
+    from fenics_nonlinear_energies_b200.assembler import SlopeStabilityCudaAssembler
+
+    gpu = SlopeStabilityCudaAssembler(params, **kw)
+    okw = {}
+    params = dict(params)
+    if kw.get("constitutive_mode") == "elastic":
+        params["elastic"] = True
+    ref = OracleAssembler("mc", params, block_size=2)
+    return gpu, ref
+
+
+def _abs_scale(ref, u):
+    from oracle import energies
+
+    v = ref.v_local(u)[ref.local.elems_local_np]
+    e, _, _ = energies.element_derivatives("mc", v, ref.elem_data, ref.params, want_hessian=False)
+    return float(np.abs(e).sum() + abs(ref.f_owned @ np.asarray(u)[: ref.f_owned.size]))
+
+
+@pytest.mark.parametrize("degree,level", [(2, 1), (4, 1), (2, 2)])
+@pytest.mark.parametrize("scale", [0.0, 0.05])
+def test_mc_fp64_matches_oracle(degree, level, scale):
+    params = meshes.slope_problem(level=level, degree=degree, lam=1.2, with_elem_B=True)
+    gpu, ref = _pair(params)
+    u = scale * np.random.default_rng(degree + level).standard_normal(gpu.layout.n_free)
+    e_ref, g_ref, h_ref = ref.all_in_one(u)
+    e, g, h = gpu.eval(torch.as_tensor(u, device="cuda"), 7)
+    assert abs(float(e.item()) - e_ref) <= 1e-12 * max(_abs_scale(ref, u), 1.0)
+    assert _rel(g.cpu().numpy(), g_ref) <= 1e-12
+    assert _rel(h.cpu().numpy(), h_ref) <= 1e-12
+    assert gpu.info["kernel_variant"] == 5
+
+
+def test_mc_plastic_points_present():
+    """The displacement scale used above drives part of the quadrature points plastic."""
+    from oracle import energies
+
+    params = meshes.slope_problem(level=1, degree=4, lam=1.2, with_elem_B=True)
+    ref = OracleAssembler("mc", params, block_size=2)
+    u = 0.05 * np.random.default_rng(5).standard_normal(ref.layout.n_free)
+    v = ref.v_local(u)[ref.local.elems_local_np]
+    strain = np.einsum("eqij,ej->eqi", ref.elem_data["elem_B"], v)
+    el = energies.element_derivatives("mc", v, ref.elem_data, dict(params, elastic=True), want_hessian=False)[0]
+    pl = energies.element_derivatives("mc", v, ref.elem_data, params, want_hessian=False)[0]
+    assert np.mean(np.abs(el - pl) > 1e-12 * np.abs(el)) > 0.1
+    assert strain.shape[1] == 25
+
+
+def test_mc_fp32():
+    params = meshes.slope_problem(level=1, degree=4, lam=1.2, with_elem_B=True)
+    gpu, ref = _pair(params, precision="fp32", hess_dtype=torch.float32)
+    u = 0.05 * np.random.default_rng(9).standard_normal(gpu.layout.n_free)
+    e_ref, g_ref, h_ref = ref.all_in_one(u)
+    e, g, h = gpu.eval(torch.as_tensor(u, device="cuda"), 7)
+    assert h.dtype == torch.float32
+    assert abs(float(e.item()) - e_ref) <= 1e-5 * _abs_scale(ref, u)
+    assert _rel(g.cpu().numpy(), g_ref) <= 1e-4
+    assert _rel(h.double().cpu().numpy(), h_ref) <= 2e-5
+
+
+def test_elastic_tangent_equals_mc_tangent_at_zero():
+    """tests/test_slope_stability_petsc.py:559-585 of the reference: at u = 0 the
+    elastic and the Mohr-Coulomb tangents coincide."""
+    params = meshes.slope_problem(level=2, degree=2, lam=1.0)
+    from fenics_nonlinear_energies_b200.assembler import SlopeStabilityCudaAssembler
+
+    mc = SlopeStabilityCudaAssembler(params)
+    el = SlopeStabilityCudaAssembler(params, constitutive_mode="elastic")
+    u = torch.zeros(mc.layout.n_free, dtype=torch.float64, device="cuda")
+    h_mc = mc.eval(u, _lib.FNE_HESS)[2].clone()
+    h_el = el.eval(u, _lib.FNE_HESS)[2].clone()
+    np.testing.assert_array_equal(mc.layout.owned_rows, el.layout.owned_rows)
+    assert torch.allclose(h_mc, h_el, rtol=1e-10, atol=0)
+
+
+def test_mc_energy_only_and_repeatability():
+    params = meshes.slope_problem(level=2, degree=4, lam=1.1)
+    from fenics_nonlinear_energies_b200.assembler import SlopeStabilityCudaAssembler
+
+    gpu = SlopeStabilityCudaAssembler(params)
+    u = torch.as_tensor(0.03 * np.random.default_rng(1).standard_normal(gpu.layout.n_free), device="cuda")
+    e1, g1, h1 = [t.clone() for t in gpu.eval(u, 7)]
+    e2, g2, h2 = [t.clone() for t in gpu.eval(u, 7)]
+    assert torch.equal(h1, h2) and torch.equal(g1, g2) and torch.equal(e1, e2)
+    e_only = gpu.eval(u, _lib.FNE_ENERGY)[0].clone()
+    assert torch.equal(e_only, e1)
