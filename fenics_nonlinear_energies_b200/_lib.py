@@ -87,6 +87,14 @@ def _load():
         "fne_destroy": (C.c_int, [vp]),
         "fne_energy_p1tri_noalloc": (C.c_int, [C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp, _f64p, vp,
                                                C.c_int64, C.c_int64, vp, vp]),
+        "fne_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int64, C.c_int64, vp, C.c_int64, C.c_int64,
+                                    vp, C.c_int64, C.c_float, vp]),
+        "fne_mlp_bias_act": (C.c_int, [C.c_int64, C.c_int, vp, vp, C.c_int, vp, vp, vp]),
+        "fne_mlp_act_bwd": (C.c_int, [C.c_int64, vp, vp, C.c_int, vp, vp, vp]),
+        "fne_mlp_colsum": (C.c_int, [C.c_int64, C.c_int, vp, vp, vp]),
+        "fne_mlp_adam": (C.c_int, [C.c_int64, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                   vp, vp]),
+        "fne_mlp_cast_bf16": (C.c_int, [C.c_int64, vp, vp, vp]),
         "fne_last_error": (C.c_char_p, []),
         "fne_version": (C.c_char_p, []),
     }

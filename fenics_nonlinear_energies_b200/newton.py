@@ -1,0 +1,246 @@
+"""Device-resident Newton driver used for end-to-end runs on one GPU.
+
+The reference's driver (``src/core/petsc/minimizers.py``) stays the production
+caller of the assembler; this module restates the parts of it the GPU runs
+need so that Newton iterations can be counted without PETSc:
+
+* ``golden_section_search`` -- ``minimizers.py:14-61`` (same bracket updates,
+  best-point tracking and final midpoint evaluation);
+* ``repair_linesearch_interval`` -- ``minimizers.py:74-127`` (bisect
+  non-finite interval ends back toward the finite centre);
+* ``newton`` -- the golden-section branch of ``minimizers.py:181-1038``:
+  gradient, stop on ``||g|| < max(tolg, tolg_rel * ||g_0||)``, linear solve
+  of ``H p = -g``, line search on ``[a, b]``, accept a step only if it lowers
+  the energy, optional stop on the energy change.
+
+The linear solve is Jacobi-preconditioned conjugate gradients on the
+assembled owned COO values (cuSPARSE SpMV through torch); CG stops at a
+negative-curvature direction and returns the last iterate (or the steepest
+descent direction), which keeps the Newton direction a descent direction for
+the non-convex Ginzburg-Landau energy.
+"""
+
+from __future__ import annotations
+
+import math
+import time
+import warnings
+
+import numpy as np
+import torch
+
+from fenics_nonlinear_energies_b200 import _lib
+
+
+def golden_section_search(f, a, b, tol):
+    """Minimise ``f`` on ``[a, b]``; returns ``(alpha, n_evals)``."""
+    gamma = 0.5 + math.sqrt(5.0) / 2.0
+    an, bn = float(a), float(b)
+    fan, fbn = f(an), f(bn)
+    dn = (bn - an) / gamma + an
+    cn = an + bn - dn
+    fcn, fdn = f(cn), f(dn)
+    n_evals = 4
+    best_alpha, best_value = an, fan
+    for alpha, value in ((bn, fbn), (cn, fcn), (dn, fdn)):
+        if value < best_value:
+            best_alpha, best_value = alpha, value
+    while bn - an > tol:
+        if fcn < fdn:
+            bn = dn
+            dn, cn = cn, an + bn - cn
+            fdn, fcn = fcn, f(cn)
+            for alpha, value in ((dn, fdn), (cn, fcn)):
+                if value < best_value:
+                    best_alpha, best_value = alpha, value
+        else:
+            an = cn
+            cn, dn = dn, an + bn - dn
+            fcn, fdn = fdn, f(dn)
+            for alpha, value in ((cn, fcn), (dn, fdn)):
+                if value < best_value:
+                    best_alpha, best_value = alpha, value
+        n_evals += 1
+    mid = 0.5 * (an + bn)
+    fmid = f(mid)
+    n_evals += 1
+    if fmid < best_value:
+        best_alpha = mid
+    return float(best_alpha), n_evals
+
+
+def repair_linesearch_interval(f, a, b, center=0.0, center_value=None, tol=1e-6, max_bisect=60):
+    """Shrink non-finite interval ends toward the finite centre; ``(a, b, n_evals, repaired)``."""
+    n_evals = 0
+    repaired = False
+    if center_value is None:
+        center_value = f(center)
+        n_evals += 1
+    if not math.isfinite(center_value):
+        return a, b, n_evals, repaired
+    tol = max(float(tol), 1e-12)
+
+    def side(bound, sign):
+        nonlocal n_evals, repaired
+        if (sign < 0 and not bound < center) or (sign > 0 and not bound > center):
+            return bound
+        fb = f(bound)
+        n_evals += 1
+        if math.isfinite(fb):
+            return bound
+        repaired = True
+        good, bad = center, bound
+        for _ in range(max_bisect):
+            mid = 0.5 * (good + bad)
+            fm = f(mid)
+            n_evals += 1
+            if math.isfinite(fm):
+                good = mid
+            else:
+                bad = mid
+            if abs(bad - good) <= tol:
+                break
+        return good
+
+    return side(float(a), -1.0), side(float(b), 1.0), n_evals, repaired
+
+
+class CsrOperator:
+    """Owned COO values of an assembler viewed as a CSR matrix in reordered numbering."""
+
+    def __init__(self, assembler):
+        rows = np.asarray(assembler.layout.owned_rows, dtype=np.int64) - assembler.layout.lo
+        cols = np.asarray(assembler.layout.owned_cols, dtype=np.int64)
+        n = assembler.n_owned
+        order = np.argsort(rows, kind="stable")
+        dev = assembler.device
+        self.order = torch.as_tensor(order, device=dev)
+        counts = np.bincount(rows, minlength=n)
+        crow = np.concatenate(([0], np.cumsum(counts)))
+        self.crow = torch.as_tensor(crow, dtype=torch.int64, device=dev)
+        self.col = torch.as_tensor(cols[order], dtype=torch.int64, device=dev)
+        diag_pos = np.full(n, -1, dtype=np.int64)
+        is_diag = rows == cols
+        diag_pos[rows[is_diag]] = np.flatnonzero(is_diag)
+        self.diag_pos = torch.as_tensor(np.maximum(diag_pos, 0), device=dev)
+        self.has_diag = torch.as_tensor(diag_pos >= 0, device=dev)
+        self.n = n
+        self.A = None
+        self.dinv = None
+
+    def update(self, values):
+        v = values.double()
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", UserWarning)  # beta-state / invariant-check notices
+            self.A = torch.sparse_csr_tensor(self.crow, self.col, v.index_select(0, self.order),
+                                             size=(self.n, self.n), check_invariants=False)
+        d = torch.where(self.has_diag, v.index_select(0, self.diag_pos), torch.ones_like(v[: self.n]))
+        d = torch.where(d.abs() > 0, d.abs(), torch.ones_like(d))
+        self.dinv = 1.0 / d
+
+    def matvec(self, x):
+        return (self.A @ x.unsqueeze(1)).squeeze(1)
+
+
+def pcg(op, b, rtol=1e-3, maxit=500):
+    """Jacobi-preconditioned CG; stops at negative curvature.  Returns ``(x, iterations)``."""
+    x = torch.zeros_like(b)
+    r = b.clone()
+    z = op.dinv * r
+    p = z.clone()
+    rz = torch.dot(r, z)
+    bnorm = float(torch.linalg.vector_norm(b))
+    if bnorm == 0.0:
+        return x, 0
+    for it in range(1, maxit + 1):
+        Ap = op.matvec(p)
+        pAp = float(torch.dot(p, Ap))
+        if not (pAp > 0.0):
+            return (x if it > 1 else b.clone()), it
+        alpha = float(rz) / pAp
+        x.add_(p, alpha=alpha)
+        r.add_(Ap, alpha=-alpha)
+        if float(torch.linalg.vector_norm(r)) <= rtol * bnorm:
+            return x, it
+        z = op.dinv * r
+        rz_new = torch.dot(r, z)
+        p.mul_(float(rz_new) / float(rz)).add_(z)
+        rz = rz_new
+    return x, maxit
+
+
+def newton(assembler, x0, *, tolg=0.0, tolg_rel=1e-6, tolf=0.0, maxit=100, linesearch_interval=(-0.5, 2.0),
+           linesearch_tol=1e-3, ksp_rtol=1e-3, ksp_max_it=500, verbose=False):
+    """Minimise the assembler's energy from ``x0`` (device tensor of the owned reordered DOFs).
+
+    Returns ``(x, info)`` with ``info["iterations"]`` the number of Newton
+    steps taken, ``info["converged"]``, the final energy and gradient norm.
+    """
+    dev = assembler.device
+    x = torch.as_tensor(x0, dtype=torch.float64, device=dev).clone()
+    op = CsrOperator(assembler)
+    flags_eg = _lib.FNE_ENERGY | _lib.FNE_GRAD
+    e_buf = torch.empty(1, dtype=torch.float64, device=dev)
+    g = torch.empty(assembler.n_owned, dtype=torch.float64, device=dev)
+    x_trial = torch.empty_like(x)
+
+    def energy_at(xv):
+        val = float(assembler.eval(xv, _lib.FNE_ENERGY, energy=e_buf)[0].item())
+        return val if math.isfinite(val) else math.inf
+
+    t0 = time.perf_counter()
+    assembler.eval(x, flags_eg, energy=e_buf, grad=g)
+    fx = float(e_buf.item())
+    g0 = None
+    history = []
+    message = "Maximum number of iterations reached"
+    nit = 0
+    for _ in range(maxit):
+        if not math.isfinite(fx):
+            message = "Non-finite energy"
+            break
+        assembler.eval(x, _lib.FNE_GRAD, grad=g)
+        normg = float(torch.linalg.vector_norm(g))
+        if not math.isfinite(normg):
+            message = "Non-finite gradient norm"
+            break
+        if g0 is None:
+            g0 = normg
+        target = max(tolg, tolg_rel * g0)
+        if normg < target:
+            message = "Gradient norm converged"
+            break
+        nit += 1
+        assembler.eval(x, _lib.FNE_HESS)
+        op.update(assembler.owned_values)
+        p, ksp_its = pcg(op, -g, rtol=ksp_rtol, maxit=ksp_max_it)
+
+        def f_alpha(alpha):
+            torch.add(x, p, alpha=alpha, out=x_trial)
+            return energy_at(x_trial)
+
+        a, b, n_rep, _ = repair_linesearch_interval(f_alpha, *linesearch_interval, center=0.0, center_value=fx,
+                                                    tol=linesearch_tol)
+        alpha, n_ls = golden_section_search(f_alpha, a, b, linesearch_tol)
+        f_new = f_alpha(alpha)
+        accepted = math.isfinite(f_new) and f_new < fx
+        dE = fx - f_new if accepted else 0.0
+        if accepted:
+            x.copy_(x_trial)
+            fx = f_new
+        history.append({"it": nit, "energy": fx, "grad_norm": normg, "alpha": alpha, "ksp_its": ksp_its,
+                        "ls_evals": n_rep + n_ls + 1, "accepted": accepted})
+        if verbose:
+            print(f"it={nit} J={fx:.10g} |g|={normg:.3e} alpha={alpha:.4f} ksp={ksp_its}", flush=True)
+        if not accepted:
+            message = "Line search made no progress"
+            break
+        if tolf > 0.0 and abs(dE) < tolf:
+            message = "Energy change converged"
+            break
+    assembler.eval(x, _lib.FNE_GRAD, grad=g)
+    normg = float(torch.linalg.vector_norm(g))
+    info = {"iterations": nit, "message": message, "energy": fx, "grad_norm": normg, "grad_norm0": g0,
+            "converged": g0 is not None and normg < max(tolg, tolg_rel * g0) * (1.0 + 1e-12),
+            "time_s": time.perf_counter() - t0, "history": history}
+    return x, info

@@ -211,6 +211,29 @@ int fne_energy_p1tri_noalloc(int32_t family, int64_t n_elem, const int32_t* code
                              const double* dirichlet, const double* params, const double* rhs,
                              int64_t n_owned, int64_t lo, double* energy, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Learned Newton warm start (no counterpart in the reference).  Kernels of a
+ * small MLP over nodal features: BF16 operands, FP32 accumulation / master
+ * weights.  All pointers are device pointers; BF16 arrays are passed as void*.
+ * ------------------------------------------------------------------------- */
+/* C[m, n] = sum_k A(m, k) B(k, n) + beta C[m, n], A(m, k) = A[m*sam + k*sak],
+ * B(k, n) = B[k*sbk + n*sbn] (BF16), C row-major with leading dimension ldc
+ * (FP32).  Tensor cores (mma.sync m16n8k16), 64x64 tiles. */
+int fne_gemm_bf16(int M, int N, int K, const void* A, int64_t sam, int64_t sak, const void* B, int64_t sbk,
+                  int64_t sbn, float* C, int64_t ldc, float beta, void* stream);
+/* Z += bias (per column); H = silu(Z) (act = 1) or Z (act = 0); H32 / H16 may be NULL. */
+int fne_mlp_bias_act(int64_t rows, int cols, float* Z, const float* bias, int act, float* H32, void* H16,
+                     void* stream);
+/* dZ = dH * silu'(Z) (act = 1) or dH (act = 0); dZ32 / dZ16 may be NULL. */
+int fne_mlp_act_bwd(int64_t n, const float* Z, const float* dH, int act, float* dZ32, void* dZ16, void* stream);
+/* out[c] = sum_r X[r, c] (FP64 accumulation, fixed order). */
+int fne_mlp_colsum(int64_t rows, int cols, const float* X, float* out, void* stream);
+/* One Adam step on FP32 parameters (bias-corrected with ``step`` >= 1);
+ * writes the BF16 copy p16 when it is not NULL. */
+int fne_mlp_adam(int64_t n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
+                 int step, void* p16, void* stream);
+int fne_mlp_cast_bf16(int64_t n, const float* x, void* y, void* stream);
+
 const char* fne_last_error(void);
 const char* fne_version(void);
 

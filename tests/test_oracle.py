@@ -102,3 +102,27 @@ def test_oracle_assembler_consistency(numbering):
     hv_fd = (asm.gradient_fn(u + h * d) - asm.gradient_fn(u - h * d)) / (2 * h)
     np.testing.assert_allclose(A @ d, hv_fd, rtol=1e-5, atol=1e-7)
     assert abs(A - A.T).max() < 1e-14
+
+
+def test_golden_section_restatement():
+    from fenics_nonlinear_energies_b200.newton import golden_section_search, repair_linesearch_interval
+
+    calls = []
+
+    def f(a):
+        calls.append(a)
+        return (a - 0.7) ** 2
+
+    alpha, n = golden_section_search(f, -0.5, 2.0, 1e-3)
+    assert abs(alpha - 0.7) < 1e-3 and n == len(calls)
+    # non-finite right end is bisected back toward the centre
+    g = lambda a: float("inf") if a > 1.0 else (a - 0.5) ** 2  # noqa: E731
+    a, b, _, repaired = repair_linesearch_interval(g, -0.5, 2.0, center=0.0, center_value=g(0.0), tol=1e-6)
+    assert repaired and a == -0.5 and 1.0 - 1e-5 < b <= 1.0
+
+
+def test_mlp_oracle_bf16_rounding():
+    from oracle.mlp import bf16_round
+
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, -2.5, 0.0], dtype=np.float32)
+    np.testing.assert_array_equal(bf16_round(x), [1.0, 1.0, 1.0 + 2 ** -7, -2.5, 0.0])
