@@ -1,12 +1,18 @@
 """Benchmark: fused energy + gradient + Hessian assembly, elements/s.
 
-Workload (one "step"): Ginzburg-Landau, eps = 0.01 on [-1, 1]^2, structured
-1024 x 1024 grid of P1 triangles (2,097,152 elements, 1,046,529 free DOFs,
-7,317,521 owned COO entries), u ~ U[-0.5, 0.5] from a fixed seed; FP32
-element gradients / Hessians (float32 COO values), FP64 energy reduction.
-One step = one fused E+grad+Hess pass over every element into the device
-gradient and the owned COO values (the reference's energy_fn + gradient_fn +
-assemble_hessian_element).
+Default workload (``--workload gl1024_fp32h``, one "step"): Ginzburg-Landau,
+eps = 0.01 on [-1, 1]^2, structured 1024 x 1024 grid of P1 triangles
+(2,097,152 elements, 1,046,529 free DOFs, 7,317,521 owned COO entries),
+u ~ U[-0.5, 0.5] from a fixed seed; FP32 element gradients / Hessians
+(float32 COO values), FP64 energy reduction.  One step = one fused
+E+grad+Hess pass over every element into the device gradient and the owned
+COO values (the reference's energy_fn + gradient_fn + assemble_hessian_element).
+
+Other workloads (same JSON line, same timing rules; ``--workload NAME``):
+p-Laplace 128x128 P1 (FP64, zero state), Ginzburg-Landau 1024^2 in FP64,
+the Neo-Hookean beam 160x8x8 hexes x 6 tets (FP64 and FP32 Hessian) and its
+320x16x16 refinement, and the plane-strain Mohr-Coulomb slope with P4 / P2
+triangles at h = 0.08 (203,000 elements).
 
 ``value``: device-resident inputs, CUDA events around each pass, L2 flushed
 (256 MiB write) between passes outside the timed events.
@@ -15,8 +21,10 @@ H2D of u from pinned memory, the pass, D2H of energy, gradient and COO values.
 
 Multi-GPU: every rank runs its own replica of the workload (weak scaling).
 ``--impl reference``: the CPU restatement of the reference path (the JAX
-element kernels + np.add.at scatter, restated in oracle/) on the host cores.
+element kernels + np.add.at scatter, restated in oracle/) on the host cores,
+on a bounded sample of the same workload family.
 """
+
 
 from __future__ import annotations
 
@@ -32,8 +40,6 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-GRID = 1024
-WORKLOAD = "ginzburg_landau_p1_1024x1024_fp32hess"
 
 
 def _peaks():
@@ -44,14 +50,12 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic_per_launch():
-    p = ROOT / "profiles" / "k_rows_tri_gl_fp32_traffic.json"
-    if p.exists():
-        try:
-            return float(json.loads(p.read_text())["dram_bytes_per_launch"])
-        except Exception:
-            return None
-    return None
+# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu
+# capture of the same workload (dram__bytes_read.sum + dram__bytes_write.sum),
+# with the profile summary that records it.  Keyed by (workload, kernel).
+NCU_TRAFFIC = {
+    ("gl1024_fp32h", "k_sweep_tri"): (213.2e6, "profiles/k_sweep_tri_gl1024_fp32.md"),
+}
 
 
 class ClockSampler:
@@ -144,25 +148,220 @@ def _max_over_ranks(x, world):
     return float(t.item())
 
 
-def cpu_port_baseline(grid=512, passes=3):
-    """The oracle (CPU restatement of the reference path) on a bounded sample."""
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+class Workload:
+    """One benchmark configuration.
+
+    ``build(rank)`` returns ``(assembler, u_owned_reordered)``;
+    ``conn_nodes`` / ``geom_values`` are the node-level connectivity entries
+    and the per-element geometry values one pass reads (algorithmic bytes);
+    ``sample()`` returns ``(family, oracle_kwargs, params, u, n_el, label)`` for
+    the bounded CPU restatement run.
+    """
+
+    def __init__(self, name, family, precision, hess_fp32, conn_nodes, geom_values, geom_bytes, has_rhs, desc,
+                 build, sample):
+        self.name, self.family, self.precision, self.hess_fp32 = name, family, precision, hess_fp32
+        self.conn_nodes, self.geom_values, self.geom_bytes, self.has_rhs = conn_nodes, geom_values, geom_bytes, has_rhs
+        self.desc, self.build, self.sample = desc, build, sample
+
+    @property
+    def dtype(self):
+        if self.precision == "fp32":
+            return "f32 (element grad/Hessian), f64 (energy)"
+        return "f64"
+
+
+def _reordered(asm, u_free):
+    import numpy as np
+
+    return np.ascontiguousarray(np.asarray(u_free, dtype=np.float64)[np.asarray(asm.layout.perm)])
+
+
+def twisted_beam_positions(params, theta):
+    """Deformed positions of the beam twisted about its axis by ``theta * x / L``
+    (the right face carries the full rotation of the load step)."""
+    import numpy as np
+
+    X = params["nodes2coord"]
+    a = theta * X[:, 0] / float(X[:, 0].max())
+    c, s = np.cos(a), np.sin(a)
+    return np.stack([X[:, 0], c * X[:, 1] + s * X[:, 2], -s * X[:, 1] + c * X[:, 2]], axis=1).ravel()
+
+
+def slope_state(params, amplitude=0.02):
+    """Smooth synthetic slope displacement (u_x, u_y) interleaved per node."""
+    import numpy as np
+
+    x, y = params["nodes"][:, 0], params["nodes"][:, 1]
+    ux = amplitude * 4.0 * (y / 20.0) * (x / 40.0) * (1.0 - x / 40.0)
+    uy = -amplitude * (y / 20.0) ** 2
+    return np.stack([ux, uy], axis=1).ravel()
+
+
+def _tri(kind, n, precision, seed_from_rank=True):
+    def build(rank):
+        import torch
+
+        from fenics_nonlinear_energies_b200 import meshes
+        from fenics_nonlinear_energies_b200.assembler import GLCudaAssembler, PLaplaceCudaAssembler
+
+        hd = torch.float32 if precision == "fp32" else torch.float64
+        if kind == "gl":
+            params, u0 = meshes.gl_problem(n=n, seed=rank)
+            asm = GLCudaAssembler(params, precision=precision, hess_dtype=hd)
+        else:
+            params, u0 = meshes.plaplace_problem(n=n, seed=None)
+            asm = PLaplaceCudaAssembler(params, precision=precision, hess_dtype=hd)
+        return asm, _reordered(asm, u0)
+
+    def sample():
+        from fenics_nonlinear_energies_b200 import meshes
+
+        m = min(n, 512)
+        if kind == "gl":
+            params, u0 = meshes.gl_problem(n=m, seed=0)
+        else:
+            params, u0 = meshes.plaplace_problem(n=m, seed=None)
+        return kind, {}, params, u0, 2 * m * m, f"{m}x{m} P1 grid"
+
+    return build, sample
+
+
+def _he(nx, ny, nz, precision, theta=4.0 * 3.141592653589793 / 24.0):
+    def build(rank):
+        import torch
+
+        from fenics_nonlinear_energies_b200 import meshes
+        from fenics_nonlinear_energies_b200.assembler import HECudaAssembler
+
+        params, _ = meshes.he_beam_problem(nx=nx, ny=ny, nz=nz)
+        hd = torch.float32 if precision == "fp32" else torch.float64
+        asm = HECudaAssembler(params, precision=precision, hess_dtype=hd)
+        pos = twisted_beam_positions(params, theta)
+        asm.update_dirichlet(pos)
+        return asm, _reordered(asm, pos[params["freedofs"]])
+
+    def sample():
+        from fenics_nonlinear_energies_b200 import meshes
+
+        sx = max(1, nx // 8)
+        params, _ = meshes.he_beam_problem(nx=sx, ny=ny, nz=nz)
+        pos = twisted_beam_positions(params, theta)
+        params = dict(params, u_0_ref=pos)
+        return "he", {"block_size": 3, "coordinate_key": "nodes2coord", "dirichlet_key": "u_0_ref"}, params, \
+            pos[params["freedofs"]], 6 * sx * ny * nz, f"{sx}x{ny}x{nz}-hex beam"
+
+    return build, sample
+
+
+def _mc(degree, h, precision):
+    def build(rank):
+        import torch
+
+        from fenics_nonlinear_energies_b200 import meshes
+        from fenics_nonlinear_energies_b200.assembler import SlopeStabilityCudaAssembler
+
+        params = meshes.slope_problem(h=h, degree=degree, lam=1.0)
+        hd = torch.float32 if precision == "fp32" else torch.float64
+        asm = SlopeStabilityCudaAssembler(params, precision=precision, hess_dtype=hd)
+        return asm, _reordered(asm, slope_state(params)[params["freedofs"]])
+
+    def sample():
+        from fenics_nonlinear_energies_b200 import meshes
+
+        params = meshes.slope_problem(level=3, degree=degree, lam=1.0, with_elem_B=True)
+        u = slope_state(params)[params["freedofs"]]
+        return "mc", {"block_size": 2}, params, u, int(params["elems_scalar"].shape[0]), \
+            f"slope h=1 P{degree}"
+
+    return build, sample
+
+
+WORKLOADS = {
+    "gl1024_fp32h": Workload(
+        "gl1024_fp32h", "gl", "fp32", True, 3, 7, 4, False,
+        "Ginzburg-Landau eps=0.01 on [-1,1]^2, 1024x1024 P1 triangles (2,097,152 elements), "
+        "u ~ U[-0.5,0.5] seeded; FP32 element grad/Hessian, FP64 energy", *_tri("gl", 1024, "fp32")),
+    "gl1024_fp64": Workload(
+        "gl1024_fp64", "gl", "fp64", False, 3, 7, 8, False,
+        "Ginzburg-Landau eps=0.01 on [-1,1]^2, 1024x1024 P1 triangles (2,097,152 elements), FP64",
+        *_tri("gl", 1024, "fp64")),
+    "plaplace128_fp64": Workload(
+        "plaplace128_fp64", "plaplace", "fp64", False, 3, 7, 8, True,
+        "p-Laplace p=3, f=-10, unit square 128x128 P1 triangles (32,768 elements), zero state, FP64",
+        *_tri("plaplace", 128, "fp64")),
+    "he160x8x8_fp64": Workload(
+        "he160x8x8_fp64", "he", "fp64", False, 4, 13, 8, False,
+        "Neo-Hookean beam [0,0.4]x[-0.01,0.01]^2, 160x8x8 hexes x 6 tets (61,440), E=10, nu=0.3, "
+        "state twisted by 4pi/24 (first load step), FP64", *_he(160, 8, 8, "fp64")),
+    "he160x8x8_fp32h": Workload(
+        "he160x8x8_fp32h", "he", "fp32", True, 4, 13, 4, False,
+        "Neo-Hookean beam 160x8x8 hexes x 6 tets (61,440), first load step, FP32 element grad/Hessian",
+        *_he(160, 8, 8, "fp32")),
+    "he320x16x16_fp64": Workload(
+        "he320x16x16_fp64", "he", "fp64", False, 4, 13, 8, False,
+        "Neo-Hookean beam 320x16x16 hexes x 6 tets (491,520), first load step, FP64", *_he(320, 16, 16, "fp64")),
+    "mc_p4_h0.08_fp64": Workload(
+        "mc_p4_h0.08_fp64", "mc", "fp64", False, 15, 5, 8, True,
+        "Mohr-Coulomb plane-strain slope 40x20 (height 10, 1:1), P4 triangles h=0.08 (203,000 elements), "
+        "c=6, phi=45 deg, E=2e4, nu=0.49, lambda=1 (Davis-B), 25-point rule, smooth synthetic state, FP64",
+        *_mc(4, 0.08, "fp64")),
+    "mc_p4_h0.08_fp32": Workload(
+        "mc_p4_h0.08_fp32", "mc", "fp32", True, 15, 5, 8, True,
+        "Mohr-Coulomb slope P4 h=0.08 (203,000 elements), FP32 element grad/Hessian", *_mc(4, 0.08, "fp32")),
+    "mc_p2_h0.08_fp64": Workload(
+        "mc_p2_h0.08_fp64", "mc", "fp64", False, 6, 5, 8, True,
+        "Mohr-Coulomb slope P2 h=0.08 (203,000 elements), 7-point rule, FP64", *_mc(2, 0.08, "fp64")),
+}
+DEFAULT_WORKLOAD = "gl1024_fp32h"
+
+KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri", 5: "k_mc_elem+k_mc_gather"}
+
+
+def algorithmic_bytes(w, asm, n_el):
+    """Bytes one pass must move: node-level connectivity (int32), per-element
+    geometry, the free state u (FP64), the load vector where the family has one,
+    the owned gradient write (FP64) and the owned COO value write."""
+    n_free = asm.layout.n_free
+    nnz = int(asm.owned_values.numel())
+    hb = 4 if w.hess_fp32 else 8
+    b = n_el * (4 * w.conn_nodes + w.geom_bytes * w.geom_values) + n_free * 8 + asm.n_owned * 8 + nnz * hb
+    if w.has_rhs:
+        b += asm.n_owned * 8
+    return b
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement (the oracle) on a bounded sample
+# ---------------------------------------------------------------------------
+def _oracle_sample(w, min_seconds=8.0, max_passes=5):
     import torch
 
     from oracle.assembler import OracleAssembler
-    from fenics_nonlinear_energies_b200 import meshes
 
-    params, u0 = meshes.gl_problem(n=grid, seed=0)
-    asm = OracleAssembler("gl", params)
-    asm.all_in_one(u0)  # warm-up
-    t = time.perf_counter()
-    for _ in range(passes):
-        asm.all_in_one(u0)
-    dt = (time.perf_counter() - t) / passes
-    n_el = 2 * grid * grid
-    return {"value": n_el / dt, "unit": "elements/s", "cores": int(torch.get_num_threads()), "kind": "port",
-            "sample": f"GL {grid}x{grid} P1 grid ({n_el} elements), {passes} fused E+grad+Hess passes, "
-                      "torch.func float64 autodiff + np.add.at scatter",
-            "seconds_per_pass": dt}
+    family, okw, params, u, n_el, label = w.sample()
+    asm = OracleAssembler(family, params, **okw)
+    u = u[asm.layout.perm]
+    return asm, u, n_el, label, min_seconds, max_passes, int(torch.get_num_threads())
+
+
+def cpu_port_baseline(w):
+    """The oracle (CPU restatement of the reference path) on a bounded sample."""
+    asm, u, n_el, label, min_s, max_p, cores = _oracle_sample(w)
+    asm.all_in_one(u)  # warm-up
+    times = []
+    while len(times) < max_p and sum(times) < min_s:
+        t = time.perf_counter()
+        asm.all_in_one(u)
+        times.append(time.perf_counter() - t)
+    dt = sum(times) / len(times)
+    return {"value": n_el / dt, "unit": "elements/s", "cores": cores, "kind": "port",
+            "sample": f"{label} ({n_el} elements), {len(times)} fused E+grad+Hess passes of the CPU "
+                      "restatement (torch.func float64 autodiff of the reference element energy + np.add.at "
+                      "scatter)", "seconds_per_pass": dt}
 
 
 def run_reference(args):
@@ -172,54 +371,54 @@ def run_reference(args):
     import torch
 
     torch.set_num_threads(os.cpu_count() or 1)
-    grid = 512
-    from oracle.assembler import OracleAssembler
-    from fenics_nonlinear_energies_b200 import meshes
-
-    params, u0 = meshes.gl_problem(n=grid, seed=0)
-    asm = OracleAssembler("gl", params)
+    w = WORKLOADS[args.workload]
+    asm, u, n_el, label, _, _, _ = _oracle_sample(w)
     for _ in range(args.warmup):
-        asm.all_in_one(u0)
+        asm.all_in_one(u)
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
-        asm.all_in_one(u0)
+        asm.all_in_one(u)
         times.append(time.perf_counter() - t)
-    n_el = 2 * grid * grid
     dt = sum(times) / len(times)
     value = n_el / dt
     line = {
         "impl": "reference", "metric": "elements/s (E+grad+Hess)", "value": value, "unit": "elements/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_grid": f"{grid}x{grid}", "elements_per_step": n_el},
+        "config": {"workload": w.name, "description": w.desc, "sample": label, "elements_per_step": n_el},
         "cpu_baseline": {"value": value, "unit": "elements/s", "cores": int(torch.get_num_threads()),
                          "kind": "port",
-                         "sample": f"GL {grid}x{grid} P1 grid ({n_el} elements) per step; CPU restatement of the "
-                                   "reference JAX element kernels (torch.func float64 autodiff) + np.add.at scatter"},
+                         "sample": f"{label} ({n_el} elements) per step; CPU restatement of the reference JAX "
+                                   "element kernels (torch.func float64 autodiff) + np.add.at scatter"},
         "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the CUDA path
+# ---------------------------------------------------------------------------
 def run(args):
+    import numpy as np
     import torch
 
     world, rank, local = _dist_setup()
     torch.cuda.set_device(local)
     from fenics_nonlinear_energies_b200 import _lib
-    from fenics_nonlinear_energies_b200.assembler import GLCudaAssembler
-    from fenics_nonlinear_energies_b200 import meshes
 
-    params, u0 = meshes.gl_problem(n=GRID, seed=rank)
-    asm = GLCudaAssembler(params, precision="fp32", hess_dtype=torch.float32)
-    n_el = int(params["elems"].shape[0])
+    w = WORKLOADS[args.workload]
+    t_setup = time.perf_counter()
+    asm, u0 = w.build(rank)
+    t_setup = time.perf_counter() - t_setup
+    n_el = int(asm.info["n_elem"])
     dev = torch.device("cuda", local)
     u = torch.as_tensor(u0, device=dev)
     flags = _lib.FNE_ENERGY | _lib.FNE_GRAD | _lib.FNE_HESS
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    launches_per_pass = asm.launches_per_eval(flags)
 
     for _ in range(args.warmup):
         asm.eval(u, flags)
@@ -241,11 +440,12 @@ def run(args):
     total_s = _max_over_ranks(sum(kernel_ms) * 1e-3, world)
     value = world * n_el * args.steps / total_s
     ms_step = total_s * 1e3 / args.steps
+    energy = float(asm.eval(u, flags)[0].item())
 
     # end to end through the public API with host buffers
-    pin_u = torch.from_numpy(u0).pin_memory()
+    pin_u = torch.from_numpy(np.ascontiguousarray(u0)).pin_memory()
     host_g = torch.empty(asm.n_owned, dtype=torch.float64).pin_memory()
-    host_h = torch.empty(asm.owned_values.numel(), dtype=torch.float32).pin_memory()
+    host_h = torch.empty(asm.owned_values.numel(), dtype=asm.owned_values.dtype).pin_memory()
     host_e = torch.empty(1, dtype=torch.float64).pin_memory()
     dev_u = torch.empty_like(u)
     e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -268,35 +468,36 @@ def run(args):
     e2e_s = _max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev) * 1e-3, world)
     e2e_value = world * n_el * args.steps / e2e_s
 
-    # roofline of the fused row-gather kernel (one launch per step)
-    n_free = asm.layout.n_free
-    nnz = int(asm.owned_values.numel())
-    alg_bytes = n_el * (3 * 4 + 7 * 4) + n_free * 8 + asm.n_owned * 8 + nnz * 4
+    # roofline of the pass (one kernel launch per pass for the P1 families)
+    alg_bytes = algorithmic_bytes(w, asm, n_el)
     peak, peak_kind = _peaks()
     avg_launch_s = (sum(kernel_ms) / len(kernel_ms)) * 1e-3
     achieved = alg_bytes / avg_launch_s / 1e9
-    traffic = _traffic_per_launch()
+    kname = KERNEL_NAMES.get(asm.info["kernel_variant"], "?")
+    traffic = NCU_TRAFFIC.get((w.name, kname))
+    nnz = int(asm.owned_values.numel())
 
     if rank == 0:
-        cpu = cpu_port_baseline() if (world == 1 and not args.no_cpu_baseline) else None
+        cpu = cpu_port_baseline(w) if (world == 1 and not args.no_cpu_baseline) else None
         line = {
             "metric": "elements/s (E+grad+Hess)", "value": value, "unit": "elements/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (element grad/Hessian), f64 (energy)",
-            "data": "synthetic (seeded U[-0.5,0.5] initial guess on the structured grid)",
-            "config": {"workload": WORKLOAD, "elements": n_el, "free_dofs": n_free, "coo_nnz": nnz,
+            "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
+            "data": "synthetic (seeded / closed-form state on the generated mesh)",
+            "config": {"workload": w.name, "description": w.desc, "elements": n_el, "free_dofs": asm.layout.n_free,
+                       "coo_nnz": nnz, "energy": energy, "setup_s": t_setup,
                        "l2": "flushed by a 256 MiB write between passes (outside the timed events)",
                        "parallelism": f"{world} independent replica(s), one per GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": f"{peak_kind} burst copy",
-                         "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri",
-                                    4: "k_sweep_tri"}.get(asm.info["kernel_variant"], "?")
-                                   + "<float, GL, E|G|H, float>"},
+                         "frac": achieved / peak, "peak_kind": f"{peak_kind} burst copy (hbm_gbs)",
+                         "traffic": traffic[0] if traffic else None,
+                         "traffic_source": traffic[1] if traffic else None,
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "kernel": kname, "launches_per_pass": launches_per_pass},
             "e2e": {"value": e2e_value, "unit": "elements/s",
                     "h2d_bytes_per_step": int(u0.nbytes),
-                    "d2h_bytes_per_step": int(8 + host_g.numel() * 8 + host_h.numel() * 4)},
-            "gpu_launches": args.steps,
+                    "d2h_bytes_per_step": int(8 + host_g.numel() * 8 + host_h.numel() * host_h.element_size())},
+            "gpu_launches": args.steps * launches_per_pass,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
@@ -314,6 +515,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":

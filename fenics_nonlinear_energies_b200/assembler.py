@@ -160,6 +160,14 @@ class CudaElementAssemblerBase:
     def _adds_dirichlet_only_energy(self):
         return False
 
+    def launches_per_eval(self, flags):
+        """Kernel launches one ``eval(u, flags)`` issues: one fused kernel for the
+        P1 families; element kernel plus Hessian and gradient gathers for
+        Mohr-Coulomb."""
+        if self.info["kernel_variant"] != 5:
+            return 1
+        return 1 + int(bool(flags & _lib.FNE_HESS)) + int(bool(flags & _lib.FNE_GRAD))
+
     # ---- vector helpers -----------------------------------------------------
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream

@@ -218,7 +218,8 @@ def run_load_path(params, theta_total, steps, *, predictor=None, features=None, 
         t0 = time.perf_counter()
         x_plain, info_plain = newton(asm, to_dev(y), **kw)
         rec = {"step": k, "theta": theta, "plain_its": info_plain["iterations"],
-               "plain_converged": info_plain["converged"], "energy": info_plain["energy"]}
+               "plain_converged": info_plain["converged"], "plain_message": info_plain["message"],
+               "energy": info_plain["energy"]}
         x_use = x_plain
         if predictor is not None:
             u_k = (y - X_free).reshape(-1, 3)

@@ -41,6 +41,7 @@ def run(nx=80, ny=4, nz=4, train_paths=16, test_paths=4, steps=24, epochs=150, s
     feats = None
     F_all, T_all = [], []
     gen_its, gen_time, gen_steps, gen_fail = 0, 0.0, 0, 0
+    fail_msgs = {}
     for i, (theta, E) in enumerate(random_paths(train_paths, seed)):
         params, _ = meshes.he_beam_problem(nx=nx, ny=ny, nz=nz, E=E)
         if feats is None:
@@ -51,6 +52,9 @@ def run(nx=80, ny=4, nz=4, train_paths=16, test_paths=4, steps=24, epochs=150, s
         gen_its += sum(r["plain_its"] for r in recs)
         gen_steps += len(recs)
         gen_fail += sum(not r["plain_converged"] for r in recs)
+        for r in recs:
+            if not r["plain_converged"]:
+                fail_msgs[r["plain_message"]] = fail_msgs.get(r["plain_message"], 0) + 1
         F, T = training_pairs(feats, sols, theta, E)
         F_all.append(F)
         T_all.append(T)
@@ -83,7 +87,8 @@ def run(nx=80, ny=4, nz=4, train_paths=16, test_paths=4, steps=24, epochs=150, s
         "training_samples": int(F.shape[0]), "training_step_solutions": int(F.shape[0] // len(feats.X)),
         "mlp": {"dims": [F.shape[1], 256, 256, 256, T.shape[1]], "dtype": "bf16 weights, fp32 accumulate",
                 "epochs": epochs, "final_mse": hist[-1], "train_time_s": train_time},
-        "generation": {"newton_its": gen_its, "steps": gen_steps, "failed_steps": gen_fail, "time_s": gen_time},
+        "generation": {"newton_its": gen_its, "steps": gen_steps, "failed_steps": gen_fail, "failure_messages": fail_msgs,
+                       "time_s": gen_time},
         "test": {"plain_newton_its": plain_its, "learned_newton_its": learned_its, "accepted_steps": accepted,
                  "steps": n_steps, "reduction": 1.0 - learned_its / max(1, plain_its), "paths": per_path},
         "tolerance": "||g|| <= 1e-6 ||g_0|| per step", "total_time_s": time.perf_counter() - t_all,

@@ -90,3 +90,16 @@ def test_newton_converges(family):
     assert abs(info["energy"] - ref.energy_fn(xs)) <= 1e-10 * max(1.0, abs(info["energy"]))
     assert np.linalg.norm(ref.gradient_fn(xs)) <= 1.01e-6 * info["grad_norm0"]
     assert info["energy"] < ref.energy_fn(u0)
+
+
+def test_learned_warm_start_cuts_newton_iterations():
+    """Train on solver-generated load-path solutions of a small twisted beam and
+    compare, on a held-out path, the Newton iterations from the MLP prediction
+    with those from the plain previous-step start (same 1e-6 gradient tolerance
+    and energy; a rejected prediction is charged both solves)."""
+    from fenics_nonlinear_energies_b200 import warmstart_experiment as wx
+
+    res = wx.run(nx=32, ny=3, nz=3, train_paths=6, test_paths=1, steps=12, epochs=60, seed=3, log=lambda *_: None)
+    t = res["test"]
+    assert t["accepted_steps"] >= t["steps"] - 1
+    assert t["learned_newton_its"] <= 0.85 * t["plain_newton_its"], t
