@@ -125,7 +125,7 @@ class CudaElementAssemblerBase:
             d.s[i] = float(v)
         d.nq = int(self._nq())
         d.dirichlet_only_energy = 1 if (self._adds_dirichlet_only_energy() and self.rank == 0) else 0
-        d.kernel_variant = {"auto": 0, "row_gather": 1, "incidence": 2}[kernel_variant]
+        d.kernel_variant = {"auto": 0, "row_gather": 1, "incidence": 2, "cuda_cores": 1}[kernel_variant]
         self._handle = _lib.C.c_void_p()
         check(lib.fne_create(_lib.C.byref(d), _lib.C.byref(self._handle)))
         del keep
@@ -160,11 +160,15 @@ class CudaElementAssemblerBase:
     def _adds_dirichlet_only_energy(self):
         return False
 
+    def check_device_status(self):
+        """Raise if a bounded device wait of an earlier pass gave up (synchronous)."""
+        check(lib.fne_check_device_status(self._handle))
+
     def launches_per_eval(self, flags):
         """Kernel launches one ``eval(u, flags)`` issues: one fused kernel for the
         P1 families; element kernel plus Hessian and gradient gathers for
         Mohr-Coulomb."""
-        if self.info["kernel_variant"] != 5:
+        if self.info["kernel_variant"] not in (5, 6):
             return 1
         return 1 + int(bool(flags & _lib.FNE_HESS)) + int(bool(flags & _lib.FNE_GRAD))
 

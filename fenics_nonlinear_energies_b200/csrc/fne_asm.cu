@@ -1637,6 +1637,11 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   return FNE_OK;
 }
 
+extern "C" int fne_check_device_status(fne_handle* h) {
+  if (!h) return set_error(FNE_EINVAL, "fne_check_device_status: null handle");
+  return h->mc ? mc_check_status(h->mc) : FNE_OK;
+}
+
 extern "C" int fne_set_dirichlet(fne_handle* h, const double* dirichlet) {
   if (!h || (!dirichlet && h->n_total > 0)) return set_error(FNE_EINVAL, "fne_set_dirichlet: null argument");
   if (h->n_total == 0) return FNE_OK;

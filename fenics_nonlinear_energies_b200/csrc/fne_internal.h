@@ -114,6 +114,7 @@ int mc_create(const fne_desc* d, McHandle** out);
 int mc_eval(McHandle* h, const double* u, int flags, double* energy, double* grad, void* hess, void* stream);
 int mc_set_dirichlet(McHandle* h, const double* dirichlet);
 void mc_info(const McHandle* h, fne_info* info);
+int mc_check_status(McHandle* h);
 void mc_destroy(McHandle* h);
 
 // Gather code of one element node: >= 0 reordered id of component 0 (free

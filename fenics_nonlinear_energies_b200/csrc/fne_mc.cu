@@ -299,26 +299,398 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_elem(McArgs A, McConstR<Re
         }
         __syncwarp();
       }
-      Real* Ke = Kbuf + (long long)e * N * N;
+      // node-pair layout: Kbuf[e][pair][c * 2 + d] = K[(a, c), (b, d)], a <= b
+      Real* Ke = Kbuf + (long long)e * NPAIR * 4;
 #pragma unroll
       for (int k = 0; k < PPL; ++k) {
         if (lane + 32 * k < NPAIR) {
-          const int a = pa[k], b = pb[k];
-          Ke[(2 * a) * N + 2 * b] = kacc[k][0];
-          Ke[(2 * a) * N + 2 * b + 1] = kacc[k][1];
-          Ke[(2 * a + 1) * N + 2 * b] = kacc[k][2];
-          Ke[(2 * a + 1) * N + 2 * b + 1] = kacc[k][3];
-          if (a != b) {
-            Ke[(2 * b) * N + 2 * a] = kacc[k][0];
-            Ke[(2 * b + 1) * N + 2 * a] = kacc[k][1];
-            Ke[(2 * b) * N + 2 * a + 1] = kacc[k][2];
-            Ke[(2 * b + 1) * N + 2 * a + 1] = kacc[k][3];
-          }
+          Real* o = Ke + 4 * (lane + 32 * k);
+          o[0] = kacc[k][0];
+          o[1] = kacc[k][1];
+          o[2] = kacc[k][2];
+          o[3] = kacc[k][3];
         }
       }
     }
     __syncwarp();
   }
+  if (WANT & MW_E) {
+    if (A.rhs)
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_owned; i += gridDim.x * blockDim.x)
+        eacc -= A.rhs[i] * A.u[A.lo + i];
+    mc_energy_finalize(eacc, partials, counter, eout);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core element kernel (FP32, P2 / P4): tcgen05.mma, kind::tf32.
+//
+// For affine triangles the physical basis gradients are g_ai = sum_k J^-1_ik
+// R_ak with R the reference gradients at the quadrature point, so
+//   K[(a,c),(b,d)] = sum_q sum_{k,l} R_qak R_qbl  At_q[c,k,d,l],
+//   At_q[c,k,d,l]  = w_q sum_{i,j} J^-1_ik J^-1_jl Ct_q[v(c,i), v(d,j)],
+// (v: Voigt index of the strain component that DOF (c) feeds through the
+// derivative in direction i).  Over a tile of TE elements this is one GEMM
+//   D[(a,b), (e,c,d)] = P[(a,b), (q,k,l)] . At[(q,k,l), (e,c,d)]
+// with a constant A operand P (node pairs a <= b x (q,k,l), built on the host)
+// and the per-element B operand At (computed by the CTA from the constitutive
+// update).  M = 128 node pairs (120 used for P4, 21 for P2), K = 4 nq padded to
+// a multiple of 8, N = 4 TE.  FP32 accuracy from three TF32 products:
+// D = P_hi At_hi + P_hi At_lo + P_lo At_hi (hi = top 19 bits, lo = remainder).
+// Operands live in shared memory in the no-swizzle K-major core-matrix
+// layout (8 rows x 16 bytes per core matrix); the accumulator lives in TMEM
+// and is read back with tcgen05.ld into the node-pair layout of Kbuf.
+// The element gradient (sum_q B^T w sigma) runs on the CUDA cores while the
+// tensor core works.
+// ---------------------------------------------------------------------------
+namespace tc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: no swizzle, K-major core matrices.
+// lbo: byte distance between the two 16-byte K halves of one MMA step;
+// sbo: byte distance between consecutive groups of 8 rows.
+__device__ __forceinline__ uint64_t mat_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;                // base offset 0, absolute LBO mode, no swizzle
+}
+
+// Instruction descriptor: D f32, A/B tf32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit) {
+  for (long long it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 16 consecutive 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+
+}  // namespace tc
+
+// Tile geometry of the tensor-core kernel for (NP, NQ).
+template <int NP, int NQ>
+struct McTile {
+  static constexpr int NPAIR = NP * (NP + 1) / 2;
+  static constexpr int KK = 4 * NQ;                 // (q, k, l)
+  static constexpr int KP = (KK + 7) / 8 * 8;       // padded to the MMA K step (8 tf32)
+  static constexpr int M = 128;                     // node pairs (padded)
+  static constexpr int TE = NP > 6 ? 24 : 64;       // elements per tile
+  static constexpr int N = 4 * TE;                  // (e, c, d)
+  static constexpr int TMEM_COLS = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+  static constexpr int THREADS = 256;
+  static constexpr int MIN_BLOCKS = NP > 6 ? 1 : 2;
+  // shared memory (bytes); operand buffers first (16-byte aligned)
+  static constexpr int A_BYTES = M * KP * 4;
+  static constexpr int B_BYTES = N * KP * 4;
+  static constexpr int OFF_AHI = 0, OFF_ALO = A_BYTES, OFF_BHI = 2 * A_BYTES, OFF_BLO = 2 * A_BYTES + B_BYTES;
+  static constexpr int OFF_S = 2 * A_BYTES + 2 * B_BYTES;          // [TE][NQ][4] gradient helper
+  static constexpr int OFF_R = OFF_S + TE * NQ * 16;                // dh1, dh2 [NQ * NP], qw [NQ]
+  static constexpr int OFF_U = OFF_R + ((2 * NQ * NP + NQ) * 4 + 15) / 16 * 16;  // [TE][2 NP]
+  static constexpr int OFF_G = OFF_U + (TE * 2 * NP * 4 + 15) / 16 * 16;          // [TE][5]
+  static constexpr int OFF_BAR = OFF_G + (TE * 5 * 4 + 15) / 16 * 16;             // mbarrier, tmem addr, flags
+  static constexpr int SMEM = OFF_BAR + 64;
+};
+
+// try_wait polls before the kernel gives up on an MMA completion (each poll
+// may itself suspend briefly): far above any tile's MMA time, still bounded.
+constexpr long long kMcWaitLimit = 1LL << 22;
+
+struct McTcArgs {
+  const float* Phi;  // [KP/4][M][4] constant operand, hi part (core-matrix order)
+  const float* Plo;  // same, lo part
+  int* err;          // device status word (0 = ok; 1 = MMA completion wait timed out)
+};
+
+template <int NP, int NQ, int WANT>
+__global__ void __launch_bounds__(256, McTile<NP, NQ>::MIN_BLOCKS)
+    k_mc_tc(McArgs A, McConstR<float> C, McTcArgs T, float* __restrict__ Kbuf, float* __restrict__ gbuf,
+            double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ eout) {
+  using G = McTile<NP, NQ>;
+  constexpr int N2 = 2 * NP, TE = G::TE, N = G::N, M = G::M, KP = G::KP, NPAIR = G::NPAIR;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  float* sAhi = reinterpret_cast<float*>(smem + G::OFF_AHI);
+  float* sAlo = reinterpret_cast<float*>(smem + G::OFF_ALO);
+  float* sBhi = reinterpret_cast<float*>(smem + G::OFF_BHI);
+  float* sBlo = reinterpret_cast<float*>(smem + G::OFF_BLO);
+  float4* sS = reinterpret_cast<float4*>(smem + G::OFF_S);
+  float* sD1 = reinterpret_cast<float*>(smem + G::OFF_R);
+  float* sD2 = sD1 + NQ * NP;
+  float* sW = sD2 + NQ * NP;
+  float* sU = reinterpret_cast<float*>(smem + G::OFF_U);
+  float* sGm = reinterpret_cast<float*>(smem + G::OFF_G);
+  unsigned long long* sBar = reinterpret_cast<unsigned long long*>(smem + G::OFF_BAR);
+  uint32_t* sTmem = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 8);
+  int* sFail = reinterpret_cast<int*>(smem + G::OFF_BAR + 12);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  // constant operand and reference tables (once per CTA)
+  {
+    const float4* ph = reinterpret_cast<const float4*>(T.Phi);
+    const float4* pl = reinterpret_cast<const float4*>(T.Plo);
+    float4* ah = reinterpret_cast<float4*>(sAhi);
+    float4* al = reinterpret_cast<float4*>(sAlo);
+    for (int i = tid; i < M * KP / 4; i += blockDim.x) {
+      ah[i] = ph[i];
+      al[i] = pl[i];
+    }
+    // B padding chunks (k >= KK) stay zero for the whole kernel
+    for (int i = tid; i < (KP - G::KK) / 4 * N; i += blockDim.x) {
+      const int off = (G::KK / 4) * N * 4 + i * 4;
+      reinterpret_cast<float4*>(sBhi + off)[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+      reinterpret_cast<float4*>(sBlo + off)[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int i = tid; i < NQ * NP; i += blockDim.x) {
+      sD1[i] = (float)A.dhat1[i];
+      sD2[i] = (float)A.dhat2[i];
+    }
+    for (int i = tid; i < NQ; i += blockDim.x) sW[i] = (float)A.qw[i];
+  }
+  const uint32_t bar = tc::smem_u32(sBar);
+  if (tid == 0) {
+    *sFail = 0;
+    tc::mbar_init(bar);
+  }
+  if (warp == 0) tc::tmem_alloc(tc::smem_u32(sTmem), G::TMEM_COLS);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = *sTmem;
+  constexpr uint32_t idesc = tc::idesc_tf32(M, N);
+
+  double eacc = 0.0;
+  uint32_t phase = 0;
+  const int n_tiles = (A.n_el + TE - 1) / TE;
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int e0 = tile * TE;
+    const int ne = min(TE, A.n_el - e0);
+    // (1) nodal values and element geometry of the tile
+    for (int i = tid; i < TE * N2; i += blockDim.x) {
+      const int el = i / N2;
+      float v = 0.f;
+      if (el < ne) {
+        const int code = A.codes[(long long)(e0 + el) * N2 + (i - el * N2)];
+        v = (float)(code >= 0 ? A.u[code] : A.dir[-1 - code]);
+      }
+      sU[i] = v;
+    }
+    for (int i = tid; i < TE * 5; i += blockDim.x) {
+      const int el = i / 5;
+      sGm[i] = el < ne ? (float)A.geom[(long long)e0 * 5 + i] : 0.f;
+    }
+    __syncthreads();
+    // (2) constitutive update per (element, quadrature point) -> At (B operand), gradient helper
+    for (int p = tid; p < TE * NQ; p += blockDim.x) {
+      const int el = p / NQ, q = p - el * NQ;
+      float4 at[4];  // (c, d) blocks: [k * 2 + l]
+      float4 sg = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (el < ne) {
+        const float* gm = sGm + el * 5;
+        const float i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
+        const float* ue = sU + el * N2;
+        float ex = 0.f, ey = 0.f, exy = 0.f;
+#pragma unroll 5
+        for (int a = 0; a < NP; ++a) {
+          const float r1 = sD1[q * NP + a], r2 = sD2[q * NP + a];
+          const float px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
+          const float ux = ue[2 * a], uy = ue[2 * a + 1];
+          ex += px * ux;
+          ey += py * uy;
+          exy += py * ux + px * uy;
+        }
+        float eps[3] = {ex, ey, exy};
+        if (A.epsp) {
+          const double* ep = A.epsp + ((long long)(e0 + el) * NQ + q) * 3;
+          eps[0] -= (float)ep[0];
+          eps[1] -= (float)ep[1];
+          eps[2] -= (float)ep[2];
+        }
+        float sig[3], Ct[6], psi;
+        mc_point(C, eps, sig, Ct, psi);
+        const float w = gm[4] * sW[q];
+        if ((WANT & MW_E) && A.wflag[e0 + el]) eacc += (double)(w * psi);
+        // full symmetric tangent (Voigt 0 = xx, 1 = yy, 2 = xy)
+        const float Cf[3][3] = {{Ct[0], Ct[1], Ct[2]}, {Ct[1], Ct[3], Ct[4]}, {Ct[2], Ct[4], Ct[5]}};
+        // v(c, i): component c of the DOF, physical derivative direction i
+        const int vci[2][2] = {{0, 2}, {2, 1}};
+        const float Mx[2][2] = {{i00, i01}, {i10, i11}};  // g_i = sum_k Mx[i][k] R_k
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll
+          for (int d = 0; d < 2; ++d) {
+            float Acd[2][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+              for (int j = 0; j < 2; ++j) Acd[i][j] = w * Cf[vci[c][i]][vci[d][j]];
+            float r[4];
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+#pragma unroll
+              for (int l = 0; l < 2; ++l)
+                r[k * 2 + l] = Mx[0][k] * (Acd[0][0] * Mx[0][l] + Acd[0][1] * Mx[1][l]) +
+                               Mx[1][k] * (Acd[1][0] * Mx[0][l] + Acd[1][1] * Mx[1][l]);
+            at[c * 2 + d] = make_float4(r[0], r[1], r[2], r[3]);
+          }
+        }
+        // gradient helper s[c][k] = w sum_i Mx[i][k] sigma[v(c, i)]
+        const float s00 = w * (Mx[0][0] * sig[0] + Mx[1][0] * sig[2]);
+        const float s01 = w * (Mx[0][1] * sig[0] + Mx[1][1] * sig[2]);
+        const float s10 = w * (Mx[0][0] * sig[2] + Mx[1][0] * sig[1]);
+        const float s11 = w * (Mx[0][1] * sig[2] + Mx[1][1] * sig[1]);
+        sg = make_float4(s00, s01, s10, s11);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) at[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      sS[el * NQ + q] = sg;
+      // B operand rows n = el * 4 + (c * 2 + d), K chunk q (16 bytes: k * 2 + l)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int off = q * N * 4 + (el * 4 + j) * 4;
+        const float4 v = at[j];
+        const float4 hi = make_float4(tc::tf32_hi(v.x), tc::tf32_hi(v.y), tc::tf32_hi(v.z), tc::tf32_hi(v.w));
+        reinterpret_cast<float4*>(sBhi + off)[0] = hi;
+        reinterpret_cast<float4*>(sBlo + off)[0] = make_float4(v.x - hi.x, v.y - hi.y, v.z - hi.z, v.w - hi.w);
+      }
+    }
+    tc::fence_proxy_async();  // generic-proxy smem writes -> visible to the tensor core
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    // (3) one thread issues the MMAs: 3 TF32 products per K step of 8
+    if ((WANT & MW_H) && tid == 0) {
+      const uint32_t ahi = tc::smem_u32(sAhi), alo = tc::smem_u32(sAlo);
+      const uint32_t bhi = tc::smem_u32(sBhi), blo = tc::smem_u32(sBlo);
+#pragma unroll 1
+      for (int s = 0; s < KP / 8; ++s) {
+        const uint32_t ao = (uint32_t)(s * 2 * M * 16), bo = (uint32_t)(s * 2 * N * 16);
+        const uint64_t dAh = tc::mat_desc(ahi + ao, M * 16, 128), dAl = tc::mat_desc(alo + ao, M * 16, 128);
+        const uint64_t dBh = tc::mat_desc(bhi + bo, N * 16, 128), dBl = tc::mat_desc(blo + bo, N * 16, 128);
+        tc::mma_tf32(tmem, dAh, dBh, idesc, s > 0 ? 1u : 0u);
+        tc::mma_tf32(tmem, dAh, dBl, idesc, 1u);
+        tc::mma_tf32(tmem, dAl, dBh, idesc, 1u);
+      }
+      tc::commit(bar);
+    }
+    // (4) element gradient on the CUDA cores while the MMAs run
+    if (WANT & MW_G) {
+      for (int i = tid; i < TE * N2; i += blockDim.x) {
+        const int el = i / N2, r = i - el * N2, a = r >> 1, c = r & 1;
+        if (el >= ne) continue;
+        float acc = 0.f;
+#pragma unroll 5
+        for (int q = 0; q < NQ; ++q) {
+          const float4 s = sS[el * NQ + q];
+          const float r1 = sD1[q * NP + a], r2 = sD2[q * NP + a];
+          acc += c == 0 ? r1 * s.x + r2 * s.y : r1 * s.z + r2 * s.w;
+        }
+        gbuf[(long long)(e0 + el) * N2 + r] = acc;
+      }
+    }
+    // (5) epilogue: TMEM -> Kbuf[e][pair][c * 2 + d]
+    if (WANT & MW_H) {
+      if (tc::mbar_wait(bar, phase, kMcWaitLimit))
+        phase ^= 1u;
+      else if (lane == 0)
+        atomicExch(sFail, 1);
+      tc::fence_after();
+      const int quad = warp & 3, half = warp >> 2;
+      const int m = quad * 32 + lane;
+      if (!*sFail && quad * 32 < NPAIR) {
+        constexpr int COLS = N / 2;  // columns per warp half
+#pragma unroll 1
+        for (int c0 = 0; c0 < COLS; c0 += 16) {
+          float v[16];
+          const int col = half * COLS + c0;
+          tc::tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)col, v);
+          if (m < NPAIR) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int el = (col >> 2) + j;
+              if (el < ne)
+                reinterpret_cast<float4*>(Kbuf + ((long long)(e0 + el) * NPAIR + m) * 4)[0] =
+                    make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+            }
+          }
+        }
+      }
+      tc::fence_before();
+    }
+    __syncthreads();
+    if (*sFail) break;
+  }
+  if (*sFail && tid == 0) {
+    // one more bounded wait so no MMA is in flight when TMEM is released
+    tc::mbar_wait(bar, phase, kMcWaitLimit);
+    atomicExch(T.err, 1);
+  }
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if (warp == 0) tc::tmem_dealloc(tmem, G::TMEM_COLS);
   if (WANT & MW_E) {
     if (A.rhs)
       for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_owned; i += gridDim.x * blockDim.x)
@@ -366,6 +738,10 @@ struct McHandle {
   void *Kbuf = nullptr, *gbuf = nullptr;
   int grid_elem = 1, n_partials = 1;
   int64_t device_bytes = 0, n_contrib = 0;
+  // tensor-core path (FP32, P2 / P4): constant operand halves, status word
+  int tc = 0, grid_tc = 1;
+  float *Phi = nullptr, *Plo = nullptr;
+  int* err = nullptr;
 };
 
 namespace {
@@ -382,6 +758,20 @@ int mc_upload(McHandle* h, T** p, const T* src, size_t count) {
     if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
   }
   return FNE_OK;
+}
+
+// Hessian / gradient gathers after the element kernel (checks its launch first).
+template <typename Real, typename HOut>
+cudaError_t mc_gathers(McHandle* h, int flags, const Real* K, const Real* g, double* grad, void* hess,
+                       cudaStream_t st) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int gg = std::max(1, std::min(h->num_sms * 16, (int)((std::max<int64_t>(h->nnz, h->n_rows) + 255) / 256)));
+  if ((flags & MW_H) && h->nnz > 0)
+    k_mc_gather<Real, HOut><<<gg, 256, 0, st>>>((int)h->nnz, h->hptr, h->hidx, K, static_cast<HOut*>(hess));
+  if ((flags & MW_G) && h->n_rows > 0)
+    k_mc_grad_gather<Real><<<gg, 256, 0, st>>>(h->n_rows, h->gptr, h->gidx, g, h->row_gpos, h->rhs, grad);
+  return cudaGetLastError();
 }
 
 template <typename Real, typename HOut, int NP, int NQ>
@@ -406,6 +796,22 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
   Real* g = static_cast<Real*>(h->gbuf);
   const int grid = h->grid_elem;
   const int T = 32 * kMcWarps;
+  if constexpr (sizeof(Real) == 4 && NP > 3) {
+    if (h->tc && (flags & MW_H)) {
+      using G = McTile<NP, NQ>;
+      McTcArgs T{h->Phi, h->Plo, h->err};
+      float* K = static_cast<float*>(h->Kbuf);
+      float* g = static_cast<float*>(h->gbuf);
+      const McConstR<float> Mf = cast_const<float>(h->mc);
+      switch (flags) {
+        case 4: k_mc_tc<NP, NQ, 4><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
+        case 5: k_mc_tc<NP, NQ, 5><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
+        case 6: k_mc_tc<NP, NQ, 6><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
+        default: k_mc_tc<NP, NQ, 7><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
+      }
+      return mc_gathers<float, HOut>(h, flags, K, g, grad, hess, st);
+    }
+  }
   switch (flags) {
     case 1: k_mc_elem<Real, NP, NQ, 1><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
     case 2: k_mc_elem<Real, NP, NQ, 2><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
@@ -416,14 +822,7 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
     case 7: k_mc_elem<Real, NP, NQ, 7><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
     default: return cudaErrorInvalidValue;
   }
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  const int gg = std::max(1, std::min(h->num_sms * 16, (int)((std::max<int64_t>(h->nnz, h->n_rows) + 255) / 256)));
-  if ((flags & MW_H) && h->nnz > 0)
-    k_mc_gather<Real, HOut><<<gg, 256, 0, st>>>((int)h->nnz, h->hptr, h->hidx, K, static_cast<HOut*>(hess));
-  if ((flags & MW_G) && h->n_rows > 0)
-    k_mc_grad_gather<Real><<<gg, 256, 0, st>>>(h->n_rows, h->gptr, h->gidx, g, h->row_gpos, h->rhs, grad);
-  return cudaGetLastError();
+  return mc_gathers<Real, HOut>(h, flags, K, g, grad, hess, st);
 }
 
 template <typename Real, typename HOut>
@@ -435,12 +834,58 @@ cudaError_t mc_dispatch(McHandle* h, int flags, const double* u, double* energy,
   return cudaErrorInvalidValue;
 }
 
+// Constant operand P[(a, b), (q, k, l)] = R_qak R_qbl of the tensor-core
+// kernel, split into TF32 hi / lo parts and laid out as the kernel's shared
+// memory image ([K / 4][M][4] floats, zero padding); also sizes the grid and
+// opts the kernel into its shared memory.
+template <int NP, int NQ>
+int mc_tc_prepare(McHandle* h, const double* tables, std::vector<float>& phi, std::vector<float>& plo) {
+  using G = McTile<NP, NQ>;
+  const double* d1 = tables;
+  const double* d2 = tables + NQ * NP;
+  phi.assign((size_t)G::M * G::KP, 0.f);
+  plo.assign((size_t)G::M * G::KP, 0.f);
+  int m = 0;
+  for (int a = 0; a < NP; ++a)
+    for (int b = a; b < NP; ++b, ++m)
+      for (int q = 0; q < NQ; ++q)
+        for (int k = 0; k < 2; ++k)
+          for (int l = 0; l < 2; ++l) {
+            const double ra = k == 0 ? d1[q * NP + a] : d2[q * NP + a];
+            const double rb = l == 0 ? d1[q * NP + b] : d2[q * NP + b];
+            const float v = (float)(ra * rb);
+            uint32_t bits;
+            std::memcpy(&bits, &v, 4);
+            bits &= 0xFFFFE000u;
+            float hi;
+            std::memcpy(&hi, &bits, 4);
+            const int kk = q * 4 + k * 2 + l;
+            const size_t off = (size_t)(kk / 4) * G::M * 4 + (size_t)m * 4 + (kk % 4);
+            phi[off] = hi;
+            plo[off] = v - hi;
+          }
+  cudaError_t e = cudaFuncSetAttribute(k_mc_tc<NP, NQ, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mc_tc<NP, NQ, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mc_tc<NP, NQ, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mc_tc<NP, NQ, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+  if (e != cudaSuccess)
+    return set_error(FNE_ECUDA, std::string("Mohr-Coulomb: tensor-core kernel shared memory: ") +
+                                    cudaGetErrorString(e));
+  const int n_tiles = (h->n_local + G::TE - 1) / G::TE;
+  h->grid_tc = std::max(1, std::min(n_tiles, h->num_sms * G::MIN_BLOCKS));
+  return FNE_OK;
+}
+
 }  // namespace
 
 void mc_destroy(McHandle* h) {
   if (!h) return;
   void* ptrs[] = {h->codes, h->geom, h->epsp, h->dhat1, h->dhat2, h->qw, h->wflag, h->dir, h->rhs,
-                  h->partials, h->counter, h->hptr, h->hidx, h->gptr, h->gidx, h->row_gpos, h->Kbuf, h->gbuf};
+                  h->partials, h->counter, h->hptr, h->hidx, h->gptr, h->gidx, h->row_gpos, h->Kbuf, h->gbuf,
+                  h->Phi, h->Plo, h->err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -522,7 +967,17 @@ int mc_create(const fne_desc* d, McHandle** out) {
     }
     return (a < row_ptr[k + 1] && d->owned_cols[bycol[a]] == col) ? bycol[a] : -1;
   };
-  // contributions (two passes: count, fill), in element order
+  // contributions (two passes: count, fill), in element order; element
+  // matrices are stored per node pair a <= b: slot pair(a, b) * 4 + c * 2 + d
+  const int npair = np * (np + 1) / 2;
+  auto pair_slot = [np](int i, int j) -> int {
+    int a = i >> 1, c = i & 1, b = j >> 1, dd = j & 1;
+    if (a > b) {
+      std::swap(a, b);
+      std::swap(c, dd);
+    }
+    return (a * np - a * (a - 1) / 2 + (b - a)) * 4 + c * 2 + dd;
+  };
   std::vector<int32_t> hptr(d->nnz + 1, 0), gptr(n_rows + 1, 0), hidx, gidx, hfill, gfill;
   for (int pass = 0; pass < 2; ++pass) {
     if (pass == 1) {
@@ -543,7 +998,7 @@ int mc_create(const fne_desc* d, McHandle** out) {
           if (c[j] < 0) continue;
           const int32_t p = find(k, c[j]);
           if (p < 0) return set_error(FNE_ELAYOUT, "Scatter lookup found mismatched owned COO entries");
-          if (pass == 0) hptr[p + 1]++; else hidx[hfill[p]++] = (int32_t)(le * n * n + i * n + j);
+          if (pass == 0) hptr[p + 1]++; else hidx[hfill[p]++] = (int32_t)(le * npair * 4 + pair_slot(i, j));
         }
       }
     }
@@ -615,13 +1070,30 @@ int mc_create(const fne_desc* d, McHandle** out) {
   MC_TRY(mc_upload(h, &h->row_gpos, row_gpos.data(), row_gpos.size()));
   {
     unsigned char* kb = nullptr;
-    MC_TRY(mc_upload(h, &kb, (const unsigned char*)nullptr, (size_t)nl * n * n * rsz));
+    MC_TRY(mc_upload(h, &kb, (const unsigned char*)nullptr, (size_t)nl * npair * 4 * rsz));
     h->Kbuf = kb;
     unsigned char* gb = nullptr;
     MC_TRY(mc_upload(h, &gb, (const unsigned char*)nullptr, (size_t)nl * n * rsz));
     h->gbuf = gb;
   }
   h->n_contrib = hptr[d->nnz];
+  // tensor-core path: FP32 P2 / P4 unless CUDA cores are requested
+  h->tc = d->precision == FNE_FP32 && np > 3 && d->kernel_variant != 1;
+  if (h->tc) {
+    std::vector<float> phi, plo;
+    int rc_tc = np == 15 ? mc_tc_prepare<15, 25>(h, d->e3, phi, plo) : mc_tc_prepare<6, 7>(h, d->e3, phi, plo);
+    if (rc_tc) {
+      mc_destroy(h);
+      return rc_tc;
+    }
+    MC_TRY(mc_upload(h, &h->Phi, phi.data(), phi.size()));
+    MC_TRY(mc_upload(h, &h->Plo, plo.data(), plo.size()));
+    MC_TRY(mc_upload(h, &h->err, (const int*)nullptr, 1));
+    if (cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess) {
+      mc_destroy(h);
+      return set_error(FNE_ECUDA, "Mohr-Coulomb: cudaMemset");
+    }
+  }
 #undef MC_TRY
   *out = h;
   return FNE_OK;
@@ -647,6 +1119,16 @@ int mc_set_dirichlet(McHandle* h, const double* dirichlet) {
   return FNE_OK;
 }
 
+int mc_check_status(McHandle* h) {
+  if (!h->err) return FNE_OK;
+  int v = 0;
+  cudaError_t e = cudaMemcpy(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("fne_check_device_status: ") + cudaGetErrorString(e));
+  if (v == 0) return FNE_OK;
+  cudaMemset(h->err, 0, sizeof(int));
+  return set_error(FNE_ETIMEOUT, "Mohr-Coulomb tensor-core kernel: an MMA completion wait gave up");
+}
+
 void mc_info(const McHandle* h, fne_info* info) {
   info->n_rows = h->n_rows;
   info->nnz = h->nnz;
@@ -654,7 +1136,7 @@ void mc_info(const McHandle* h, fne_info* info) {
   info->n_incidences = h->n_contrib;
   info->device_bytes = h->device_bytes;
   info->max_row_len = 0;
-  info->kernel_variant = 5;
+  info->kernel_variant = h->tc ? 6 : 5;
 }
 
 }  // namespace fne

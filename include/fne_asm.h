@@ -147,7 +147,11 @@ typedef struct {
                                  * free DOF (Ginzburg-Landau assembler,
                                  * src/problems/ginzburg_landau/jax_petsc/
                                  * reordered_element_assembler.py:34-52, 96-97) */
-  int32_t kernel_variant;       /* 0 = automatic; 1 = row-gather; 2 = incidence-parallel */
+  int32_t kernel_variant;       /* P1 families: 0 = automatic; 1 = row-gather;
+                                 * 2 = incidence-parallel.
+                                 * Mohr-Coulomb: 0 = automatic (tensor cores for
+                                 * FP32 P2/P4, CUDA cores otherwise);
+                                 * 1 = CUDA cores only.                        */
 } fne_desc;
 
 typedef struct fne_handle fne_handle;
@@ -159,11 +163,20 @@ typedef struct {
   int64_t n_incidences; /* (row-node, element) pairs in the gather plan        */
   int64_t device_bytes; /* device memory the handle owns                       */
   int32_t max_row_len;
-  int32_t kernel_variant;
+  int32_t kernel_variant; /* 1 row-gather (triangles), 2 row-gather (tets),
+                           * 3 incidence-parallel, 4 banded sweep,
+                           * 5 Mohr-Coulomb CUDA cores, 6 Mohr-Coulomb tcgen05 */
 } fne_info;
 
 int fne_create(const fne_desc* desc, fne_handle** out);
 int fne_info_get(const fne_handle* h, fne_info* info);
+/*
+ * Synchronous read of the handle's device status word (kernels that wait on
+ * the tensor core record a bounded wait that gave up there instead of
+ * hanging).  FNE_OK, or FNE_ETIMEOUT (the word is then cleared).  No
+ * counterpart in the reference, whose element kernels run on the CPU.
+ */
+int fne_check_device_status(fne_handle* h);
 /* Replace the Dirichlet values; ``dirichlet`` is a host array [n_total]. */
 int fne_set_dirichlet(fne_handle* h, const double* dirichlet);
 /*

@@ -106,3 +106,46 @@ def test_mc_energy_only_and_repeatability():
     assert torch.equal(h1, h2) and torch.equal(g1, g2) and torch.equal(e1, e2)
     e_only = gpu.eval(u, _lib.FNE_ENERGY)[0].clone()
     assert torch.equal(e_only, e1)
+
+
+@pytest.mark.parametrize("degree", [2, 4])
+def test_mc_tensor_core_path(degree):
+    """FP32 P2 / P4 runs the tcgen05 kernel (3xTF32 Bt.D.B): same FP32
+    tolerances against the FP64 oracle, agreement with the CUDA-core FP32
+    kernel, bit-repeatable, and the device status word stays clear."""
+    params = meshes.slope_problem(level=2, degree=degree, lam=1.2, with_elem_B=True)
+    gpu, ref = _pair(params, precision="fp32", hess_dtype=torch.float32)
+    assert gpu.info["kernel_variant"] == 6
+    cc, _ = _pair(params, precision="fp32", hess_dtype=torch.float32, kernel_variant="cuda_cores")
+    assert cc.info["kernel_variant"] == 5
+    np.testing.assert_array_equal(gpu.layout.owned_cols, cc.layout.owned_cols)
+    u = 0.05 * np.random.default_rng(11).standard_normal(gpu.layout.n_free)
+    e_ref, g_ref, h_ref = ref.all_in_one(u)
+    ut = torch.as_tensor(u, device="cuda")
+    e, g, h = [t.clone() for t in gpu.eval(ut, 7)]
+    gpu.check_device_status()
+    assert abs(float(e.item()) - e_ref) <= 1e-5 * _abs_scale(ref, u)
+    assert _rel(g.cpu().numpy(), g_ref) <= 1e-4
+    assert _rel(h.double().cpu().numpy(), h_ref) <= 2e-5
+    e2, g2, h2 = gpu.eval(ut, 7)
+    assert torch.equal(h, h2) and torch.equal(g, g2) and torch.equal(e, e2)
+    ec, gc, hc = cc.eval(ut, 7)
+    assert _rel(h.double().cpu().numpy(), hc.double().cpu().numpy()) <= 2e-5
+    # energy-only and gradient-only passes use the CUDA-core kernel and agree
+    assert abs(float(gpu.eval(ut, _lib.FNE_ENERGY)[0].item()) - float(e.item())) <= 1e-6 * _abs_scale(ref, u)
+    gg = gpu.eval(ut, _lib.FNE_GRAD)[1]
+    assert _rel(gg.cpu().numpy(), g.cpu().numpy()) <= 1e-5
+
+
+def test_mc_tensor_core_hessian_only_and_plastic_mix():
+    """Hessian-only pass through the tensor-core kernel at a state with
+    elastic, line-return and apex points; ragged last tile (element count not
+    a multiple of the tile)."""
+    params = meshes.slope_problem(level=1, degree=4, lam=1.3, with_elem_B=True)
+    gpu, ref = _pair(params, precision="fp32", hess_dtype=torch.float32)
+    assert gpu.info["n_elem"] % 24 != 0
+    u = 0.2 * np.random.default_rng(12).standard_normal(gpu.layout.n_free)
+    _, _, h_ref = ref.all_in_one(u)
+    h = gpu.eval(torch.as_tensor(u, device="cuda"), _lib.FNE_HESS)[2]
+    gpu.check_device_status()
+    assert _rel(h.double().cpu().numpy(), h_ref) <= 2e-5
