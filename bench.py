@@ -174,6 +174,10 @@ class Workload:
         return "f64"
 
 
+# kernel choice passed to the assembler ("auto" unless --kernel-variant is given)
+KERNEL_VARIANT = {"value": "auto"}
+
+
 def _reordered(asm, u_free):
     import numpy as np
 
@@ -211,10 +215,10 @@ def _tri(kind, n, precision, seed_from_rank=True):
         hd = torch.float32 if precision == "fp32" else torch.float64
         if kind == "gl":
             params, u0 = meshes.gl_problem(n=n, seed=rank)
-            asm = GLCudaAssembler(params, precision=precision, hess_dtype=hd)
+            asm = GLCudaAssembler(params, precision=precision, hess_dtype=hd, kernel_variant=KERNEL_VARIANT["value"])
         else:
             params, u0 = meshes.plaplace_problem(n=n, seed=None)
-            asm = PLaplaceCudaAssembler(params, precision=precision, hess_dtype=hd)
+            asm = PLaplaceCudaAssembler(params, precision=precision, hess_dtype=hd, kernel_variant=KERNEL_VARIANT["value"])
         return asm, _reordered(asm, u0)
 
     def sample():
@@ -239,7 +243,7 @@ def _he(nx, ny, nz, precision, theta=4.0 * 3.141592653589793 / 24.0):
 
         params, _ = meshes.he_beam_problem(nx=nx, ny=ny, nz=nz)
         hd = torch.float32 if precision == "fp32" else torch.float64
-        asm = HECudaAssembler(params, precision=precision, hess_dtype=hd)
+        asm = HECudaAssembler(params, precision=precision, hess_dtype=hd, kernel_variant=KERNEL_VARIANT["value"])
         pos = twisted_beam_positions(params, theta)
         asm.update_dirichlet(pos)
         return asm, _reordered(asm, pos[params["freedofs"]])
@@ -266,7 +270,8 @@ def _mc(degree, h, precision):
 
         params = meshes.slope_problem(h=h, degree=degree, lam=1.0)
         hd = torch.float32 if precision == "fp32" else torch.float64
-        asm = SlopeStabilityCudaAssembler(params, precision=precision, hess_dtype=hd)
+        asm = SlopeStabilityCudaAssembler(params, precision=precision, hess_dtype=hd,
+                                          kernel_variant=KERNEL_VARIANT["value"])
         return asm, _reordered(asm, slope_state(params)[params["freedofs"]])
 
     def sample():
@@ -322,8 +327,8 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "gl1024_fp32h"
 
-KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri", 5: "k_mc_elem+k_mc_gather",
-                6: "k_mc_tc+k_mc_gather"}
+KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri", 5: "k_mc_elem+k_node_gather",
+                6: "k_mc_tc+k_node_gather", 7: "k_he_elem+k_node_gather"}
 
 
 def algorithmic_bytes(w, asm, n_el):
@@ -498,7 +503,8 @@ def run(args):
                          "traffic": traffic[0] if traffic else None,
                          "traffic_source": traffic[1] if traffic else None,
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": kname, "launches_per_pass": launches_per_pass},
+                         "kernel": kname, "kernel_variant": args.kernel_variant,
+                         "launches_per_pass": launches_per_pass},
             "e2e": {"value": e2e_value, "unit": "elements/s",
                     "h2d_bytes_per_step": int(u0.nbytes),
                     "d2h_bytes_per_step": int(8 + host_g.numel() * 8 + host_h.numel() * host_h.element_size())},
@@ -522,7 +528,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-variant", default="auto", choices=["auto", "row_gather", "incidence", "element", "cuda_cores"])
     args = ap.parse_args()
+    KERNEL_VARIANT["value"] = args.kernel_variant
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":

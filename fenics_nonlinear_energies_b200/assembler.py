@@ -125,7 +125,8 @@ class CudaElementAssemblerBase:
             d.s[i] = float(v)
         d.nq = int(self._nq())
         d.dirichlet_only_energy = 1 if (self._adds_dirichlet_only_energy() and self.rank == 0) else 0
-        d.kernel_variant = {"auto": 0, "row_gather": 1, "incidence": 2, "cuda_cores": 1}[kernel_variant]
+        d.kernel_variant = {"auto": 0, "row_gather": 1, "incidence": 2, "element": 2,
+                            "cuda_cores": 1}[kernel_variant]
         self._handle = _lib.C.c_void_p()
         check(lib.fne_create(_lib.C.byref(d), _lib.C.byref(self._handle)))
         del keep
@@ -166,11 +167,11 @@ class CudaElementAssemblerBase:
 
     def launches_per_eval(self, flags):
         """Kernel launches one ``eval(u, flags)`` issues: one fused kernel for the
-        P1 families; element kernel plus Hessian and gradient gathers for
-        Mohr-Coulomb."""
-        if self.info["kernel_variant"] not in (5, 6):
+        triangle families and the tet row-gather kernel; element kernel plus one
+        node-block gather for Mohr-Coulomb and the element-parallel tet pass."""
+        if self.info["kernel_variant"] not in (5, 6, 7) or flags == _lib.FNE_ENERGY:
             return 1
-        return 1 + int(bool(flags & _lib.FNE_HESS)) + int(bool(flags & _lib.FNE_GRAD))
+        return 2
 
     # ---- vector helpers -----------------------------------------------------
     def _stream(self):

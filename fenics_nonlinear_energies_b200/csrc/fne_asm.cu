@@ -28,6 +28,7 @@
 #include <mutex>
 #include <string>
 
+#include "fne_gather.cuh"
 #include "fne_internal.h"
 
 namespace fne {
@@ -631,6 +632,98 @@ __global__ void __launch_bounds__(kTetRows) k_rows_tet(RowArgs A, const Chunk* _
 }
 
 // ---------------------------------------------------------------------------
+// Element-parallel Neo-Hookean pass (P1 tets, kernel_variant 2): one thread evaluates
+// one tetrahedron once -- FP64 energy, the 12 gradient entries and the 10
+// node-pair blocks (a <= b) of the element Hessian,
+//   H_(a,c),(b,d) = vol [2 C1 (g_a . g_b) delta_cd + c2 (cof g_a)_c (cof g_b)_d
+//                        + c3 eps_cdm (F (g_a x g_b))_m],
+// stored per element (90 + 12 values); k_node_gather (fne_gather.cuh) then
+// sums them per output block of the owned COO values and per gradient row in
+// a fixed order (no atomics, deterministic), replacing the reference's
+// np.add.at scatter.
+// ---------------------------------------------------------------------------
+constexpr int kHePairs = 10;
+constexpr int kHeSlots = 9 * kHePairs;
+
+template <typename Real, int WANT>
+__global__ void __launch_bounds__(256) k_he_elem(const Chunk* __restrict__ R, int n_el, const double* __restrict__ u,
+                                                 const double* __restrict__ dir, Phys P, Real* __restrict__ kbuf,
+                                                 Real* __restrict__ gbuf, const double* __restrict__ rhs,
+                                                 int n_owned, long long lo, EnergyOut eo) {
+  double eacc = 0.0;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += gridDim.x * blockDim.x) {
+    TetElem<Real> t;
+    load_tet(R, n_el, e, t);
+    double yd[4][3];
+    Real y[4][3];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        yd[b][d] = gather(u, dir, t.src[b], d);
+        y[b][d] = (Real)yd[b][d];
+      }
+    if ((WANT & W_E) && t.wflag) eacc += he_energy<Real>(P, yd, t);
+    if (!(WANT & (W_G | W_H))) continue;
+    HeState<Real> S;
+    he_state(P, y, t, S);
+    const Real C1 = prm<Real>(P.C1, P.C1f);
+    Real cg[4][3];  // (cof g_a)_c
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        cg[a][c] = S.cof[c][0] * t.g[a][0] + S.cof[c][1] * t.g[a][1] + S.cof[c][2] * t.g[a][2];
+    if (WANT & W_G) {
+      Real* gb = gbuf + (long long)e * 12;
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const Real Fg = S.F[c][0] * t.g[a][0] + S.F[c][1] * t.g[a][1] + S.F[c][2] * t.g[a][2];
+          gb[a * 3 + c] = t.vol * (Real(2) * C1 * Fg + S.c3 * cg[a][c]);
+        }
+    }
+    if (WANT & W_H) {
+      Real* kb = kbuf + (long long)e * kHeSlots;
+      const Real k1 = t.vol * Real(2) * C1, k2 = t.vol * S.c2, k3 = t.vol * S.c3;
+      int pr = 0;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int b = a; b < 4; ++b, ++pr) {
+          const Real* ga = t.g[a];
+          const Real* gbv = t.g[b];
+          const Real dot = ga[0] * gbv[0] + ga[1] * gbv[1] + ga[2] * gbv[2];
+          const Real x0 = ga[1] * gbv[2] - ga[2] * gbv[1];
+          const Real x1 = ga[2] * gbv[0] - ga[0] * gbv[2];
+          const Real x2 = ga[0] * gbv[1] - ga[1] * gbv[0];
+          Real w[3];
+#pragma unroll
+          for (int m = 0; m < 3; ++m) w[m] = k3 * (S.F[m][0] * x0 + S.F[m][1] * x1 + S.F[m][2] * x2);
+          Real* o = kb + pr * 9;
+          o[0] = k2 * cg[a][0] * cg[b][0] + k1 * dot;
+          o[1] = k2 * cg[a][0] * cg[b][1] + w[2];
+          o[2] = k2 * cg[a][0] * cg[b][2] - w[1];
+          o[3] = k2 * cg[a][1] * cg[b][0] - w[2];
+          o[4] = k2 * cg[a][1] * cg[b][1] + k1 * dot;
+          o[5] = k2 * cg[a][1] * cg[b][2] + w[0];
+          o[6] = k2 * cg[a][2] * cg[b][0] + w[1];
+          o[7] = k2 * cg[a][2] * cg[b][1] - w[0];
+          o[8] = k2 * cg[a][2] * cg[b][2] + k1 * dot;
+        }
+      }
+    }
+  }
+  if (WANT & W_E) {
+    if (rhs)
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_owned; i += gridDim.x * blockDim.x)
+        eacc -= rhs[i] * u[lo + i];
+    energy_finalize(eacc, eo);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Incidence-parallel kernel (P1 triangles): one thread per (row, element)
 // incidence.  Each thread runs one short chain of independent loads
 // (incidence word -> element record -> 3 nodal values), evaluates the
@@ -1125,6 +1218,15 @@ struct fne_handle {
   int sw_gpos_identity = 0;
   unsigned *sw_ent_meta = nullptr, *sw_inc_word = nullptr;
   int inc_max_rank = 0, inc_max_rows = 0, inc_max_len = 0;
+  // element-parallel tet pass: per-element blocks + contribution lists
+  bool use_elem2 = false;
+  int grid_elem2 = 1;
+  void *e2_kbuf = nullptr, *e2_gbuf = nullptr;
+  int e2_rnodes = 0;
+  int *bp_rn_blk = nullptr, *bp_rn_con = nullptr, *bp_rn_row = nullptr, *bp_rn_gpos = nullptr,
+      *bp_rn_inc = nullptr, *bp_con = nullptr, *bp_inc = nullptr;
+  unsigned* bp_blk = nullptr;
+  int64_t e2_contrib = 0;
   Phys phys{};
   // device buffers
   Chunk* rec = nullptr;
@@ -1178,7 +1280,8 @@ void free_handle(fne_handle* h) {
                   h->sw_seg_row, h->sw_seg_elem, h->sw_seg_batch, h->sw_batch_done, h->sw_ent_ptr, h->sw_inc_base,
                   h->sw_ent_row, h->sw_ent_pos, h->sw_ent_meta, h->sw_inc_word,
                   h->dir, h->rhs, h->partials, h->dir_const, h->counter, h->h_u, h->h_grad, h->h_energy,
-                  h->h_hess};
+                  h->h_hess, h->e2_kbuf, h->e2_gbuf, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row,
+                  h->bp_rn_gpos, h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -1322,6 +1425,52 @@ cudaError_t launch_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad
   }
 #undef FNE_TET_CASE
   return cudaErrorInvalidValue;
+}
+
+template <typename Real, typename HOut>
+cudaError_t launch_elem2_t(fne_handle* h, int want, const double* u, double* grad, void* hess, EnergyOut eo,
+                           cudaStream_t st) {
+  Real* kb = static_cast<Real*>(h->e2_kbuf);
+  Real* gb = static_cast<Real*>(h->e2_gbuf);
+  const int n_owned = (int)(h->hi - h->lo);
+  const dim3 grid(h->grid_elem2), block(256);
+#define FNE_E2_CASE(W)                                                                                      \
+  case W:                                                                                                   \
+    k_he_elem<Real, W><<<grid, block, 0, st>>>(h->rec, h->n_local, u, h->dir, h->phys, kb, gb, h->rhs,      \
+                                               n_owned, h->lo, eo);                                         \
+    break;
+  switch (want) {
+    FNE_E2_CASE(2)
+    FNE_E2_CASE(3)
+    FNE_E2_CASE(4)
+    FNE_E2_CASE(5)
+    FNE_E2_CASE(6)
+    FNE_E2_CASE(7)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef FNE_E2_CASE
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (h->e2_rnodes == 0) return cudaSuccess;
+  NodeGatherArgs G{h->e2_rnodes, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
+                   h->bp_rn_inc, h->bp_blk, h->bp_con, h->bp_inc, h->rhs};
+  const int gg = std::max(1, std::min(h->num_sms * 16, (h->e2_rnodes + 7) / 8));
+  HOut* H = static_cast<HOut*>(hess);
+  if ((want & W_H) && (want & W_G))
+    k_node_gather<Real, HOut, 3, 4, true, true><<<gg, 256, 0, st>>>(G, kb, gb, H, grad);
+  else if (want & W_H)
+    k_node_gather<Real, HOut, 3, 4, true, false><<<gg, 256, 0, st>>>(G, kb, gb, H, grad);
+  else if (want & W_G)
+    k_node_gather<Real, HOut, 3, 4, false, true><<<gg, 256, 0, st>>>(G, kb, gb, H, grad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_elem2(fne_handle* h, int want, const double* u, double* grad, void* hess, EnergyOut eo,
+                         cudaStream_t st) {
+  if (h->precision == FNE_FP64) return launch_elem2_t<double, double>(h, want, u, grad, hess, eo, st);
+  if (h->hess_fp32) return launch_elem2_t<float, float>(h, want, u, grad, hess, eo, st);
+  return launch_elem2_t<float, double>(h, want, u, grad, hess, eo, st);
 }
 
 cudaError_t launch_rows(fne_handle* h, int want, const RowArgs& A, const IncArgs& Q, const SweepArgs& SW,
@@ -1589,6 +1738,36 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     FNE_TRY(upload(h, &h->inc_elem, plan.inc_elem.data(), plan.inc_elem.size()));
     FNE_TRY(upload(h, &h->inc_info, plan.inc_info.data(), plan.inc_info.size()));
   }
+  if (d->family == FNE_NEOHOOKEAN && d->kernel_variant == 2 && plan.n_rows > 0) {
+    // element-parallel pass + node-block gather on request (falls back to the
+    // row-gather kernel when the pattern is not node-blocked)
+    BlockPlan bp;
+    std::vector<int64_t> edofs((size_t)h->n_local * 12);
+    for (int32_t le = 0; le < h->n_local; ++le)
+      for (int i = 0; i < 12; ++i) edofs[(size_t)le * 12 + i] = d->elems[plan.local_elems[le] * 12 + i];
+    if (build_block_plan(h->n_local, 4, 3, edofs.data(), d, bp) == FNE_OK &&
+        (int64_t)h->n_local * kHeSlots < (int64_t)INT32_MAX) {
+      h->use_elem2 = true;
+      h->e2_rnodes = bp.n_rnodes;
+      h->e2_contrib = (int64_t)bp.con.size();
+      h->grid_elem2 = std::max(1, std::min(h->num_sms * 8, (h->n_local + 255) / 256));
+      h->n_partials = std::max(h->n_partials, h->grid_elem2);
+      FNE_TRY(upload(h, &h->bp_rn_blk, bp.rn_blk.data(), bp.rn_blk.size()));
+      FNE_TRY(upload(h, &h->bp_rn_con, bp.rn_con.data(), bp.rn_con.size()));
+      FNE_TRY(upload(h, &h->bp_rn_row, bp.rn_row.data(), bp.rn_row.size()));
+      FNE_TRY(upload(h, &h->bp_rn_gpos, bp.rn_gpos.data(), bp.rn_gpos.size()));
+      FNE_TRY(upload(h, &h->bp_rn_inc, bp.rn_inc.data(), bp.rn_inc.size()));
+      FNE_TRY(upload(h, &h->bp_blk, bp.blk.data(), bp.blk.size()));
+      FNE_TRY(upload(h, &h->bp_con, bp.con.data(), bp.con.size()));
+      FNE_TRY(upload(h, &h->bp_inc, bp.inc.data(), bp.inc.size()));
+      unsigned char* kb = nullptr;
+      FNE_TRY(dalloc(h, &kb, (size_t)h->n_local * kHeSlots * real_size));
+      h->e2_kbuf = kb;
+      unsigned char* gb = nullptr;
+      FNE_TRY(dalloc(h, &gb, (size_t)h->n_local * 12 * real_size));
+      h->e2_gbuf = gb;
+    }
+  }
   FNE_TRY(upload(h, &h->dir, d->dirichlet, (size_t)d->n_total));
   if (d->rhs_owned) FNE_TRY(upload(h, &h->rhs, d->rhs_owned, (size_t)(d->hi - d->lo)));
   FNE_TRY(dalloc(h, &h->partials, (size_t)h->n_partials));
@@ -1633,7 +1812,8 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   info->n_incidences = h->n_inc;
   info->device_bytes = h->device_bytes;
   info->max_row_len = h->max_row_len;
-  info->kernel_variant = is_tri(h->family) ? (h->use_sweep ? 4 : (h->use_inc ? 3 : 1)) : 2;
+  info->kernel_variant = is_tri(h->family) ? (h->use_sweep ? 4 : (h->use_inc ? 3 : 1)) : (h->use_elem2 ? 7 : 2);
+  if (h->use_elem2) info->n_incidences = h->e2_contrib;
   return FNE_OK;
 }
 
@@ -1687,7 +1867,8 @@ extern "C" int fne_eval(fne_handle* h, const double* u, int flags, double* energ
                  h->sw_ent_ptr,  h->sw_inc_base,  h->sw_ent_row,    h->sw_ent_pos,
                  h->sw_ent_meta, h->sw_inc_word,  h->sweep_win_mask, h->sweep_rwin_mask,
                  h->sw_gpos_identity};
-    e = launch_rows(h, flags, A, Q, SW, grad, hess, eo, st, false);
+    e = h->use_elem2 ? launch_elem2(h, flags, u, grad, hess, eo, st)
+                     : launch_rows(h, flags, A, Q, SW, grad, hess, eo, st, false);
   }
   if (e != cudaSuccess) return cuda_fail(e, "fne_eval launch");
   return FNE_OK;

@@ -108,6 +108,30 @@ struct SweepPlan {
 // does not fit (window larger than max_win_entries, rows longer than 126...).
 bool build_sweep_plan(RowPlan& P, int nb, int n_seg, int max_win_entries, int max_win_rows, SweepPlan& Q);
 
+// Node-block gather plan: the element matrices (stored per element as node
+// pairs a <= b of bs x bs blocks) are summed per output block (row node A,
+// column node B) -- the bs x bs values of rows (A, c) at columns (B, d).
+// Row node k owns blocks [rn_blk[k], rn_blk[k+1]) in the order of their
+// columns inside its rows, and contributions [rn_con[k], rn_con[k+1]).
+// blk word: bits 0-15 column offset of node B's first free column inside the
+// rows of A, bits 16-18 mask of B's free components, bits 19-31 number of
+// contributions.  con: el * npn^2 + a * npn + b (local element el, local
+// nodes a of A and b of B), element order within a block.  rn_row / rn_gpos:
+// COO start position / gradient slot of row (A, c), -1 when that DOF is not
+// an owned free row.  inc: el * npn + a per (row node, element) incidence.
+struct BlockPlan {
+  int32_t n_rnodes = 0;
+  std::vector<int32_t> rn_blk, rn_con, rn_row, rn_gpos, rn_inc;
+  std::vector<uint32_t> blk;
+  std::vector<int32_t> con, inc;
+};
+
+// elem_dofs: [n_local * npn * bs] total DOFs (dof = bs * node + component) of
+// the local elements in kernel order.  Returns FNE_OK, or FNE_ELAYOUT /
+// FNE_EBOUNDS (set_error called) when the COO pattern is not node-blocked or
+// exceeds the packed format.
+int build_block_plan(int64_t n_local, int npn, int bs, const int64_t* elem_dofs, const fne_desc* d, BlockPlan& P);
+
 // Mohr-Coulomb (plane strain, Pk triangles) handle, csrc/fne_mc.cu.
 struct McHandle;
 int mc_create(const fne_desc* d, McHandle** out);

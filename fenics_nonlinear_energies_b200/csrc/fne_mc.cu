@@ -19,11 +19,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
 
+#include "fne_gather.cuh"
 #include "fne_internal.h"
 
 namespace fne {
@@ -438,15 +440,15 @@ struct McTile {
   static constexpr int KP = (KK + 7) / 8 * 8;       // padded to the MMA K step (8 tf32)
   static constexpr int M = 128;                     // node pairs (padded)
   static constexpr int TE = NP > 6 ? 24 : 64;       // elements per tile
-  static constexpr int N = 4 * TE;                  // (e, c, d)
+  static constexpr int N = 4 * TE;                  // (c, d, e): row (c * 2 + d) * TE + e
   static constexpr int TMEM_COLS = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
-  static constexpr int THREADS = 256;
+  static constexpr int THREADS = NP > 6 ? 512 : 256;
   static constexpr int MIN_BLOCKS = NP > 6 ? 1 : 2;
   // shared memory (bytes); operand buffers first (16-byte aligned)
   static constexpr int A_BYTES = M * KP * 4;
   static constexpr int B_BYTES = N * KP * 4;
   static constexpr int OFF_AHI = 0, OFF_ALO = A_BYTES, OFF_BHI = 2 * A_BYTES, OFF_BLO = 2 * A_BYTES + B_BYTES;
-  static constexpr int OFF_S = 2 * A_BYTES + 2 * B_BYTES;          // [TE][NQ][4] gradient helper
+  static constexpr int OFF_S = 2 * A_BYTES + 2 * B_BYTES;          // [NQ][TE][4] gradient helper
   static constexpr int OFF_R = OFF_S + TE * NQ * 16;                // dh1, dh2 [NQ * NP], qw [NQ]
   static constexpr int OFF_U = OFF_R + ((2 * NQ * NP + NQ) * 4 + 15) / 16 * 16;  // [TE][2 NP]
   static constexpr int OFF_G = OFF_U + (TE * 2 * NP * 4 + 15) / 16 * 16;          // [TE][5]
@@ -465,17 +467,19 @@ struct McTcArgs {
 };
 
 template <int NP, int NQ, int WANT>
-__global__ void __launch_bounds__(256, McTile<NP, NQ>::MIN_BLOCKS)
+__global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_BLOCKS)
     k_mc_tc(McArgs A, McConstR<float> C, McTcArgs T, float* __restrict__ Kbuf, float* __restrict__ gbuf,
             double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ eout) {
   using G = McTile<NP, NQ>;
-  constexpr int N2 = 2 * NP, TE = G::TE, N = G::N, M = G::M, KP = G::KP, NPAIR = G::NPAIR;
+  constexpr int N2 = 2 * NP, TE = G::TE, N = G::N, M = G::M, KP = G::KP, NPAIR = G::NPAIR, NT = G::THREADS;
+  constexpr int UPT = (TE * N2 + NT - 1) / NT;  // nodal values per thread (prefetch)
+  constexpr int GPT = (TE * 5 + NT - 1) / NT;   // geometry values per thread (prefetch)
   extern __shared__ __align__(1024) unsigned char smem[];
   float* sAhi = reinterpret_cast<float*>(smem + G::OFF_AHI);
   float* sAlo = reinterpret_cast<float*>(smem + G::OFF_ALO);
   float* sBhi = reinterpret_cast<float*>(smem + G::OFF_BHI);
   float* sBlo = reinterpret_cast<float*>(smem + G::OFF_BLO);
-  float4* sS = reinterpret_cast<float4*>(smem + G::OFF_S);
+  float4* sS = reinterpret_cast<float4*>(smem + G::OFF_S);  // [NQ][TE]
   float* sD1 = reinterpret_cast<float*>(smem + G::OFF_R);
   float* sD2 = sD1 + NQ * NP;
   float* sW = sD2 + NQ * NP;
@@ -492,21 +496,21 @@ __global__ void __launch_bounds__(256, McTile<NP, NQ>::MIN_BLOCKS)
     const float4* pl = reinterpret_cast<const float4*>(T.Plo);
     float4* ah = reinterpret_cast<float4*>(sAhi);
     float4* al = reinterpret_cast<float4*>(sAlo);
-    for (int i = tid; i < M * KP / 4; i += blockDim.x) {
+    for (int i = tid; i < M * KP / 4; i += NT) {
       ah[i] = ph[i];
       al[i] = pl[i];
     }
     // B padding chunks (k >= KK) stay zero for the whole kernel
-    for (int i = tid; i < (KP - G::KK) / 4 * N; i += blockDim.x) {
+    for (int i = tid; i < (KP - G::KK) / 4 * N; i += NT) {
       const int off = (G::KK / 4) * N * 4 + i * 4;
       reinterpret_cast<float4*>(sBhi + off)[0] = make_float4(0.f, 0.f, 0.f, 0.f);
       reinterpret_cast<float4*>(sBlo + off)[0] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    for (int i = tid; i < NQ * NP; i += blockDim.x) {
+    for (int i = tid; i < NQ * NP; i += NT) {
       sD1[i] = (float)A.dhat1[i];
       sD2[i] = (float)A.dhat2[i];
     }
-    for (int i = tid; i < NQ; i += blockDim.x) sW[i] = (float)A.qw[i];
+    for (int i = tid; i < NQ; i += NT) sW[i] = (float)A.qw[i];
   }
   const uint32_t bar = tc::smem_u32(sBar);
   if (tid == 0) {
@@ -519,32 +523,57 @@ __global__ void __launch_bounds__(256, McTile<NP, NQ>::MIN_BLOCKS)
   tc::fence_after();
   const uint32_t tmem = *sTmem;
   constexpr uint32_t idesc = tc::idesc_tf32(M, N);
+  const int n_tiles = (A.n_el + TE - 1) / TE;
+
+  // register prefetch of one tile's gather codes, nodal values and geometry
+  int cv[UPT];
+  float uv[UPT], gv[GPT];
+  auto fetch_codes = [&](int tile) {
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+      const int i = tid + k * NT, el = i / N2;
+      const int e = tile * TE + el;
+      cv[k] = (tile < n_tiles && i < TE * N2 && e < A.n_el) ? __ldg(A.codes + (long long)e * N2 + (i - el * N2))
+                                                             : INT_MIN;
+    }
+#pragma unroll
+    for (int k = 0; k < GPT; ++k) {
+      const int i = tid + k * NT, el = i / 5;
+      const int e = tile * TE + el;
+      gv[k] = (tile < n_tiles && i < TE * 5 && e < A.n_el) ? (float)__ldg(A.geom + (long long)tile * TE * 5 + i)
+                                                           : 0.f;
+    }
+  };
+  auto fetch_values = [&]() {
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+      const int c = cv[k];
+      uv[k] = c == INT_MIN ? 0.f : (float)(c >= 0 ? __ldg(A.u + c) : __ldg(A.dir + (-1 - c)));
+    }
+  };
+  auto stash = [&]() {
+#pragma unroll
+    for (int k = 0; k < UPT; ++k)
+      if (tid + k * NT < TE * N2) sU[tid + k * NT] = uv[k];
+#pragma unroll
+    for (int k = 0; k < GPT; ++k)
+      if (tid + k * NT < TE * 5) sGm[tid + k * NT] = gv[k];
+  };
 
   double eacc = 0.0;
   uint32_t phase = 0;
-  const int n_tiles = (A.n_el + TE - 1) / TE;
+  fetch_codes(blockIdx.x);
+  fetch_values();
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int e0 = tile * TE;
     const int ne = min(TE, A.n_el - e0);
-    // (1) nodal values and element geometry of the tile
-    for (int i = tid; i < TE * N2; i += blockDim.x) {
-      const int el = i / N2;
-      float v = 0.f;
-      if (el < ne) {
-        const int code = A.codes[(long long)(e0 + el) * N2 + (i - el * N2)];
-        v = (float)(code >= 0 ? A.u[code] : A.dir[-1 - code]);
-      }
-      sU[i] = v;
-    }
-    for (int i = tid; i < TE * 5; i += blockDim.x) {
-      const int el = i / 5;
-      sGm[i] = el < ne ? (float)A.geom[(long long)e0 * 5 + i] : 0.f;
-    }
+    // (1) nodal values and element geometry of the tile (prefetched)
+    stash();
     __syncthreads();
-    // (2) constitutive update per (element, quadrature point) -> At (B operand), gradient helper
-    for (int p = tid; p < TE * NQ; p += blockDim.x) {
-      const int el = p / NQ, q = p - el * NQ;
-      float4 at[4];  // (c, d) blocks: [k * 2 + l]
+    // (2) constitutive update per (quadrature point, element) -> At (B operand rows j * TE + el), helper
+    for (int p = tid; p < TE * NQ; p += NT) {
+      const int q = p / TE, el = p - q * TE;
+      float4 at[4];  // (c, d) blocks j = c * 2 + d: [k * 2 + l]
       float4 sg = make_float4(0.f, 0.f, 0.f, 0.f);
       if (el < ne) {
         const float* gm = sGm + el * 5;
@@ -596,20 +625,18 @@ __global__ void __launch_bounds__(256, McTile<NP, NQ>::MIN_BLOCKS)
           }
         }
         // gradient helper s[c][k] = w sum_i Mx[i][k] sigma[v(c, i)]
-        const float s00 = w * (Mx[0][0] * sig[0] + Mx[1][0] * sig[2]);
-        const float s01 = w * (Mx[0][1] * sig[0] + Mx[1][1] * sig[2]);
-        const float s10 = w * (Mx[0][0] * sig[2] + Mx[1][0] * sig[1]);
-        const float s11 = w * (Mx[0][1] * sig[2] + Mx[1][1] * sig[1]);
-        sg = make_float4(s00, s01, s10, s11);
+        sg = make_float4(w * (Mx[0][0] * sig[0] + Mx[1][0] * sig[2]), w * (Mx[0][1] * sig[0] + Mx[1][1] * sig[2]),
+                         w * (Mx[0][0] * sig[2] + Mx[1][0] * sig[1]), w * (Mx[0][1] * sig[2] + Mx[1][1] * sig[1]));
       } else {
 #pragma unroll
         for (int j = 0; j < 4; ++j) at[j] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
-      sS[el * NQ + q] = sg;
-      // B operand rows n = el * 4 + (c * 2 + d), K chunk q (16 bytes: k * 2 + l)
+      sS[q * TE + el] = sg;
+      // B operand row n = j * TE + el, K chunk q (16 bytes: k * 2 + l); consecutive
+      // threads (elements) write consecutive 16-byte rows
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const int off = q * N * 4 + (el * 4 + j) * 4;
+        const int off = q * N * 4 + (j * TE + el) * 4;
         const float4 v = at[j];
         const float4 hi = make_float4(tc::tf32_hi(v.x), tc::tf32_hi(v.y), tc::tf32_hi(v.z), tc::tf32_hi(v.w));
         reinterpret_cast<float4*>(sBhi + off)[0] = hi;
@@ -635,45 +662,55 @@ __global__ void __launch_bounds__(256, McTile<NP, NQ>::MIN_BLOCKS)
       }
       tc::commit(bar);
     }
+    // next tile's gather codes and geometry in flight during the gradient / epilogue
+    fetch_codes(tile + gridDim.x);
     // (4) element gradient on the CUDA cores while the MMAs run
     if (WANT & MW_G) {
-      for (int i = tid; i < TE * N2; i += blockDim.x) {
+      for (int i = tid; i < TE * N2; i += NT) {
         const int el = i / N2, r = i - el * N2, a = r >> 1, c = r & 1;
         if (el >= ne) continue;
         float acc = 0.f;
 #pragma unroll 5
         for (int q = 0; q < NQ; ++q) {
-          const float4 s = sS[el * NQ + q];
+          const float4 s = sS[q * TE + el];
           const float r1 = sD1[q * NP + a], r2 = sD2[q * NP + a];
           acc += c == 0 ? r1 * s.x + r2 * s.y : r1 * s.z + r2 * s.w;
         }
         gbuf[(long long)(e0 + el) * N2 + r] = acc;
       }
     }
-    // (5) epilogue: TMEM -> Kbuf[e][pair][c * 2 + d]
+    fetch_values();
+    // (5) epilogue: TMEM -> Kbuf[e][pair][c * 2 + d]; warp w reads lanes 32 (w % 4) ..
+    // (node pairs) for its share of the tile's elements
     if (WANT & MW_H) {
       if (tc::mbar_wait(bar, phase, kMcWaitLimit))
         phase ^= 1u;
       else if (lane == 0)
         atomicExch(sFail, 1);
       tc::fence_after();
-      const int quad = warp & 3, half = warp >> 2;
+      constexpr int NGRP = NT / 128, EPG = TE / NGRP;  // element groups, elements per group
+      const int quad = warp & 3, grp = warp >> 2;
       const int m = quad * 32 + lane;
       if (!*sFail && quad * 32 < NPAIR) {
-        constexpr int COLS = N / 2;  // columns per warp half
 #pragma unroll 1
-        for (int c0 = 0; c0 < COLS; c0 += 16) {
-          float v[16];
-          const int col = half * COLS + c0;
-          tc::tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)col, v);
+        for (int el = grp * EPG; el < (grp + 1) * EPG; el += 2) {
+          uint32_t r[4][2];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(j * TE + el);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];"
+                         : "=r"(r[j][0]), "=r"(r[j][1])
+                         : "r"(ta)
+                         : "memory");
+          }
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
           if (m < NPAIR) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const int el = (col >> 2) + j;
-              if (el < ne)
-                reinterpret_cast<float4*>(Kbuf + ((long long)(e0 + el) * NPAIR + m) * 4)[0] =
-                    make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-            }
+            for (int x = 0; x < 2; ++x)
+              if (el + x < ne)
+                reinterpret_cast<float4*>(Kbuf + ((long long)(e0 + el + x) * NPAIR + m) * 4)[0] =
+                    make_float4(__uint_as_float(r[0][x]), __uint_as_float(r[1][x]), __uint_as_float(r[2][x]),
+                                __uint_as_float(r[3][x]));
           }
         }
       }
@@ -693,7 +730,7 @@ __global__ void __launch_bounds__(256, McTile<NP, NQ>::MIN_BLOCKS)
   if (warp == 0) tc::tmem_dealloc(tmem, G::TMEM_COLS);
   if (WANT & MW_E) {
     if (A.rhs)
-      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_owned; i += gridDim.x * blockDim.x)
+      for (int i = blockIdx.x * NT + threadIdx.x; i < A.n_owned; i += gridDim.x * NT)
         eacc -= A.rhs[i] * A.u[A.lo + i];
     mc_energy_finalize(eacc, partials, counter, eout);
   }
@@ -738,6 +775,11 @@ struct McHandle {
   void *Kbuf = nullptr, *gbuf = nullptr;
   int grid_elem = 1, n_partials = 1;
   int64_t device_bytes = 0, n_contrib = 0;
+  // node-block gather (default) or per-position contribution lists
+  int use_blk = 0, n_rnodes = 0;
+  int *bp_rn_blk = nullptr, *bp_rn_con = nullptr, *bp_rn_row = nullptr, *bp_rn_gpos = nullptr,
+      *bp_rn_inc = nullptr, *bp_con = nullptr, *bp_inc = nullptr;
+  unsigned* bp_blk = nullptr;
   // tensor-core path (FP32, P2 / P4): constant operand halves, status word
   int tc = 0, grid_tc = 1;
   float *Phi = nullptr, *Plo = nullptr;
@@ -761,11 +803,25 @@ int mc_upload(McHandle* h, T** p, const T* src, size_t count) {
 }
 
 // Hessian / gradient gathers after the element kernel (checks its launch first).
-template <typename Real, typename HOut>
+template <typename Real, typename HOut, int NP>
 cudaError_t mc_gathers(McHandle* h, int flags, const Real* K, const Real* g, double* grad, void* hess,
                        cudaStream_t st) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (h->use_blk) {
+    if (h->n_rnodes == 0 || !(flags & (MW_G | MW_H))) return cudaSuccess;
+    NodeGatherArgs G{h->n_rnodes, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
+                     h->bp_rn_inc, h->bp_blk, h->bp_con, h->bp_inc, h->rhs};
+    const int grid = std::max(1, std::min(h->num_sms * 16, (h->n_rnodes + 7) / 8));
+    HOut* H = static_cast<HOut*>(hess);
+    if ((flags & MW_H) && (flags & MW_G))
+      k_node_gather<Real, HOut, 2, NP, true, true><<<grid, 256, 0, st>>>(G, K, g, H, grad);
+    else if (flags & MW_H)
+      k_node_gather<Real, HOut, 2, NP, true, false><<<grid, 256, 0, st>>>(G, K, g, H, grad);
+    else
+      k_node_gather<Real, HOut, 2, NP, false, true><<<grid, 256, 0, st>>>(G, K, g, H, grad);
+    return cudaGetLastError();
+  }
   const int gg = std::max(1, std::min(h->num_sms * 16, (int)((std::max<int64_t>(h->nnz, h->n_rows) + 255) / 256)));
   if ((flags & MW_H) && h->nnz > 0)
     k_mc_gather<Real, HOut><<<gg, 256, 0, st>>>((int)h->nnz, h->hptr, h->hidx, K, static_cast<HOut*>(hess));
@@ -809,7 +865,7 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
         case 6: k_mc_tc<NP, NQ, 6><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
         default: k_mc_tc<NP, NQ, 7><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
       }
-      return mc_gathers<float, HOut>(h, flags, K, g, grad, hess, st);
+      return mc_gathers<float, HOut, NP>(h, flags, K, g, grad, hess, st);
     }
   }
   switch (flags) {
@@ -822,7 +878,7 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
     case 7: k_mc_elem<Real, NP, NQ, 7><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
     default: return cudaErrorInvalidValue;
   }
-  return mc_gathers<Real, HOut>(h, flags, K, g, grad, hess, st);
+  return mc_gathers<Real, HOut, NP>(h, flags, K, g, grad, hess, st);
 }
 
 template <typename Real, typename HOut>
@@ -885,7 +941,8 @@ void mc_destroy(McHandle* h) {
   if (!h) return;
   void* ptrs[] = {h->codes, h->geom, h->epsp, h->dhat1, h->dhat2, h->qw, h->wflag, h->dir, h->rhs,
                   h->partials, h->counter, h->hptr, h->hidx, h->gptr, h->gidx, h->row_gpos, h->Kbuf, h->gbuf,
-                  h->Phi, h->Plo, h->err};
+                  h->Phi, h->Plo, h->err, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
+                  h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -931,9 +988,23 @@ int mc_create(const fne_desc* d, McHandle** out) {
     wflag.push_back(w != 0.0 ? 1 : 0);
   }
   const int64_t nl = (int64_t)local.size();
-  // rows of the owned COO pattern (row-grouped)
+  // node-block gather plan (default); per-position contribution lists below
+  // only when the pattern is not node-blocked
   const int64_t n_owned = hi - lo;
-  std::vector<int32_t> rowof(n_owned, -1), row_ptr, row_gpos;
+  BlockPlan bp;
+  bool use_blk = false;
+  {
+    std::vector<int64_t> edofs((size_t)nl * n);
+    for (int64_t le = 0; le < nl; ++le)
+      for (int i = 0; i < n; ++i) edofs[(size_t)le * n + i] = d->elems[local[le] * n + i];
+    use_blk = build_block_plan(nl, np, 2, edofs.data(), d, bp) == FNE_OK;
+  }
+  const int npair = np * (np + 1) / 2;
+  std::vector<int32_t> rowof, row_ptr, row_gpos;
+  std::vector<int32_t> hptr, gptr, hidx, gidx;
+  int32_t n_rows = 0;
+  if (!use_blk) {
+  rowof.assign(n_owned, -1);
   for (int64_t j = 0; j < d->nnz; ++j) {
     const int64_t r = d->owned_rows[j];
     if (r < lo || r >= hi) return set_error(FNE_EBOUNDS, "Mohr-Coulomb: owned row outside [lo, hi)");
@@ -951,7 +1022,7 @@ int mc_create(const fne_desc* d, McHandle** out) {
       row_gpos.push_back((int32_t)i);
     }
   row_ptr.push_back((int32_t)d->nnz);
-  const int32_t n_rows = (int32_t)row_gpos.size();
+  n_rows = (int32_t)row_gpos.size();
   // column lookup: positions of every row sorted by column id
   std::vector<int32_t> bycol(d->nnz);
   for (int32_t k = 0; k < n_rows; ++k) {
@@ -969,7 +1040,6 @@ int mc_create(const fne_desc* d, McHandle** out) {
   };
   // contributions (two passes: count, fill), in element order; element
   // matrices are stored per node pair a <= b: slot pair(a, b) * 4 + c * 2 + d
-  const int npair = np * (np + 1) / 2;
   auto pair_slot = [np](int i, int j) -> int {
     int a = i >> 1, c = i & 1, b = j >> 1, dd = j & 1;
     if (a > b) {
@@ -978,7 +1048,9 @@ int mc_create(const fne_desc* d, McHandle** out) {
     }
     return (a * np - a * (a - 1) / 2 + (b - a)) * 4 + c * 2 + dd;
   };
-  std::vector<int32_t> hptr(d->nnz + 1, 0), gptr(n_rows + 1, 0), hidx, gidx, hfill, gfill;
+  hptr.assign(d->nnz + 1, 0);
+  gptr.assign(n_rows + 1, 0);
+  std::vector<int32_t> hfill, gfill;
   for (int pass = 0; pass < 2; ++pass) {
     if (pass == 1) {
       for (int64_t p = 0; p < d->nnz; ++p) hptr[p + 1] += hptr[p];
@@ -1003,6 +1075,7 @@ int mc_create(const fne_desc* d, McHandle** out) {
       }
     }
   }
+  }  // !use_blk
 
   auto* h = new (std::nothrow) McHandle();
   if (!h) return set_error(FNE_ENOMEM, "Mohr-Coulomb: out of host memory");
@@ -1012,7 +1085,7 @@ int mc_create(const fne_desc* d, McHandle** out) {
   h->nq = nq;
   h->n = n;
   h->n_local = (int)nl;
-  h->n_rows = n_rows;
+  h->n_rows = use_blk ? (int32_t)n_owned : n_rows;
   h->nnz = d->nnz;
   h->lo = lo;
   h->hi = hi;
@@ -1063,6 +1136,18 @@ int mc_create(const fne_desc* d, McHandle** out) {
     mc_destroy(h);
     return set_error(FNE_ECUDA, "Mohr-Coulomb: cudaMemset");
   }
+  h->use_blk = use_blk ? 1 : 0;
+  if (use_blk) {
+    h->n_rnodes = bp.n_rnodes;
+    MC_TRY(mc_upload(h, &h->bp_rn_blk, bp.rn_blk.data(), bp.rn_blk.size()));
+    MC_TRY(mc_upload(h, &h->bp_rn_con, bp.rn_con.data(), bp.rn_con.size()));
+    MC_TRY(mc_upload(h, &h->bp_rn_row, bp.rn_row.data(), bp.rn_row.size()));
+    MC_TRY(mc_upload(h, &h->bp_rn_gpos, bp.rn_gpos.data(), bp.rn_gpos.size()));
+    MC_TRY(mc_upload(h, &h->bp_rn_inc, bp.rn_inc.data(), bp.rn_inc.size()));
+    MC_TRY(mc_upload(h, &h->bp_blk, bp.blk.data(), bp.blk.size()));
+    MC_TRY(mc_upload(h, &h->bp_con, bp.con.data(), bp.con.size()));
+    MC_TRY(mc_upload(h, &h->bp_inc, bp.inc.data(), bp.inc.size()));
+  }
   MC_TRY(mc_upload(h, &h->hptr, hptr.data(), hptr.size()));
   MC_TRY(mc_upload(h, &h->hidx, hidx.data(), hidx.size()));
   MC_TRY(mc_upload(h, &h->gptr, gptr.data(), gptr.size()));
@@ -1076,7 +1161,7 @@ int mc_create(const fne_desc* d, McHandle** out) {
     MC_TRY(mc_upload(h, &gb, (const unsigned char*)nullptr, (size_t)nl * n * rsz));
     h->gbuf = gb;
   }
-  h->n_contrib = hptr[d->nnz];
+  h->n_contrib = use_blk ? (int64_t)bp.con.size() : (int64_t)hptr[d->nnz];
   // tensor-core path: FP32 P2 / P4 unless CUDA cores are requested
   h->tc = d->precision == FNE_FP32 && np > 3 && d->kernel_variant != 1;
   if (h->tc) {

@@ -461,3 +461,175 @@ bool build_sweep_plan(RowPlan& P, int nb, int n_seg, int max_win_entries, int ma
 }
 
 }  // namespace fne
+
+namespace fne {
+
+int build_block_plan(int64_t n_local, int npn, int bs, const int64_t* elem_dofs, const fne_desc* d, BlockPlan& P) {
+  const int64_t lo = d->lo, hi = d->hi, nf = d->n_free, nnz = d->nnz, nt = d->n_total;
+  const int64_t* t2f = d->total_to_free_reord;
+  if (bs < 1 || bs > 3 || npn < 1 || (int64_t)npn * npn * n_local >= (int64_t)INT32_MAX ||
+      (int64_t)npn * n_local >= (int64_t)INT32_MAX || nnz >= (int64_t)INT32_MAX)
+    return set_error(FNE_EBOUNDS, "block plan: sizes beyond the packed format");
+  // reordered free id -> total DOF
+  std::vector<int64_t> orig(nf, -1);
+  for (int64_t t = 0; t < nt; ++t)
+    if (t2f[t] >= 0) orig[t2f[t]] = t;
+  const int64_t n_nodes = (nt + bs - 1) / bs;
+  // row nodes in the order of their first COO row
+  std::vector<int32_t> rn_of(n_nodes, -1);
+  std::vector<int64_t> rn_node;
+  P.rn_row.clear();
+  P.rn_gpos.clear();
+  std::vector<int32_t> row_end;  // per (rn, c): end position of the row
+  for (int64_t j = 0; j < nnz; ++j) {
+    if (j > 0 && d->owned_rows[j] == d->owned_rows[j - 1]) continue;
+    const int64_t r = d->owned_rows[j];
+    if (r < lo || r >= hi) return set_error(FNE_ELAYOUT, "block plan: owned row outside [lo, hi)");
+    const int64_t t = orig[r];
+    const int64_t node = t / bs;
+    const int c = (int)(t % bs);
+    if (rn_of[node] < 0) {
+      rn_of[node] = (int32_t)rn_node.size();
+      rn_node.push_back(node);
+      for (int k = 0; k < bs; ++k) {
+        P.rn_row.push_back(-1);
+        P.rn_gpos.push_back(-1);
+        row_end.push_back(-1);
+      }
+    }
+    const int32_t k = rn_of[node];
+    if (P.rn_row[k * bs + c] >= 0) return set_error(FNE_ELAYOUT, "block plan: COO pattern is not row-grouped");
+    P.rn_row[k * bs + c] = (int32_t)j;
+    P.rn_gpos[k * bs + c] = (int32_t)(r - lo);
+  }
+  const int32_t n_rn = (int32_t)rn_node.size();
+  for (int32_t k = 0; k < n_rn; ++k)
+    for (int c = 0; c < bs; ++c) {
+      const int32_t s0 = P.rn_row[k * bs + c];
+      if (s0 < 0) continue;
+      int64_t e = s0;
+      while (e < nnz && d->owned_rows[e] == d->owned_rows[s0]) ++e;
+      row_end[k * bs + c] = (int32_t)e;
+    }
+  // owned free rows without COO entries would be missed
+  for (int64_t r = lo; r < hi; ++r) {
+    const int64_t node = orig[r] / bs;
+    if (rn_of[node] < 0 || P.rn_row[rn_of[node] * bs + (int)(orig[r] % bs)] < 0)
+      return set_error(FNE_ELAYOUT, "block plan: owned row without COO entries");
+  }
+  P.n_rnodes = n_rn;
+  // column-node blocks of every row node: consecutive columns of one node
+  // form a block; all rows of the node must agree on the blocks
+  std::vector<int32_t> rn_blk(n_rn + 1, 0);
+  std::vector<int64_t> blk_node;
+  std::vector<uint32_t> blk_word;
+  for (int32_t k = 0; k < n_rn; ++k) {
+    rn_blk[k] = (int32_t)blk_node.size();
+    bool first_row = true;
+    size_t b_first = blk_node.size();
+    for (int c = 0; c < bs; ++c) {
+      const int32_t s0 = P.rn_row[k * bs + c];
+      if (s0 < 0) continue;
+      const int32_t s1 = row_end[k * bs + c];
+      size_t bi = b_first;
+      int64_t j = s0;
+      while (j < s1) {
+        const int64_t node = orig[d->owned_cols[j]] / bs;
+        const int64_t off = j - s0;
+        uint32_t mask = 0;
+        int prev = -1;
+        while (j < s1 && orig[d->owned_cols[j]] / bs == node) {
+          const int comp = (int)(orig[d->owned_cols[j]] % bs);
+          if (comp <= prev) return set_error(FNE_ELAYOUT, "block plan: node columns not in component order");
+          prev = comp;
+          mask |= 1u << comp;
+          ++j;
+        }
+        if (off > 0xFFFF) return set_error(FNE_EBOUNDS, "block plan: row longer than 65535 entries");
+        const uint32_t w = (uint32_t)off | (mask << 16);
+        if (first_row) {
+          blk_node.push_back(node);
+          blk_word.push_back(w);
+        } else {
+          if (bi >= blk_node.size() || blk_node[bi] != node || blk_word[bi] != w)
+            return set_error(FNE_ELAYOUT, "block plan: rows of one node differ in their columns");
+          ++bi;
+        }
+      }
+      if (!first_row && bi != blk_node.size())
+        return set_error(FNE_ELAYOUT, "block plan: rows of one node differ in their columns");
+      first_row = false;
+    }
+  }
+  rn_blk[n_rn] = (int32_t)blk_node.size();
+  // (row node, column node) -> block: per row node, blocks sorted by node
+  std::vector<int32_t> sorted_blk(blk_node.size());
+  for (int32_t k = 0; k < n_rn; ++k) {
+    for (int32_t b = rn_blk[k]; b < rn_blk[k + 1]; ++b) sorted_blk[b] = b;
+    std::sort(sorted_blk.begin() + rn_blk[k], sorted_blk.begin() + rn_blk[k + 1],
+              [&](int32_t x, int32_t y) { return blk_node[x] < blk_node[y]; });
+  }
+  auto find_blk = [&](int32_t k, int64_t node) -> int32_t {
+    int32_t a = rn_blk[k], b = rn_blk[k + 1];
+    while (a < b) {
+      const int32_t m = (a + b) >> 1;
+      if (blk_node[sorted_blk[m]] < node) a = m + 1; else b = m;
+    }
+    return (a < rn_blk[k + 1] && blk_node[sorted_blk[a]] == node) ? sorted_blk[a] : -1;
+  };
+  auto has_free = [&](int64_t node) {
+    for (int c = 0; c < bs; ++c) {
+      const int64_t t = node * bs + c;
+      if (t < nt && t2f[t] >= 0) return true;
+    }
+    return false;
+  };
+  // contributions (count, fill) in element order; gradient incidences
+  const int nde = npn * bs;
+  std::vector<int32_t> cnt(blk_node.size() + 1, 0), fill;
+  std::vector<int32_t> icnt(n_rn + 1, 0), ifill;
+  std::vector<int32_t> con, inc;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      for (size_t b = 0; b < blk_node.size(); ++b) cnt[b + 1] += cnt[b];
+      for (int32_t k = 0; k < n_rn; ++k) icnt[k + 1] += icnt[k];
+      con.assign(cnt[blk_node.size()], 0);
+      inc.assign(icnt[n_rn], 0);
+      fill.assign(cnt.begin(), cnt.end() - 1);
+      ifill.assign(icnt.begin(), icnt.end() - 1);
+    }
+    for (int64_t el = 0; el < n_local; ++el) {
+      const int64_t* ed = elem_dofs + el * nde;
+      for (int a = 0; a < npn; ++a) {
+        const int64_t na = ed[a * bs] / bs;
+        if (na < 0 || na >= n_nodes) return set_error(FNE_EBOUNDS, "block plan: element DOF out of range");
+        const int32_t k = rn_of[na];
+        if (k < 0) continue;
+        if (pass == 0) icnt[k + 1]++; else inc[ifill[k]++] = (int32_t)(el * npn + a);
+        for (int b = 0; b < npn; ++b) {
+          const int64_t nb = ed[b * bs] / bs;
+          if (!has_free(nb)) continue;
+          const int32_t blk = find_blk(k, nb);
+          if (blk < 0) return set_error(FNE_ELAYOUT, "Scatter lookup found mismatched owned COO entries");
+          if (pass == 0) cnt[blk + 1]++; else con[fill[blk]++] = (int32_t)((el * npn + a) * npn + b);
+        }
+      }
+    }
+  }
+  P.blk.resize(blk_node.size());
+  for (size_t b = 0; b < blk_node.size(); ++b) {
+    const int32_t c = cnt[b + 1] - cnt[b];
+    if (c >= (1 << 13)) return set_error(FNE_EBOUNDS, "block plan: more than 8191 contributions to one block");
+    P.blk[b] = blk_word[b] | ((uint32_t)c << 19);
+  }
+  P.rn_blk = std::move(rn_blk);
+  P.rn_con.assign(n_rn + 1, 0);
+  for (int32_t k = 0; k < n_rn; ++k) P.rn_con[k + 1] = cnt[P.rn_blk[k + 1]];
+  P.rn_con[0] = 0;
+  P.con = std::move(con);
+  P.rn_inc = std::move(icnt);
+  P.inc = std::move(inc);
+  return FNE_OK;
+}
+
+}  // namespace fne

@@ -147,8 +147,10 @@ typedef struct {
                                  * free DOF (Ginzburg-Landau assembler,
                                  * src/problems/ginzburg_landau/jax_petsc/
                                  * reordered_element_assembler.py:34-52, 96-97) */
-  int32_t kernel_variant;       /* P1 families: 0 = automatic; 1 = row-gather;
-                                 * 2 = incidence-parallel.
+  int32_t kernel_variant;       /* P1 triangles: 0 = automatic (banded sweep);
+                                 * 1 = row-gather; 2 = incidence-parallel.
+                                 * P1 tets: 0/1 = row-gather; 2 = element-
+                                 * parallel pass + node-block gather.
                                  * Mohr-Coulomb: 0 = automatic (tensor cores for
                                  * FP32 P2/P4, CUDA cores otherwise);
                                  * 1 = CUDA cores only.                        */
@@ -165,7 +167,8 @@ typedef struct {
   int32_t max_row_len;
   int32_t kernel_variant; /* 1 row-gather (triangles), 2 row-gather (tets),
                            * 3 incidence-parallel, 4 banded sweep,
-                           * 5 Mohr-Coulomb CUDA cores, 6 Mohr-Coulomb tcgen05 */
+                           * 5 Mohr-Coulomb CUDA cores, 6 Mohr-Coulomb tcgen05,
+                           * 7 element-parallel tets + node-block gather */
 } fne_info;
 
 int fne_create(const fne_desc* desc, fne_handle** out);

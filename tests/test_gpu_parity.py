@@ -208,3 +208,27 @@ def test_full_size_gl_properties():
     rows, cols = gpu.layout.owned_rows, gpu.layout.owned_cols
     A = sparse.coo_matrix((h.double().cpu().numpy(), (rows, cols)), shape=(gpu.layout.n_free,) * 2).tocsr()
     assert abs(A - A.T).max() <= 1e-6 * abs(A).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_he_element_pass_matches_row_gather(precision):
+    """The element-parallel tet pass (opt-in) and the row-gather kernel
+    (default) give the same values (FP64: 1e-12; FP32: 2e-5), bit-repeatably."""
+    params, y0 = meshes.he_beam_problem(nx=6, ny=3, nz=2)
+    cls = _asm_classes()["he"]
+    hd = torch.float32 if precision == "fp32" else torch.float64
+    a = cls(params, precision=precision, hess_dtype=hd, kernel_variant="element")
+    b = cls(params, precision=precision, hess_dtype=hd)
+    assert a.info["kernel_variant"] == 7 and b.info["kernel_variant"] == 2
+    u = torch.as_tensor(y0 + 1e-3 * np.random.default_rng(8).standard_normal(y0.size), device="cuda")
+    ea, ga, ha = [t.clone() for t in a.eval(u, 7)]
+    eb, gb, hb = [t.clone() for t in b.eval(u, 7)]
+    tol = FP64_TOL if precision == "fp64" else FP32_TOL
+    assert abs(float(ea.item()) - float(eb.item())) <= 1e-12 * abs(float(eb.item()))
+    assert _rel(ga.cpu().numpy(), gb.cpu().numpy()) <= tol
+    assert _rel(ha.double().cpu().numpy(), hb.double().cpu().numpy()) <= tol
+    ea2, ga2, ha2 = a.eval(u, 7)
+    assert torch.equal(ha, ha2) and torch.equal(ga, ga2) and torch.equal(ea, ea2)
+    # gradient-only and Hessian-only passes agree with the fused one
+    assert torch.equal(a.eval(u, _lib.FNE_GRAD)[1], ga)
+    assert torch.equal(a.eval(u, _lib.FNE_HESS)[2], ha)
