@@ -328,7 +328,7 @@ WORKLOADS = {
 DEFAULT_WORKLOAD = "gl1024_fp32h"
 
 KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri", 5: "k_mc_elem+k_node_gather",
-                6: "k_mc_tc+k_node_gather", 7: "k_he_elem+k_node_gather"}
+                6: "k_mc_tc+k_node_gather", 7: "k_he_elem+k_node_gather", 8: "k_push_tri"}
 
 
 def algorithmic_bytes(w, asm, n_el):
@@ -528,7 +528,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel-variant", default="auto", choices=["auto", "row_gather", "incidence", "element", "cuda_cores"])
+    ap.add_argument("--kernel-variant", default="auto", choices=["auto", "row_gather", "incidence", "element", "cuda_cores", "push"])
     args = ap.parse_args()
     KERNEL_VARIANT["value"] = args.kernel_variant
     if args.warmup < 3 and args.impl == "b200":

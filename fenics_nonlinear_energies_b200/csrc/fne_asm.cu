@@ -843,6 +843,11 @@ struct SweepArgs {
   int win_mask;
   int rwin_mask;
   int gpos_identity;
+  // push variant: per element the 7-bit column offsets of its 3 x 3 entries
+  // inside the rows of its nodes (21 bits per local node), and the COO row
+  // index of every owned reordered DOF
+  const unsigned long long* __restrict__ eoff;
+  const int* __restrict__ row_of;
 };
 
 // Per-thread prefetch state of one batch: the element it evaluates and the
@@ -1034,6 +1039,144 @@ __global__ void __launch_bounds__(NB, 2) k_sweep_tri(RowArgs A, SweepArgs S, con
 }
 
 // ---------------------------------------------------------------------------
+// Push variant of the banded sweep (P1 triangles, kernel_variant 3): same
+// segments, batches and streamed row windows, but every element thread adds
+// its 3 x 3 Hessian and 3 gradient entries straight into the shared-memory
+// windows with shared-memory atomics (positions = row start + the element's
+// 7-bit column offsets), so no row entries, incidence words or staged
+// element matrices are needed.  Sums of three or more contributions to one
+// entry within a batch are not bit-reproducible from run to run (FP32/FP64
+// rounding order); the pull sweep above is.
+// ---------------------------------------------------------------------------
+template <typename Real>
+struct PushPf {
+  TriElem<Real> t;
+  Real v[3];
+  unsigned long long off;
+  int row[3], pos[3];
+  bool ok;
+};
+
+template <typename Real>
+__device__ __forceinline__ void push_load1(const SweepArgs& S, const Chunk* __restrict__ R, int nrec, int e, bool ok,
+                                           PushPf<Real>& f) {
+  f.ok = ok;
+  if (ok) {
+    load_tri(R, nrec, e, f.t);
+    f.off = __ldg(S.eoff + e);
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ void push_load2(const RowArgs& A, const SweepArgs& S, PushPf<Real>& f) {
+  if (!f.ok) return;
+  const long long n_owned = A.n_rows;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int code = f.t.src[k];
+    f.v[k] = (Real)gather(A.u, A.dir, code, 0);
+    const long long g = (long long)code - A.lo;
+    const int r = (code >= 0 && g >= 0 && g < n_owned) ? __ldg(S.row_of + g) : -1;
+    f.row[k] = r;
+    f.pos[k] = r >= 0 ? __ldg(A.row_ptr + r) : 0;
+  }
+}
+
+template <typename Real, int FAM, int WANT, typename HOut, int NB>
+__global__ void __launch_bounds__(NB, 2) k_push_tri(RowArgs A, SweepArgs S, const Chunk* __restrict__ R, Phys P,
+                                                    double* __restrict__ grad, HOut* __restrict__ hess,
+                                                    EnergyOut eo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* swin = reinterpret_cast<Real*>(smem_raw);  // [win_mask + 1]
+  Real* sgw = swin + (S.win_mask + 1);             // [rwin_mask + 1]
+  const int seg = blockIdx.x;
+  const int R0 = S.seg_row[seg], R1 = S.seg_row[seg + 1];
+  const int p_lo = S.seg_elem[3 * seg], o_lo = S.seg_elem[3 * seg + 1], o_hi = S.seg_elem[3 * seg + 2];
+  const int b0 = S.seg_batch[seg], b1 = S.seg_batch[seg + 1];
+  if (WANT & W_H)
+    for (int j = threadIdx.x; j <= S.win_mask; j += NB) swin[j] = Real(0);
+  if (WANT & W_G)
+    for (int j = threadIdx.x; j <= S.rwin_mask; j += NB) sgw[j] = Real(0);
+  double eacc = 0.0;
+  int done = R0;
+  int p_done = A.row_ptr[R0];
+  PushPf<Real> cur, nxt;
+  int c_bd = R0, c_p1 = p_done;
+  if (b0 < b1) {
+    c_bd = S.batch_done[b0];
+    c_p1 = A.row_ptr[c_bd];
+    const int e = p_lo + threadIdx.x;
+    push_load1(S, R, A.nrec, e, e < o_hi, cur);
+    push_load2(A, S, cur);
+  }
+  __syncthreads();
+  for (int b = b0; b < b1; ++b) {
+    const int e = p_lo + (b - b0) * NB + threadIdx.x;
+    const bool has_next = b + 1 < b1;
+    int n_bd = c_bd, n_p1 = c_p1;
+    if (has_next) n_bd = S.batch_done[b + 1];
+    push_load1(S, R, A.nrec, e + NB, has_next && e + NB < o_hi, nxt);
+    if (cur.ok) {
+      Real g[3], H[6];
+      tri_full<Real, FAM>(P, cur.v, cur.t, g, H);
+      if ((WANT & W_E) && e >= o_lo && cur.t.wflag) eacc += tri_energy_r<Real, FAM>(P, cur.v, cur.t);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int r = cur.row[a];
+        if (r < R0 || r >= R1) continue;
+        if (WANT & W_G) atomicAdd(sgw + (r & S.rwin_mask), g[a]);
+        if (WANT & W_H) {
+          const unsigned bits = (unsigned)(cur.off >> (21 * a)) & 0x1FFFFFu;
+#pragma unroll
+          for (int bb = 0; bb < 3; ++bb) {
+            const unsigned o = (bits >> (kOffBits * bb)) & 127u;
+            if (o != kNoCol) atomicAdd(swin + ((cur.pos[a] + (int)o) & S.win_mask), H[sym_index(a, bb)]);
+          }
+        }
+      }
+    }
+    if (has_next) {
+      push_load2(A, S, nxt);
+      n_p1 = A.row_ptr[n_bd];
+    }
+    __syncthreads();
+    // stream out the rows that are now final
+    if (c_bd > done) {
+      if (WANT & W_H)
+        for (int q = p_done + threadIdx.x; q < c_p1; q += NB) {
+          hess[q] = (HOut)swin[q & S.win_mask];
+          swin[q & S.win_mask] = Real(0);
+        }
+      for (int r = done + threadIdx.x; r < c_bd; r += NB) {
+        const int gp = S.gpos_identity ? r : A.row_gpos[r];
+        if (WANT & W_G) {
+          grad[gp] = (double)sgw[r & S.rwin_mask] - (A.rhs ? A.rhs[gp] : 0.0);
+          sgw[r & S.rwin_mask] = Real(0);
+        }
+        if ((WANT & W_E) && A.rhs) eacc -= A.rhs[gp] * A.u[A.lo + gp];
+      }
+      done = c_bd;
+      p_done = c_p1;
+    }
+    __syncthreads();
+    cur = nxt;
+    c_bd = n_bd;
+    c_p1 = n_p1;
+  }
+  if (done < R1) {
+    const int p1 = A.row_ptr[R1];
+    if (WANT & W_H)
+      for (int q = p_done + threadIdx.x; q < p1; q += NB) hess[q] = (HOut)swin[q & S.win_mask];
+    for (int r = done + threadIdx.x; r < R1; r += NB) {
+      const int gp = S.gpos_identity ? r : A.row_gpos[r];
+      if (WANT & W_G) grad[gp] = (double)sgw[r & S.rwin_mask] - (A.rhs ? A.rhs[gp] : 0.0);
+      if ((WANT & W_E) && A.rhs) eacc -= A.rhs[gp] * A.u[A.lo + gp];
+    }
+  }
+  if (WANT & W_E) energy_finalize(eacc, eo);
+}
+
+// ---------------------------------------------------------------------------
 // energy-only kernels (element-centric, grid-stride)
 // ---------------------------------------------------------------------------
 constexpr int kElemThreads = 256;
@@ -1212,6 +1355,9 @@ struct fne_handle {
   int device = 0, num_sms = 148;
   bool use_inc = false;
   bool use_sweep = false;
+  bool use_push = false;
+  unsigned long long* sw_eoff = nullptr;
+  int* sw_row_of = nullptr;
   int sweep_nb = 0, sweep_win_mask = 0, sweep_rwin_mask = 0;
   int *sw_seg_row = nullptr, *sw_seg_elem = nullptr, *sw_seg_batch = nullptr, *sw_batch_done = nullptr,
       *sw_ent_ptr = nullptr, *sw_inc_base = nullptr, *sw_ent_row = nullptr, *sw_ent_pos = nullptr;
@@ -1278,7 +1424,7 @@ void free_handle(fne_handle* h) {
   void* ptrs[] = {h->rec, h->rec_dir_only, h->row_ptr, h->row_node, h->row_gpos, h->inc_ptr, h->inc_elem,
                   h->row_comp, h->inc_info, h->cta_row, h->cta_inc, h->inc_elem2, h->inc_word, h->inc_rowl,
                   h->sw_seg_row, h->sw_seg_elem, h->sw_seg_batch, h->sw_batch_done, h->sw_ent_ptr, h->sw_inc_base,
-                  h->sw_ent_row, h->sw_ent_pos, h->sw_ent_meta, h->sw_inc_word,
+                  h->sw_ent_row, h->sw_ent_pos, h->sw_ent_meta, h->sw_inc_word, h->sw_eoff, h->sw_row_of,
                   h->dir, h->rhs, h->partials, h->dir_const, h->counter, h->h_u, h->h_grad, h->h_energy,
                   h->h_hess, h->e2_kbuf, h->e2_gbuf, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row,
                   h->bp_rn_gpos, h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk};
@@ -1373,7 +1519,12 @@ cudaError_t launch_tri_t(fne_handle* h, int want, const RowArgs& A, const IncArg
   constexpr int NBS = sizeof(Real) == 4 ? 512 : 256;
 #define FNE_TRI_CASE(W)                                                                                        \
   case W:                                                                                                      \
-    if (h->use_sweep) {                                                                                        \
+    if (h->use_push) {                                                                                         \
+      if (set_attr)                                                                                            \
+        return cudaFuncSetAttribute(k_push_tri<Real, FAM, W, HOut, NBS>,                                      \
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                     \
+      k_push_tri<Real, FAM, W, HOut, NBS><<<grid, NBS, sm, st>>>(A, SW, h->rec, h->phys, grad, H, eo);        \
+    } else if (h->use_sweep) {                                                                                 \
       if (set_attr)                                                                                            \
         return cudaFuncSetAttribute(k_sweep_tri<Real, FAM, W, HOut, NBS>,                                     \
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                     \
@@ -1614,16 +1765,37 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   const int sweep_nb = f32 ? 512 : 256;
   if (is_tri(d->family) && plan.n_rows > 0 && d->kernel_variant == 2)
     use_inc = build_inc_plan(plan, kIncThreads, inc);
-  if (is_tri(d->family) && plan.n_rows > 0 && d->kernel_variant == 0) {
-    // shared memory per CTA: 12*nb element quantities + entry window + row window,
-    // sized so that two CTAs fit on one SM
+  const bool want_push = is_tri(d->family) && d->kernel_variant == 3;
+  if (is_tri(d->family) && plan.n_rows > 0 && (d->kernel_variant == 0 || want_push)) {
+    // shared memory per CTA: 12*nb element quantities (pull sweep only) +
+    // entry window + row window, sized so that two CTAs fit on one SM
     const int64_t budget = std::min<int64_t>(smem_optin, (228 * 1024) / 2 - 1024) / (int64_t)real_size;
-    const int64_t avail = budget - 12 * (int64_t)sweep_nb;
+    const int64_t avail = budget - (want_push ? 0 : 12 * (int64_t)sweep_nb);
     const int n_seg = (int)std::max<int64_t>(
         1, std::min<int64_t>(2 * n_sms, (int64_t)plan.local_elems.size() / (4 * sweep_nb)));
     if (avail > 0)
       use_sweep = build_sweep_plan(plan, sweep_nb, n_seg, (int)(avail * 3 / 4), (int)(avail / 4), sweep);
-    if (use_sweep && 12 * (int64_t)sweep_nb + sweep.win_entries + sweep.win_rows > budget) use_sweep = false;
+    if (use_sweep && (want_push ? 0 : 12 * (int64_t)sweep_nb) + sweep.win_entries + sweep.win_rows > budget)
+      use_sweep = false;
+  }
+  // push variant: per-element column offsets and the row index of every owned DOF
+  std::vector<unsigned long long> eoff;
+  std::vector<int32_t> row_of;
+  const bool use_push = use_sweep && want_push;
+  if (use_push) {
+    eoff.assign(plan.local_elems.size(), ~0ull);
+    for (int32_t k = 0; k < plan.n_rows; ++k) {
+      const int32_t nd = plan.row_node[k];
+      for (int32_t i = plan.inc_ptr[nd]; i < plan.inc_ptr[nd + 1]; ++i) {
+        const uint32_t info = plan.inc_info[i];
+        const int a = (int)(info & 7u);
+        const unsigned long long bits = (info >> kOffShift) & ((1u << (3 * kOffBits)) - 1u);
+        unsigned long long& w = eoff[plan.inc_elem[i]];
+        w = (w & ~(0x1FFFFFull << (21 * a))) | (bits << (21 * a));
+      }
+    }
+    row_of.assign((size_t)(d->hi - d->lo), -1);
+    for (int32_t k = 0; k < plan.n_rows; ++k) row_of[plan.row_gpos[k]] = k;
   }
 
   auto* h = new (std::nothrow) fne_handle();
@@ -1645,6 +1817,7 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   h->max_row_len = plan.max_row_len;
   h->use_inc = use_inc;
   h->use_sweep = use_sweep;
+  h->use_push = use_push;
   h->phys.p = d->s[0];
   h->phys.eps = d->s[0];
   for (int i = 0; i < 9; ++i) h->phys.ip[i] = d->s[1 + i];
@@ -1667,7 +1840,7 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     h->sweep_nb = sweep.nb;
     h->sweep_win_mask = sweep.win_entries - 1;
     h->sweep_rwin_mask = sweep.win_rows - 1;
-    h->smem_bytes = ((size_t)12 * sweep.nb + sweep.win_entries + sweep.win_rows) * real_size;
+    h->smem_bytes = ((size_t)(use_push ? 0 : 12 * sweep.nb) + sweep.win_entries + sweep.win_rows) * real_size;
   } else if (use_inc) {
     h->grid_rows = inc.n_cta;
     h->inc_max_rank = inc.max_rank;
@@ -1728,6 +1901,10 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     h->sw_gpos_identity = sweep.gpos_identity ? 1 : 0;
     FNE_TRY(upload(h, &h->sw_ent_meta, sweep.ent_meta.data(), sweep.ent_meta.size()));
     FNE_TRY(upload(h, &h->sw_inc_word, sweep.inc_word.data(), sweep.inc_word.size()));
+    if (use_push) {
+      FNE_TRY(upload(h, &h->sw_eoff, eoff.data(), eoff.size()));
+      FNE_TRY(upload(h, &h->sw_row_of, row_of.data(), row_of.size()));
+    }
   } else if (use_inc) {
     FNE_TRY(upload(h, &h->cta_row, inc.cta_row.data(), inc.cta_row.size()));
     FNE_TRY(upload(h, &h->cta_inc, inc.cta_inc.data(), inc.cta_inc.size()));
@@ -1812,7 +1989,8 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   info->n_incidences = h->n_inc;
   info->device_bytes = h->device_bytes;
   info->max_row_len = h->max_row_len;
-  info->kernel_variant = is_tri(h->family) ? (h->use_sweep ? 4 : (h->use_inc ? 3 : 1)) : (h->use_elem2 ? 7 : 2);
+  info->kernel_variant = is_tri(h->family) ? (h->use_push ? 8 : (h->use_sweep ? 4 : (h->use_inc ? 3 : 1)))
+                                           : (h->use_elem2 ? 7 : 2);
   if (h->use_elem2) info->n_incidences = h->e2_contrib;
   return FNE_OK;
 }
@@ -1866,7 +2044,7 @@ extern "C" int fne_eval(fne_handle* h, const double* u, int flags, double* energ
     SweepArgs SW{h->sw_seg_row,  h->sw_seg_elem,  h->sw_seg_batch,  h->sw_batch_done,
                  h->sw_ent_ptr,  h->sw_inc_base,  h->sw_ent_row,    h->sw_ent_pos,
                  h->sw_ent_meta, h->sw_inc_word,  h->sweep_win_mask, h->sweep_rwin_mask,
-                 h->sw_gpos_identity};
+                 h->sw_gpos_identity, h->sw_eoff, h->sw_row_of};
     e = h->use_elem2 ? launch_elem2(h, flags, u, grad, hess, eo, st)
                      : launch_rows(h, flags, A, Q, SW, grad, hess, eo, st, false);
   }

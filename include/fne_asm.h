@@ -148,7 +148,9 @@ typedef struct {
                                  * src/problems/ginzburg_landau/jax_petsc/
                                  * reordered_element_assembler.py:34-52, 96-97) */
   int32_t kernel_variant;       /* P1 triangles: 0 = automatic (banded sweep);
-                                 * 1 = row-gather; 2 = incidence-parallel.
+                                 * 1 = row-gather; 2 = incidence-parallel;
+                                 * 3 = banded sweep with shared-memory atomics
+                                 * (push; not bit-reproducible).
                                  * P1 tets: 0/1 = row-gather; 2 = element-
                                  * parallel pass + node-block gather.
                                  * Mohr-Coulomb: 0 = automatic (tensor cores for
@@ -168,7 +170,8 @@ typedef struct {
   int32_t kernel_variant; /* 1 row-gather (triangles), 2 row-gather (tets),
                            * 3 incidence-parallel, 4 banded sweep,
                            * 5 Mohr-Coulomb CUDA cores, 6 Mohr-Coulomb tcgen05,
-                           * 7 element-parallel tets + node-block gather */
+                           * 7 element-parallel tets + node-block gather,
+                           * 8 banded sweep, push variant */
 } fne_info;
 
 int fne_create(const fne_desc* desc, fne_handle** out);

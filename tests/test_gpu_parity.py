@@ -67,7 +67,7 @@ def _abs_energy_scale(ref, u):
     return float(np.abs(e).sum() + np.abs(ref.f_owned @ np.asarray(u)[: ref.f_owned.size]) + 1e-300)
 
 
-@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence"])
+@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence", "push"])
 @pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
 def test_plaplace_fp64(numbering, variant):
     params, _ = meshes.plaplace_problem(n=40, numbering=numbering)
@@ -84,7 +84,7 @@ def test_plaplace_zero_initial_guess():
     assert torch.all(gpu.owned_values == 0)
 
 
-@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence"])
+@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence", "push"])
 @pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
 def test_gl_fp64(numbering, variant):
     params, u0 = meshes.gl_problem(n=16, seed=3, numbering=numbering)
@@ -92,7 +92,7 @@ def test_gl_fp64(numbering, variant):
     _check(gpu, ref, u0, FP64_TOL, energy_scale=_abs_energy_scale(ref, u0))
 
 
-@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence"])
+@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence", "push"])
 def test_gl_fp32(variant):
     params, u0 = meshes.gl_problem(n=40, seed=4)
     gpu, ref = _make("gl", params, precision="fp32", hess_dtype=torch.float32, kernel_variant=variant)
