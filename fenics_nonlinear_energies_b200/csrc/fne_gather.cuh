@@ -29,8 +29,10 @@ struct NodeGatherArgs {
 
 // Element matrices: kbuf[el * NPAIR * BS * BS + pair(a, b) * BS * BS + c * BS + d]
 // = K[(a, c), (b, d)] for a <= b (pair in row-major upper-triangle order);
-// element gradients: gbuf[(el * NPN + a) * BS + c].
-template <typename Real, typename HOut, int BS, int NPN, bool WANT_H, bool WANT_G>
+// element gradients: gbuf[(el * NPN + a) * BS + c].  SLOTS: the contribution
+// codes are slots of a buffer of oriented blocks (kbuf[slot * BS * BS + c * BS
+// + d]), as written by the direct-write epilogue for shared blocks.
+template <typename Real, typename HOut, int BS, int NPN, bool WANT_H, bool WANT_G, bool SLOTS = false>
 __global__ void __launch_bounds__(256) k_node_gather(NodeGatherArgs G, const Real* __restrict__ kbuf,
                                                      const Real* __restrict__ gbuf, HOut* __restrict__ out,
                                                      double* __restrict__ grad) {
@@ -75,12 +77,18 @@ __global__ void __launch_bounds__(256) k_node_gather(NodeGatherArgs G, const Rea
             bool tr[U];
 #pragma unroll
             for (int x = 0; x < U; ++x) {
-              const int el = code[x] / NN;
-              const int r = code[x] - el * NN;
-              const int a = r / NPN, bb = r - a * NPN;
-              tr[x] = a > bb;
-              const int lo = tr[x] ? bb : a, hi = tr[x] ? a : bb;
-              const Real* s = kbuf + (long long)el * KS + (lo * NPN - lo * (lo - 1) / 2 + (hi - lo)) * BS * BS;
+              const Real* s;
+              if (SLOTS) {
+                tr[x] = false;
+                s = kbuf + (long long)code[x] * BS * BS;
+              } else {
+                const int el = code[x] / NN;
+                const int r = code[x] - el * NN;
+                const int a = r / NPN, bb = r - a * NPN;
+                tr[x] = a > bb;
+                const int lo = tr[x] ? bb : a, hi = tr[x] ? a : bb;
+                s = kbuf + (long long)el * KS + (lo * NPN - lo * (lo - 1) / 2 + (hi - lo)) * BS * BS;
+              }
 #pragma unroll
               for (int i = 0; i < BS * BS; ++i) v[x][i] = s[i];
             }
@@ -93,12 +101,18 @@ __global__ void __launch_bounds__(256) k_node_gather(NodeGatherArgs G, const Rea
           }
           for (; j < cnt; ++j) {
             const int code = __ldg(G.con + start + j);
-            const int el = code / NN;
-            const int r = code - el * NN;
-            const int a = r / NPN, bb = r - a * NPN;
-            const bool tr = a > bb;
-            const int lo = tr ? bb : a, hi = tr ? a : bb;
-            const Real* s = kbuf + (long long)el * KS + (lo * NPN - lo * (lo - 1) / 2 + (hi - lo)) * BS * BS;
+            bool tr = false;
+            const Real* s;
+            if (SLOTS) {
+              s = kbuf + (long long)code * BS * BS;
+            } else {
+              const int el = code / NN;
+              const int r = code - el * NN;
+              const int a = r / NPN, bb = r - a * NPN;
+              tr = a > bb;
+              const int lo = tr ? bb : a, hi = tr ? a : bb;
+              s = kbuf + (long long)el * KS + (lo * NPN - lo * (lo - 1) / 2 + (hi - lo)) * BS * BS;
+            }
             Real v[BS * BS];
 #pragma unroll
             for (int i = 0; i < BS * BS; ++i) v[i] = s[i];
@@ -142,6 +156,31 @@ __global__ void __launch_bounds__(256) k_node_gather(NodeGatherArgs G, const Rea
         const int gp = __ldg(G.rn_gpos + A * BS + lane);
         if (gp >= 0) grad[gp] = (double)v - (G.rhs ? G.rhs[gp] : 0.0);
       }
+    }
+  }
+}
+
+// Gradient rows, one thread per row node: the node's element entries summed
+// in element order, minus the load vector.
+template <typename Real, int BS>
+__global__ void __launch_bounds__(256) k_rowgrad(int n_rnodes, const int* __restrict__ rn_inc,
+                                                 const int* __restrict__ inc, const int* __restrict__ rn_gpos,
+                                                 const Real* __restrict__ gbuf, const double* __restrict__ rhs,
+                                                 double* __restrict__ grad) {
+  for (int A = blockIdx.x * blockDim.x + threadIdx.x; A < n_rnodes; A += gridDim.x * blockDim.x) {
+    Real gs[BS];
+#pragma unroll
+    for (int c = 0; c < BS; ++c) gs[c] = Real(0);
+    const int i1 = __ldg(rn_inc + A + 1);
+    for (int i = __ldg(rn_inc + A); i < i1; ++i) {
+      const long long code = __ldg(inc + i);
+#pragma unroll
+      for (int c = 0; c < BS; ++c) gs[c] += gbuf[code * BS + c];
+    }
+#pragma unroll
+    for (int c = 0; c < BS; ++c) {
+      const int gp = __ldg(rn_gpos + A * BS + c);
+      if (gp >= 0) grad[gp] = (double)gs[c] - (rhs ? rhs[gp] : 0.0);
     }
   }
 }

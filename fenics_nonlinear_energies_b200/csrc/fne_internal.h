@@ -124,7 +124,26 @@ struct BlockPlan {
   std::vector<int32_t> rn_blk, rn_con, rn_row, rn_gpos, rn_inc;
   std::vector<uint32_t> blk;
   std::vector<int32_t> con, inc;
+  std::vector<int32_t> elem_rn;  // [n_local * npn] row node of each element node, -1 if none
 };
+
+// Direct-write plan for kernels that hold whole element matrices: for every
+// element and directed node pair (a -> b) a 16-bit code: 0xFFFF = no output
+// (row or column node without an owned free DOF); bit 15 set = the output
+// block (node(a), node(b)) has several contributing elements, bits 0-14 =
+// this element's slot among its shared blocks (the values go to the shared
+// buffer at (sbase[e] + slot) * bs * bs, row-major (c, d)); else bits 0-11 =
+// column offset of node(b) inside the rows of node(a), bits 12-14 = mask of
+// node(b)'s free components (the element writes the block straight into the
+// COO rows).  fix: node-block plan over the shared blocks only, whose
+// contribution codes are shared-buffer slots (element order per block).
+struct DirectPlan {
+  std::vector<uint16_t> code;   // [n_local * npn * npn]
+  std::vector<int32_t> sbase;   // [n_local]
+  int64_t n_slots = 0;
+  BlockPlan fix;
+};
+int build_direct_plan(const BlockPlan& bp, int64_t n_local, int npn, int bs, DirectPlan& D);
 
 // elem_dofs: [n_local * npn * bs] total DOFs (dof = bs * node + component) of
 // the local elements in kernel order.  Returns FNE_OK, or FNE_ELAYOUT /

@@ -439,7 +439,7 @@ struct McTile {
   static constexpr int KK = 4 * NQ;                 // (q, k, l)
   static constexpr int KP = (KK + 7) / 8 * 8;       // padded to the MMA K step (8 tf32)
   static constexpr int M = 128;                     // node pairs (padded)
-  static constexpr int TE = NP > 6 ? 24 : 64;       // elements per tile
+  static constexpr int TE = NP > 6 ? 24 : 48;       // elements per tile
   static constexpr int N = 4 * TE;                  // (c, d, e): row (c * 2 + d) * TE + e
   static constexpr int TMEM_COLS = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
   static constexpr int THREADS = NP > 6 ? 512 : 256;
@@ -452,7 +452,11 @@ struct McTile {
   static constexpr int OFF_R = OFF_S + TE * NQ * 16;                // dh1, dh2 [NQ * NP], qw [NQ]
   static constexpr int OFF_U = OFF_R + ((2 * NQ * NP + NQ) * 4 + 15) / 16 * 16;  // [TE][2 NP]
   static constexpr int OFF_G = OFF_U + (TE * 2 * NP * 4 + 15) / 16 * 16;          // [TE][5]
-  static constexpr int OFF_BAR = OFF_G + (TE * 5 * 4 + 15) / 16 * 16;             // mbarrier, tmem addr, flags
+  static constexpr int OFF_PLAN = OFF_G + (TE * 5 * 4 + 15) / 16 * 16;            // [TE][NP * NP] uint16 codes
+  static constexpr int PLAN_WORDS = (TE * NP * NP + 1) / 2;                       // as uint32 words
+  static constexpr int OFF_ROW = OFF_PLAN + (PLAN_WORDS * 4 + 15) / 16 * 16;      // [TE][NP][2] row starts
+  static constexpr int OFF_SB = OFF_ROW + (TE * NP * 2 * 4 + 15) / 16 * 16;       // [TE] shared-slot bases
+  static constexpr int OFF_BAR = OFF_SB + (TE * 4 + 15) / 16 * 16;                // mbarrier, tmem addr, flags
   static constexpr int SMEM = OFF_BAR + 64;
 };
 
@@ -464,11 +468,19 @@ struct McTcArgs {
   const float* Phi;  // [KP/4][M][4] constant operand, hi part (core-matrix order)
   const float* Plo;  // same, lo part
   int* err;          // device status word (0 = ok; 1 = MMA completion wait timed out)
+  // direct-write epilogue (DirectPlan): per element and directed node pair a
+  // 16-bit code, shared-slot base, row node of every element node, COO start
+  // of every row (row node, component), and the shared-block buffer
+  const uint16_t* code;
+  const int* sbase;
+  const int* elem_rn;
+  const int* rn_row;
+  float* sbuf;
 };
 
-template <int NP, int NQ, int WANT>
+template <int NP, int NQ, int WANT, typename HOut>
 __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_BLOCKS)
-    k_mc_tc(McArgs A, McConstR<float> C, McTcArgs T, float* __restrict__ Kbuf, float* __restrict__ gbuf,
+    k_mc_tc(McArgs A, McConstR<float> C, McTcArgs T, HOut* __restrict__ hout, float* __restrict__ gbuf,
             double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ eout) {
   using G = McTile<NP, NQ>;
   constexpr int N2 = 2 * NP, TE = G::TE, N = G::N, M = G::M, KP = G::KP, NPAIR = G::NPAIR, NT = G::THREADS;
@@ -485,6 +497,10 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
   float* sW = sD2 + NQ * NP;
   float* sU = reinterpret_cast<float*>(smem + G::OFF_U);
   float* sGm = reinterpret_cast<float*>(smem + G::OFF_G);
+  uint32_t* sPlanW = reinterpret_cast<uint32_t*>(smem + G::OFF_PLAN);
+  const uint16_t* sPlan = reinterpret_cast<const uint16_t*>(smem + G::OFF_PLAN);
+  int* sRow = reinterpret_cast<int*>(smem + G::OFF_ROW);
+  int* sSb = reinterpret_cast<int*>(smem + G::OFF_SB);
   unsigned long long* sBar = reinterpret_cast<unsigned long long*>(smem + G::OFF_BAR);
   uint32_t* sTmem = reinterpret_cast<uint32_t*>(smem + G::OFF_BAR + 8);
   int* sFail = reinterpret_cast<int*>(smem + G::OFF_BAR + 12);
@@ -526,7 +542,11 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
   const int n_tiles = (A.n_el + TE - 1) / TE;
 
   // register prefetch of one tile's gather codes, nodal values and geometry
-  int cv[UPT];
+  constexpr int NN = NP * NP;
+  constexpr int RPT = (TE * NP + NT - 1) / NT;              // element nodes per thread (row starts)
+  constexpr int WPT = (G::PLAN_WORDS + NT - 1) / NT;       // plan words per thread
+  int cv[UPT], rnv[RPT], rsv[RPT][2], sbv = 0;
+  uint32_t pw[WPT];
   float uv[UPT], gv[GPT];
   auto fetch_codes = [&](int tile) {
 #pragma unroll
@@ -543,12 +563,36 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
       gv[k] = (tile < n_tiles && i < TE * 5 && e < A.n_el) ? (float)__ldg(A.geom + (long long)tile * TE * 5 + i)
                                                            : 0.f;
     }
+    if (WANT & MW_H) {
+      const int ne_t = tile < n_tiles ? min(TE, A.n_el - tile * TE) : 0;
+      const int nw = (ne_t * NN + 1) / 2;
+      const uint32_t* cw = reinterpret_cast<const uint32_t*>(T.code) + (long long)tile * TE * NN / 2;
+#pragma unroll
+      for (int k = 0; k < WPT; ++k) {
+        const int i = tid + k * NT;
+        pw[k] = i < nw ? __ldg(cw + i) : 0xFFFFFFFFu;
+      }
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int i = tid + k * NT;
+        rnv[k] = i < ne_t * NP ? __ldg(T.elem_rn + (long long)tile * TE * NP + i) : -1;
+      }
+      sbv = tid < ne_t ? __ldg(T.sbase + (long long)tile * TE + tid) : 0;
+    }
   };
   auto fetch_values = [&]() {
 #pragma unroll
     for (int k = 0; k < UPT; ++k) {
       const int c = cv[k];
       uv[k] = c == INT_MIN ? 0.f : (float)(c >= 0 ? __ldg(A.u + c) : __ldg(A.dir + (-1 - c)));
+    }
+    if (WANT & MW_H) {
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int rn = rnv[k];
+        rsv[k][0] = rn >= 0 ? __ldg(T.rn_row + 2LL * rn) : -1;
+        rsv[k][1] = rn >= 0 ? __ldg(T.rn_row + 2LL * rn + 1) : -1;
+      }
     }
   };
   auto stash = [&]() {
@@ -558,6 +602,18 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
 #pragma unroll
     for (int k = 0; k < GPT; ++k)
       if (tid + k * NT < TE * 5) sGm[tid + k * NT] = gv[k];
+    if (WANT & MW_H) {
+#pragma unroll
+      for (int k = 0; k < WPT; ++k)
+        if (tid + k * NT < G::PLAN_WORDS) sPlanW[tid + k * NT] = pw[k];
+#pragma unroll
+      for (int k = 0; k < RPT; ++k)
+        if (tid + k * NT < TE * NP) {
+          sRow[2 * (tid + k * NT)] = rsv[k][0];
+          sRow[2 * (tid + k * NT) + 1] = rsv[k][1];
+        }
+      if (tid < TE) sSb[tid] = sbv;
+    }
   };
 
   double eacc = 0.0;
@@ -691,6 +747,35 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
       constexpr int NGRP = NT / 128, EPG = TE / NGRP;  // element groups, elements per group
       const int quad = warp & 3, grp = warp >> 2;
       const int m = quad * 32 + lane;
+      // node pair of this lane: m -> (pa, pb), pa <= pb
+      int pa = 0, pb = m;
+      while (pa < NP && pb >= NP - pa) {
+        pb -= NP - pa;
+        ++pa;
+      }
+      pb += pa;
+      // one directed block (ra -> cb) of element el: straight into the COO rows,
+      // or into the shared-block buffer
+      auto put = [&](int el, int ra, int cb, float w00, float w01, float w10, float w11) {
+        const unsigned code = sPlan[el * NN + ra * NP + cb];
+        if (code == 0xFFFFu) return;
+        if (code & 0x8000u) {
+          reinterpret_cast<float4*>(T.sbuf)[(long long)sSb[el] + (code & 0x7FFFu)] = make_float4(w00, w01, w10, w11);
+          return;
+        }
+        const int off = (int)(code & 0xFFFu);
+        const unsigned dm = (code >> 12) & 3u;
+        const float w[2][2] = {{w00, w01}, {w10, w11}};
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int rs = sRow[(el * NP + ra) * 2 + c];
+          if (rs < 0) continue;
+          int k = 0;
+#pragma unroll
+          for (int d = 0; d < 2; ++d)
+            if ((dm >> d) & 1u) hout[rs + off + k++] = (HOut)w[c][d];
+        }
+      };
       if (!*sFail && quad * 32 < NPAIR) {
 #pragma unroll 1
         for (int el = grp * EPG; el < (grp + 1) * EPG; el += 2) {
@@ -707,10 +792,12 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
           if (m < NPAIR) {
 #pragma unroll
             for (int x = 0; x < 2; ++x)
-              if (el + x < ne)
-                reinterpret_cast<float4*>(Kbuf + ((long long)(e0 + el + x) * NPAIR + m) * 4)[0] =
-                    make_float4(__uint_as_float(r[0][x]), __uint_as_float(r[1][x]), __uint_as_float(r[2][x]),
-                                __uint_as_float(r[3][x]));
+              if (el + x < ne) {
+                const float v0 = __uint_as_float(r[0][x]), v1 = __uint_as_float(r[1][x]);
+                const float v2 = __uint_as_float(r[2][x]), v3 = __uint_as_float(r[3][x]);
+                put(el + x, pa, pb, v0, v1, v2, v3);                // K[(a,c),(b,d)], (c,d) row-major
+                if (pa != pb) put(el + x, pb, pa, v0, v2, v1, v3);  // transposed block (b, a)
+              }
           }
         }
       }
@@ -784,6 +871,14 @@ struct McHandle {
   int tc = 0, grid_tc = 1;
   float *Phi = nullptr, *Plo = nullptr;
   int* err = nullptr;
+  // direct-write epilogue: per-element codes, shared-block buffer and the
+  // fix-up plan over the shared blocks
+  uint16_t* dp_code = nullptr;
+  int *dp_sbase = nullptr, *dp_elem_rn = nullptr;
+  float* dp_sbuf = nullptr;
+  int n_fix = 0;
+  int *fx_rn_blk = nullptr, *fx_rn_con = nullptr, *fx_rn_row = nullptr, *fx_con = nullptr;
+  unsigned* fx_blk = nullptr;
 };
 
 namespace {
@@ -809,17 +904,28 @@ cudaError_t mc_gathers(McHandle* h, int flags, const Real* K, const Real* g, dou
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (h->use_blk) {
-    if (h->n_rnodes == 0 || !(flags & (MW_G | MW_H))) return cudaSuccess;
-    NodeGatherArgs G{h->n_rnodes, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
-                     h->bp_rn_inc, h->bp_blk, h->bp_con, h->bp_inc, h->rhs};
-    const int grid = std::max(1, std::min(h->num_sms * 16, (h->n_rnodes + 7) / 8));
+    if (h->n_rnodes == 0) return cudaSuccess;
     HOut* H = static_cast<HOut*>(hess);
-    if ((flags & MW_H) && (flags & MW_G))
-      k_node_gather<Real, HOut, 2, NP, true, true><<<grid, 256, 0, st>>>(G, K, g, H, grad);
-    else if (flags & MW_H)
-      k_node_gather<Real, HOut, 2, NP, true, false><<<grid, 256, 0, st>>>(G, K, g, H, grad);
-    else
-      k_node_gather<Real, HOut, 2, NP, false, true><<<grid, 256, 0, st>>>(G, K, g, H, grad);
+    if (flags & MW_H) {
+      if (h->tc) {  // direct-write epilogue: only the shared blocks remain
+        if (h->n_fix > 0) {
+          NodeGatherArgs F{h->n_fix, h->fx_rn_blk, h->fx_rn_con, h->fx_rn_row, nullptr,
+                           nullptr, h->fx_blk, h->fx_con, nullptr, nullptr};
+          const int gf = std::max(1, std::min(h->num_sms * 16, (h->n_fix + 7) / 8));
+          k_node_gather<float, HOut, 2, NP, true, false, true>
+              <<<gf, 256, 0, st>>>(F, h->dp_sbuf, nullptr, H, nullptr);
+        }
+      } else {
+        NodeGatherArgs G{h->n_rnodes, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
+                         h->bp_rn_inc, h->bp_blk, h->bp_con, h->bp_inc, h->rhs};
+        const int grid = std::max(1, std::min(h->num_sms * 16, (h->n_rnodes + 7) / 8));
+        k_node_gather<Real, HOut, 2, NP, true, false><<<grid, 256, 0, st>>>(G, K, g, H, grad);
+      }
+    }
+    if (flags & MW_G) {
+      const int gr = std::max(1, std::min(h->num_sms * 8, (h->n_rnodes + 255) / 256));
+      k_rowgrad<Real, 2><<<gr, 256, 0, st>>>(h->n_rnodes, h->bp_rn_inc, h->bp_inc, h->bp_rn_gpos, g, h->rhs, grad);
+    }
     return cudaGetLastError();
   }
   const int gg = std::max(1, std::min(h->num_sms * 16, (int)((std::max<int64_t>(h->nnz, h->n_rows) + 255) / 256)));
@@ -855,17 +961,17 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
   if constexpr (sizeof(Real) == 4 && NP > 3) {
     if (h->tc && (flags & MW_H)) {
       using G = McTile<NP, NQ>;
-      McTcArgs T{h->Phi, h->Plo, h->err};
-      float* K = static_cast<float*>(h->Kbuf);
+      McTcArgs T{h->Phi, h->Plo, h->err, h->dp_code, h->dp_sbase, h->dp_elem_rn, h->bp_rn_row, h->dp_sbuf};
       float* g = static_cast<float*>(h->gbuf);
+      HOut* H = static_cast<HOut*>(hess);
       const McConstR<float> Mf = cast_const<float>(h->mc);
       switch (flags) {
-        case 4: k_mc_tc<NP, NQ, 4><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
-        case 5: k_mc_tc<NP, NQ, 5><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
-        case 6: k_mc_tc<NP, NQ, 6><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
-        default: k_mc_tc<NP, NQ, 7><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, K, g, h->partials, h->counter, energy); break;
+        case 4: k_mc_tc<NP, NQ, 4, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
+        case 5: k_mc_tc<NP, NQ, 5, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
+        case 6: k_mc_tc<NP, NQ, 6, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
+        default: k_mc_tc<NP, NQ, 7, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
       }
-      return mc_gathers<float, HOut, NP>(h, flags, K, g, grad, hess, st);
+      return mc_gathers<float, HOut, NP>(h, flags, static_cast<const float*>(nullptr), g, grad, hess, st);
     }
   }
   switch (flags) {
@@ -920,13 +1026,18 @@ int mc_tc_prepare(McHandle* h, const double* tables, std::vector<float>& phi, st
             phi[off] = hi;
             plo[off] = v - hi;
           }
-  cudaError_t e = cudaFuncSetAttribute(k_mc_tc<NP, NQ, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_mc_tc<NP, NQ, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_mc_tc<NP, NQ, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_mc_tc<NP, NQ, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+  cudaError_t e = cudaSuccess;
+  auto opt_in = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+  };
+  opt_in((const void*)k_mc_tc<NP, NQ, 4, float>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 5, float>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 6, float>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 7, float>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 4, double>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 5, double>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 6, double>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 7, double>);
   if (e != cudaSuccess)
     return set_error(FNE_ECUDA, std::string("Mohr-Coulomb: tensor-core kernel shared memory: ") +
                                     cudaGetErrorString(e));
@@ -942,7 +1053,8 @@ void mc_destroy(McHandle* h) {
   void* ptrs[] = {h->codes, h->geom, h->epsp, h->dhat1, h->dhat2, h->qw, h->wflag, h->dir, h->rhs,
                   h->partials, h->counter, h->hptr, h->hidx, h->gptr, h->gidx, h->row_gpos, h->Kbuf, h->gbuf,
                   h->Phi, h->Plo, h->err, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
-                  h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk};
+                  h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk, h->dp_code, h->dp_sbase, h->dp_elem_rn,
+                  h->dp_sbuf, h->fx_rn_blk, h->fx_rn_con, h->fx_rn_row, h->fx_con, h->fx_blk};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -1153,18 +1265,33 @@ int mc_create(const fne_desc* d, McHandle** out) {
   MC_TRY(mc_upload(h, &h->gptr, gptr.data(), gptr.size()));
   MC_TRY(mc_upload(h, &h->gidx, gidx.data(), gidx.size()));
   MC_TRY(mc_upload(h, &h->row_gpos, row_gpos.data(), row_gpos.size()));
+  // tensor-core path: FP32 P2 / P4 on a node-blocked pattern unless CUDA
+  // cores are requested; its epilogue writes the COO values directly
+  h->tc = d->precision == FNE_FP32 && np > 3 && d->kernel_variant != 1 && use_blk;
+  DirectPlan dp;
+  if (h->tc && build_direct_plan(bp, nl, np, 2, dp) != FNE_OK) h->tc = 0;
   {
     unsigned char* kb = nullptr;
-    MC_TRY(mc_upload(h, &kb, (const unsigned char*)nullptr, (size_t)nl * npair * 4 * rsz));
+    if (!h->tc) MC_TRY(mc_upload(h, &kb, (const unsigned char*)nullptr, (size_t)nl * npair * 4 * rsz));
     h->Kbuf = kb;
     unsigned char* gb = nullptr;
     MC_TRY(mc_upload(h, &gb, (const unsigned char*)nullptr, (size_t)nl * n * rsz));
     h->gbuf = gb;
   }
   h->n_contrib = use_blk ? (int64_t)bp.con.size() : (int64_t)hptr[d->nnz];
-  // tensor-core path: FP32 P2 / P4 unless CUDA cores are requested
-  h->tc = d->precision == FNE_FP32 && np > 3 && d->kernel_variant != 1;
   if (h->tc) {
+    dp.code.push_back(0xFFFF);  // the kernel reads codes in 32-bit words
+    dp.code.push_back(0xFFFF);
+    MC_TRY(mc_upload(h, &h->dp_code, dp.code.data(), dp.code.size()));
+    MC_TRY(mc_upload(h, &h->dp_sbase, dp.sbase.data(), dp.sbase.size()));
+    MC_TRY(mc_upload(h, &h->dp_elem_rn, bp.elem_rn.data(), bp.elem_rn.size()));
+    MC_TRY(mc_upload(h, &h->dp_sbuf, (const float*)nullptr, (size_t)std::max<int64_t>(1, dp.n_slots) * 4));
+    h->n_fix = dp.fix.n_rnodes;
+    MC_TRY(mc_upload(h, &h->fx_rn_blk, dp.fix.rn_blk.data(), dp.fix.rn_blk.size()));
+    MC_TRY(mc_upload(h, &h->fx_rn_con, dp.fix.rn_con.data(), dp.fix.rn_con.size()));
+    MC_TRY(mc_upload(h, &h->fx_rn_row, dp.fix.rn_row.data(), dp.fix.rn_row.size()));
+    MC_TRY(mc_upload(h, &h->fx_blk, dp.fix.blk.data(), dp.fix.blk.size()));
+    MC_TRY(mc_upload(h, &h->fx_con, dp.fix.con.data(), dp.fix.con.size()));
     std::vector<float> phi, plo;
     int rc_tc = np == 15 ? mc_tc_prepare<15, 25>(h, d->e3, phi, plo) : mc_tc_prepare<6, 7>(h, d->e3, phi, plo);
     if (rc_tc) {

@@ -589,6 +589,7 @@ int build_block_plan(int64_t n_local, int npn, int bs, const int64_t* elem_dofs,
   std::vector<int32_t> cnt(blk_node.size() + 1, 0), fill;
   std::vector<int32_t> icnt(n_rn + 1, 0), ifill;
   std::vector<int32_t> con, inc;
+  P.elem_rn.assign((size_t)n_local * npn, -1);
   for (int pass = 0; pass < 2; ++pass) {
     if (pass == 1) {
       for (size_t b = 0; b < blk_node.size(); ++b) cnt[b + 1] += cnt[b];
@@ -604,6 +605,7 @@ int build_block_plan(int64_t n_local, int npn, int bs, const int64_t* elem_dofs,
         const int64_t na = ed[a * bs] / bs;
         if (na < 0 || na >= n_nodes) return set_error(FNE_EBOUNDS, "block plan: element DOF out of range");
         const int32_t k = rn_of[na];
+        P.elem_rn[(size_t)el * npn + a] = k;
         if (k < 0) continue;
         if (pass == 0) icnt[k + 1]++; else inc[ifill[k]++] = (int32_t)(el * npn + a);
         for (int b = 0; b < npn; ++b) {
@@ -629,6 +631,79 @@ int build_block_plan(int64_t n_local, int npn, int bs, const int64_t* elem_dofs,
   P.con = std::move(con);
   P.rn_inc = std::move(icnt);
   P.inc = std::move(inc);
+  return FNE_OK;
+}
+
+}  // namespace fne
+
+namespace fne {
+
+int build_direct_plan(const BlockPlan& bp, int64_t n_local, int npn, int bs, DirectPlan& D) {
+  const int nn = npn * npn;
+  if (nn > 0x7FFF || bs > 3) return set_error(FNE_EBOUNDS, "direct plan: element too large");
+  D.code.assign((size_t)n_local * nn, 0xFFFF);
+  std::vector<int32_t> n_sh(n_local, 0);
+  // pass 1: direct codes and shared counts
+  for (int32_t k = 0; k < bp.n_rnodes; ++k) {
+    int32_t c0 = bp.rn_con[k];
+    for (int32_t b = bp.rn_blk[k]; b < bp.rn_blk[k + 1]; ++b) {
+      const uint32_t w = bp.blk[b];
+      const int32_t cnt = (int32_t)(w >> 19);
+      const uint32_t off = w & 0xFFFFu, dm = (w >> 16) & 7u;
+      for (int32_t j = c0; j < c0 + cnt; ++j) {
+        const int32_t code = bp.con[j];
+        const int32_t el = code / nn, a = (code % nn) / npn, bb = code % npn;
+        if (cnt == 1) {
+          if (off > 0xFFF) return set_error(FNE_EBOUNDS, "direct plan: row longer than 4095 entries");
+          D.code[(size_t)el * nn + a * npn + bb] = (uint16_t)(off | (dm << 12));
+        } else {
+          n_sh[el]++;
+        }
+      }
+      c0 += cnt;
+    }
+  }
+  D.sbase.assign(n_local, 0);
+  int64_t tot = 0;
+  for (int64_t e = 0; e < n_local; ++e) {
+    D.sbase[e] = (int32_t)tot;
+    tot += n_sh[e];
+    if (n_sh[e] > 0x7FFE) return set_error(FNE_EBOUNDS, "direct plan: too many shared blocks in one element");
+  }
+  if (tot >= (int64_t)INT32_MAX / 16) return set_error(FNE_EBOUNDS, "direct plan: shared buffer beyond 32-bit indexing");
+  D.n_slots = tot;
+  // pass 2: shared slots and the fix-up plan over the shared blocks
+  std::fill(n_sh.begin(), n_sh.end(), 0);
+  BlockPlan& F = D.fix;
+  F = BlockPlan();
+  F.rn_blk.push_back(0);
+  F.rn_con.push_back(0);
+  for (int32_t k = 0; k < bp.n_rnodes; ++k) {
+    int32_t c0 = bp.rn_con[k];
+    bool any = false;
+    for (int32_t b = bp.rn_blk[k]; b < bp.rn_blk[k + 1]; ++b) {
+      const uint32_t w = bp.blk[b];
+      const int32_t cnt = (int32_t)(w >> 19);
+      if (cnt >= 2) {
+        any = true;
+        F.blk.push_back(w);
+        for (int32_t j = c0; j < c0 + cnt; ++j) {
+          const int32_t code = bp.con[j];
+          const int32_t el = code / nn, a = (code % nn) / npn, bb = code % npn;
+          const int32_t slot = n_sh[el]++;
+          D.code[(size_t)el * nn + a * npn + bb] = (uint16_t)(0x8000u | (uint32_t)slot);
+          F.con.push_back(D.sbase[el] + slot);
+        }
+      }
+      c0 += cnt;
+    }
+    if (any) {
+      for (int c = 0; c < bs; ++c) F.rn_row.push_back(bp.rn_row[(size_t)k * bs + c]);
+      F.rn_blk.push_back((int32_t)F.blk.size());
+      F.rn_con.push_back((int32_t)F.con.size());
+    }
+  }
+  F.n_rnodes = (int32_t)F.rn_blk.size() - 1;
   return FNE_OK;
 }
 
