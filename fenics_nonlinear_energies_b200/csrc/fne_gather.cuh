@@ -160,6 +160,37 @@ __global__ void __launch_bounds__(256) k_node_gather(NodeGatherArgs G, const Rea
   }
 }
 
+// Shared-block fix-up for bs = 2 (direct-write epilogue): one thread per
+// shared output block sums its contributions (buffer slots listed in element
+// order) and writes the block's two rows.
+template <typename HOut>
+__global__ void __launch_bounds__(256) k_fixup2(int n_blk, const int4* __restrict__ desc,
+                                                const int* __restrict__ slots, const float4* __restrict__ sbuf,
+                                                HOut* __restrict__ out) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n_blk; b += gridDim.x * blockDim.x) {
+    const int4 ds = __ldg(desc + b);
+    const int cnt = ds.w & 0xFFFF;
+    const unsigned dm = (unsigned)(ds.w >> 16) & 3u;
+    float a00 = 0.f, a01 = 0.f, a10 = 0.f, a11 = 0.f;
+    for (int j = 0; j < cnt; ++j) {
+      const float4 v = __ldg(sbuf + __ldg(slots + ds.z + j));
+      a00 += v.x;
+      a01 += v.y;
+      a10 += v.z;
+      a11 += v.w;
+    }
+    const float r0[2] = {a00, a01}, r1[2] = {a10, a11};
+    int k = 0;
+#pragma unroll
+    for (int d = 0; d < 2; ++d)
+      if ((dm >> d) & 1u) {
+        if (ds.x >= 0) out[ds.x + k] = (HOut)r0[d];
+        if (ds.y >= 0) out[ds.y + k] = (HOut)r1[d];
+        ++k;
+      }
+  }
+}
+
 // Gradient rows, one thread per row node: the node's element entries summed
 // in element order, minus the load vector.
 template <typename Real, int BS>

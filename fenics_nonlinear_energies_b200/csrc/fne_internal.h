@@ -142,6 +142,11 @@ struct DirectPlan {
   std::vector<int32_t> sbase;   // [n_local]
   int64_t n_slots = 0;
   BlockPlan fix;
+  // flat fix-up (bs = 2): per shared block 4 ints: COO position of its first
+  // column in row (A, 0) and in row (A, 1) (-1 if absent), first entry in
+  // fix.con (its contributions' buffer slots, element order), and
+  // count | component mask << 16
+  std::vector<int32_t> fdesc;
 };
 int build_direct_plan(const BlockPlan& bp, int64_t n_local, int npn, int bs, DirectPlan& D);
 

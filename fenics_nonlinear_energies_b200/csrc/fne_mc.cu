@@ -877,8 +877,7 @@ struct McHandle {
   int *dp_sbase = nullptr, *dp_elem_rn = nullptr;
   float* dp_sbuf = nullptr;
   int n_fix = 0;
-  int *fx_rn_blk = nullptr, *fx_rn_con = nullptr, *fx_rn_row = nullptr, *fx_con = nullptr;
-  unsigned* fx_blk = nullptr;
+  int *fx_con = nullptr, *fx_desc = nullptr;
 };
 
 namespace {
@@ -909,11 +908,9 @@ cudaError_t mc_gathers(McHandle* h, int flags, const Real* K, const Real* g, dou
     if (flags & MW_H) {
       if (h->tc) {  // direct-write epilogue: only the shared blocks remain
         if (h->n_fix > 0) {
-          NodeGatherArgs F{h->n_fix, h->fx_rn_blk, h->fx_rn_con, h->fx_rn_row, nullptr,
-                           nullptr, h->fx_blk, h->fx_con, nullptr, nullptr};
-          const int gf = std::max(1, std::min(h->num_sms * 16, (h->n_fix + 7) / 8));
-          k_node_gather<float, HOut, 2, NP, true, false, true>
-              <<<gf, 256, 0, st>>>(F, h->dp_sbuf, nullptr, H, nullptr);
+          const int gf = std::max(1, std::min(h->num_sms * 16, (h->n_fix + 255) / 256));
+          k_fixup2<HOut><<<gf, 256, 0, st>>>(h->n_fix, reinterpret_cast<const int4*>(h->fx_desc), h->fx_con,
+                                             reinterpret_cast<const float4*>(h->dp_sbuf), H);
         }
       } else {
         NodeGatherArgs G{h->n_rnodes, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
@@ -1054,7 +1051,7 @@ void mc_destroy(McHandle* h) {
                   h->partials, h->counter, h->hptr, h->hidx, h->gptr, h->gidx, h->row_gpos, h->Kbuf, h->gbuf,
                   h->Phi, h->Plo, h->err, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
                   h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk, h->dp_code, h->dp_sbase, h->dp_elem_rn,
-                  h->dp_sbuf, h->fx_rn_blk, h->fx_rn_con, h->fx_rn_row, h->fx_con, h->fx_blk};
+                  h->dp_sbuf, h->fx_con, h->fx_desc};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -1286,12 +1283,9 @@ int mc_create(const fne_desc* d, McHandle** out) {
     MC_TRY(mc_upload(h, &h->dp_sbase, dp.sbase.data(), dp.sbase.size()));
     MC_TRY(mc_upload(h, &h->dp_elem_rn, bp.elem_rn.data(), bp.elem_rn.size()));
     MC_TRY(mc_upload(h, &h->dp_sbuf, (const float*)nullptr, (size_t)std::max<int64_t>(1, dp.n_slots) * 4));
-    h->n_fix = dp.fix.n_rnodes;
-    MC_TRY(mc_upload(h, &h->fx_rn_blk, dp.fix.rn_blk.data(), dp.fix.rn_blk.size()));
-    MC_TRY(mc_upload(h, &h->fx_rn_con, dp.fix.rn_con.data(), dp.fix.rn_con.size()));
-    MC_TRY(mc_upload(h, &h->fx_rn_row, dp.fix.rn_row.data(), dp.fix.rn_row.size()));
-    MC_TRY(mc_upload(h, &h->fx_blk, dp.fix.blk.data(), dp.fix.blk.size()));
+    h->n_fix = (int)(dp.fdesc.size() / 4);
     MC_TRY(mc_upload(h, &h->fx_con, dp.fix.con.data(), dp.fix.con.size()));
+    MC_TRY(mc_upload(h, &h->fx_desc, dp.fdesc.data(), dp.fdesc.size()));
     std::vector<float> phi, plo;
     int rc_tc = np == 15 ? mc_tc_prepare<15, 25>(h, d->e3, phi, plo) : mc_tc_prepare<6, 7>(h, d->e3, phi, plo);
     if (rc_tc) {

@@ -704,6 +704,25 @@ int build_direct_plan(const BlockPlan& bp, int64_t n_local, int npn, int bs, Dir
     }
   }
   F.n_rnodes = (int32_t)F.rn_blk.size() - 1;
+  // flat fix-up (bs = 2): one descriptor per shared block; its contributions
+  // are the buffer slots fix.con[start .. start + count)
+  if (bs == 2) {
+    D.fdesc.clear();
+    for (int32_t k = 0; k < F.n_rnodes; ++k) {
+      int32_t c0 = F.rn_con[k];
+      for (int32_t b = F.rn_blk[k]; b < F.rn_blk[k + 1]; ++b) {
+        const uint32_t w = F.blk[b];
+        const int32_t cnt = (int32_t)(w >> 19);
+        const int32_t off = (int32_t)(w & 0xFFFFu);
+        const int32_t r0 = F.rn_row[(size_t)k * 2], r1 = F.rn_row[(size_t)k * 2 + 1];
+        D.fdesc.push_back(r0 >= 0 ? r0 + off : -1);
+        D.fdesc.push_back(r1 >= 0 ? r1 + off : -1);
+        D.fdesc.push_back(c0);
+        D.fdesc.push_back(cnt | (int32_t)(((w >> 16) & 7u) << 16));
+        c0 += cnt;
+      }
+    }
+  }
   return FNE_OK;
 }
 
