@@ -328,7 +328,7 @@ WORKLOADS = {
 DEFAULT_WORKLOAD = "gl1024_fp32h"
 
 KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri", 5: "k_mc_elem+k_node_gather",
-                6: "k_mc_tc+k_node_gather", 7: "k_he_elem+k_node_gather", 8: "k_push_tri"}
+                6: "k_mc_tc+k_fixup2", 7: "k_he_elem+k_node_gather", 8: "k_push_tri"}
 
 
 def algorithmic_bytes(w, asm, n_el):
