@@ -162,7 +162,8 @@ class Workload:
     """
 
     def __init__(self, name, family, precision, hess_fp32, conn_nodes, geom_values, geom_bytes, has_rhs, desc,
-                 build, sample):
+                 build, sample, op="egh"):
+        self.op = op  # "egh": fused E+grad+Hess pass; "hvp": matrix-free H(u) x
         self.name, self.family, self.precision, self.hess_fp32 = name, family, precision, hess_fp32
         self.conn_nodes, self.geom_values, self.geom_bytes, self.has_rhs = conn_nodes, geom_values, geom_bytes, has_rhs
         self.desc, self.build, self.sample = desc, build, sample
@@ -321,6 +322,14 @@ WORKLOADS = {
         "mc_p4_h0.16_fp32", "mc", "fp32", True, 15, 5, 8, True,
         "Mohr-Coulomb slope P4 h=0.16 (about 51,000 elements), FP32 element grad/Hessian (profiling size)",
         *_mc(4, 0.16, "fp32")),
+    "mc_p4_h0.08_hvp_fp64": Workload(
+        "mc_p4_h0.08_hvp_fp64", "mc", "fp64", False, 15, 5, 8, False,
+        "Mohr-Coulomb slope P4 h=0.08 (203,000 elements): one matrix-free Hessian-vector product H(u) x "
+        "at a linearized state (the PMG smoother's operator), FP64", *_mc(4, 0.08, "fp64"), op="hvp"),
+    "mc_p4_h0.08_hvp_fp32": Workload(
+        "mc_p4_h0.08_hvp_fp32", "mc", "fp32", False, 15, 5, 8, False,
+        "Mohr-Coulomb slope P4 h=0.08: one matrix-free Hessian-vector product, FP32 element arithmetic",
+        *_mc(4, 0.08, "fp32"), op="hvp"),
     "mc_p2_h0.08_fp64": Workload(
         "mc_p2_h0.08_fp64", "mc", "fp64", False, 6, 5, 8, True,
         "Mohr-Coulomb slope P2 h=0.08 (203,000 elements), 7-point rule, FP64", *_mc(2, 0.08, "fp64")),
@@ -383,17 +392,41 @@ def run_reference(args):
     torch.set_num_threads(os.cpu_count() or 1)
     w = WORKLOADS[args.workload]
     asm, u, n_el, label, _, _, _ = _oracle_sample(w)
+    if w.op == "hvp":
+        # the reference's "matfree_element" product: element Hessians of the
+        # linearization point (computed once), then sum_e H_e x_e by np.add.at
+        import numpy as np
+
+        from oracle import energies
+
+        v = asm.v_local(u)[asm.local.elems_local_np]
+        _, _, H = energies.element_derivatives(asm.family, v, asm.elem_data, asm.params)
+        x = np.random.default_rng(0).standard_normal(asm.layout.n_free)
+        xf = np.asarray(asm.layout.total_to_free_reord)[asm.local.local_total_nodes]
+        xl = np.zeros(xf.size)
+
+        def step():  # tangent with zero Dirichlet part, element products, scatter
+            xl[:] = 0.0
+            xl[xf >= 0] = x[xf[xf >= 0]]
+            ye = np.einsum("eij,ej->ei", H, xl[asm.local.elems_local_np])
+            out = np.zeros(xl.size)
+            np.add.at(out, asm.local.elems_local_np.ravel(), ye.ravel())
+            return out
+    else:
+        def step():
+            return asm.all_in_one(u)
     for _ in range(args.warmup):
-        asm.all_in_one(u)
+        step()
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
-        asm.all_in_one(u)
+        step()
         times.append(time.perf_counter() - t)
     dt = sum(times) / len(times)
     value = n_el / dt
     line = {
-        "impl": "reference", "metric": "elements/s (E+grad+Hess)", "value": value, "unit": "elements/s",
+        "impl": "reference", "metric": "elements/s (matrix-free H(u) x)" if w.op == "hvp" else
+        "elements/s (E+grad+Hess)", "value": value, "unit": "elements/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w.name, "description": w.desc, "sample": label, "elements_per_step": n_el},
@@ -410,6 +443,94 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # the CUDA path
 # ---------------------------------------------------------------------------
+def run_hvp(args, w, world, rank, local):
+    """One step = one matrix-free H(u) x over every element (linearized once
+    at the workload state outside the timed region)."""
+    import numpy as np
+    import torch
+
+    from fenics_nonlinear_energies_b200 import _lib
+
+    t_setup = time.perf_counter()
+    asm, u0 = w.build(rank)
+    t_setup = time.perf_counter() - t_setup
+    n_el = int(asm.info["n_elem"])
+    dev = torch.device("cuda", local)
+    asm.prepare_matrix_free_operator(torch.as_tensor(u0, device=dev), mode="matfree_element")
+    x = torch.as_tensor(np.random.default_rng(rank).standard_normal(asm.layout.n_free), device=dev)
+    y = torch.empty(max(1, asm.n_owned), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    h = asm._handle
+
+    def step(xv):
+        _lib.check(_lib.lib.fne_hvp(h, xv.data_ptr(), y.data_ptr(), stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        step(x)
+        flush.fill_(1.0)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        _barrier(world)
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            evs[i][0].record(stream)
+            step(x)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        _barrier(world)
+    ms = [a.elapsed_time(b) for a, b in evs]
+    total_s = _max_over_ranks(sum(ms) * 1e-3, world)
+    value = world * n_el * args.steps / total_s
+    # e2e: tangent H2D from pinned memory, product, D2H of the owned result
+    pin_x = x.cpu().pin_memory()
+    host_y = torch.empty(asm.n_owned, dtype=torch.float64).pin_memory()
+    dx = torch.empty_like(x)
+    e2e = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        e2e[i][0].record(stream)
+        dx.copy_(pin_x, non_blocking=True)
+        step(dx)
+        host_y.copy_(y[: asm.n_owned], non_blocking=True)
+        e2e[i][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_s = _max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e) * 1e-3, world)
+    rsz = 4 if w.precision == "fp32" else 8
+    nq = int(asm.params["quad_w"].size)
+    n_dof_e = 2 * int(asm.npe)
+    alg = n_el * (nq * 6 * rsz + 4 * n_dof_e + 8 * w.geom_values) + asm.layout.n_free * 8 + asm.n_owned * 8
+    peak, peak_kind = _peaks()
+    achieved = alg / (sum(ms) / len(ms) * 1e-3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": "elements/s (matrix-free H(u) x)", "value": value, "unit": "elements/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
+            "data": "synthetic (closed-form state, seeded tangent)",
+            "config": {"workload": w.name, "description": w.desc, "elements": n_el, "free_dofs": asm.layout.n_free,
+                       "setup_s": t_setup, "l2": "flushed by a 256 MiB write between products",
+                       "parallelism": f"{world} independent replica(s), one per GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": f"{peak_kind} burst copy (hbm_gbs)", "traffic": None,
+                         "algorithmic_bytes_per_launch": alg, "kernel": "k_mc_hvp+k_rowgrad",
+                         "launches_per_pass": 2},
+            "e2e": {"value": world * n_el * args.steps / e2e_s, "unit": "elements/s",
+                    "h2d_bytes_per_step": int(x.numel() * 8), "d2h_bytes_per_step": int(asm.n_owned * 8)},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def run(args):
     import numpy as np
     import torch
@@ -419,6 +540,8 @@ def run(args):
     from fenics_nonlinear_energies_b200 import _lib
 
     w = WORKLOADS[args.workload]
+    if w.op == "hvp":
+        return run_hvp(args, w, world, rank, local)
     t_setup = time.perf_counter()
     asm, u0 = w.build(rank)
     t_setup = time.perf_counter() - t_setup

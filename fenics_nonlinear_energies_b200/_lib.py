@@ -86,6 +86,9 @@ def _load():
         "fne_eval_host": (C.c_int, [vp, _f64p, C.c_int, _f64p, _f64p, vp]),
         "fne_destroy": (C.c_int, [vp]),
         "fne_check_device_status": (C.c_int, [vp]),
+        "fne_hvp_prepare": (C.c_int, [vp, vp, vp]),
+        "fne_hvp": (C.c_int, [vp, vp, vp, vp]),
+        "fne_hvp_diagonal": (C.c_int, [vp, vp, vp]),
         "fne_energy_p1tri_noalloc": (C.c_int, [C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp, _f64p, vp,
                                                C.c_int64, C.c_int64, vp, vp]),
         "fne_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int64, C.c_int64, vp, C.c_int64, C.c_int64,

@@ -395,6 +395,57 @@ class SlopeStabilityCudaAssembler(CudaElementAssemblerBase):
         return [float(p["E"]), float(p["nu"]), float(p["phi_deg"]), float(p["cohesion"]),
                 float(p.get("reg", 1.0e-12)), 1.0 if self.constitutive_mode == "elastic" else 0.0]
 
+    # ---- matrix-free Hessian products -----------------------------------------
+    # prepare_matrix_free_operator / matrix_free_mult / matrix_free_get_diagonal
+    # (slope_stability/jax_petsc/reordered_element_assembler.py:335-562): the
+    # linearization is kept on the device (weighted tangent per quadrature
+    # point); products never assemble K.  Vectors as in eval: CUDA tensors,
+    # NumPy arrays or objects with ``.array``.
+    _MATFREE_MODES = ("matfree_element", "matfree_overlap")
+
+    def prepare_matrix_free_operator(self, u_owned, *, mode="matfree_element"):
+        """Linearize at ``u`` (full reordered free vector on one rank); returns self."""
+        if str(mode) not in self._MATFREE_MODES:
+            raise ValueError(f"Unsupported matrix-free operator mode {mode!r}")
+        u = self._as_u(u_owned)
+        check(lib.fne_hvp_prepare(self._handle, u.data_ptr(), self._stream()))
+        self._matfree_mode = str(mode)
+        return self
+
+    def _matfree_check(self, mode):
+        if getattr(self, "_matfree_mode", None) != str(mode):
+            raise RuntimeError(f"Matrix-free operator {mode!r} is missing a matching linearization point")
+
+    def matrix_free_mult(self, mode, x, y=None):
+        """``y[owned] = H(u) x``; ``x``'s Dirichlet components are zero by construction."""
+        self._matfree_check(mode)
+        arr = getattr(x, "array", x)
+        xt = torch.as_tensor(np.asarray(arr) if not isinstance(arr, torch.Tensor) else arr)
+        xt = xt.to(device=self.device, dtype=torch.float64).contiguous().reshape(-1)
+        if xt.numel() != self.layout.n_free:
+            raise ValueError(f"tangent has {xt.numel()} entries, expected {self.layout.n_free}")
+        out = torch.empty(max(1, self.n_owned), dtype=torch.float64, device=self.device)
+        check(lib.fne_hvp(self._handle, xt.data_ptr(), out.data_ptr(), self._stream()))
+        return self._deliver(out[: self.n_owned], y)
+
+    def matrix_free_get_diagonal(self, mode, diag=None):
+        """Owned diagonal of H(u)."""
+        self._matfree_check(mode)
+        out = torch.empty(max(1, self.n_owned), dtype=torch.float64, device=self.device)
+        check(lib.fne_hvp_diagonal(self._handle, out.data_ptr(), self._stream()))
+        return self._deliver(out[: self.n_owned], diag)
+
+    @staticmethod
+    def _deliver(t, dest):
+        if dest is None:
+            return t
+        arr = getattr(dest, "array", dest)
+        if isinstance(arr, torch.Tensor):
+            arr.copy_(t)
+        else:
+            arr[:] = t.cpu().numpy()
+        return dest
+
     def _build_rhs_owned(self):
         force = np.asarray(self.params["force"], dtype=np.float64)
         free = np.asarray(self.params["freedofs"], dtype=np.int64)

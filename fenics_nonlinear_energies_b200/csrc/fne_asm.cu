@@ -1995,6 +1995,24 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   return FNE_OK;
 }
 
+extern "C" int fne_hvp_prepare(fne_handle* h, const double* u, void* stream) {
+  if (!h || (!u && h->n_free > 0)) return set_error(FNE_EINVAL, "fne_hvp_prepare: null argument");
+  if (!h->mc) return set_error(FNE_EINVAL, "fne_hvp_prepare: matrix-free products exist for the Mohr-Coulomb family");
+  return mc_hvp_prepare(h->mc, u, stream);
+}
+
+extern "C" int fne_hvp(fne_handle* h, const double* x, double* y, void* stream) {
+  if (!h || (!x && h->n_free > 0) || (!y && h->hi > h->lo)) return set_error(FNE_EINVAL, "fne_hvp: null argument");
+  if (!h->mc) return set_error(FNE_EINVAL, "fne_hvp: matrix-free products exist for the Mohr-Coulomb family");
+  return mc_hvp(h->mc, x, y, stream);
+}
+
+extern "C" int fne_hvp_diagonal(fne_handle* h, double* diag, void* stream) {
+  if (!h || (!diag && h->hi > h->lo)) return set_error(FNE_EINVAL, "fne_hvp_diagonal: null argument");
+  if (!h->mc) return set_error(FNE_EINVAL, "fne_hvp_diagonal: matrix-free products exist for the Mohr-Coulomb family");
+  return mc_hvp_diagonal(h->mc, diag, stream);
+}
+
 extern "C" int fne_check_device_status(fne_handle* h) {
   if (!h) return set_error(FNE_EINVAL, "fne_check_device_status: null handle");
   return h->mc ? mc_check_status(h->mc) : FNE_OK;

@@ -163,6 +163,9 @@ int mc_eval(McHandle* h, const double* u, int flags, double* energy, double* gra
 int mc_set_dirichlet(McHandle* h, const double* dirichlet);
 void mc_info(const McHandle* h, fne_info* info);
 int mc_check_status(McHandle* h);
+int mc_hvp_prepare(McHandle* h, const double* u, void* stream);
+int mc_hvp(McHandle* h, const double* x, double* y, void* stream);
+int mc_hvp_diagonal(McHandle* h, double* diag, void* stream);
 void mc_destroy(McHandle* h);
 
 // Gather code of one element node: >= 0 reordered id of component 0 (free

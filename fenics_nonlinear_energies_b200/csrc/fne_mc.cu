@@ -325,6 +325,130 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_elem(McArgs A, McConstR<Re
 }
 
 // ---------------------------------------------------------------------------
+// Matrix-free Hessian products (the reference's matrix_free_mult /
+// matrix_free_get_diagonal, slope_stability/jax_petsc/
+// reordered_element_assembler.py:335-562).  k_mc_lin stores, at the
+// linearization point u, the weighted consistent tangent w_q C_q (upper
+// triangle, 6 values) of every quadrature point; k_mc_hvp then evaluates per
+// element y_e = sum_q B_q^T (w_q C_q) (B_q x_e) -- or, for the diagonal,
+// d_(a,c) = sum_q B_q[:,(a,c)]^T (w_q C_q) B_q[:,(a,c)] -- without forming
+// K_e; the element vectors are summed per owned row by k_rowgrad.  One warp
+// per element, one lane per quadrature point, then one lane per element DOF.
+// ---------------------------------------------------------------------------
+template <typename Real, int NP, int NQ>
+__global__ void __launch_bounds__(32 * kMcWarps) k_mc_lin(McArgs A, McConstR<Real> M, Real* __restrict__ wct) {
+  constexpr int N = 2 * NP;
+  __shared__ Real s_dh1[NQ * NP], s_dh2[NQ * NP], s_w[NQ];
+  __shared__ Real s_u[kMcWarps][N];
+  for (int i = threadIdx.x; i < NQ * NP; i += blockDim.x) {
+    s_dh1[i] = (Real)A.dhat1[i];
+    s_dh2[i] = (Real)A.dhat2[i];
+  }
+  for (int i = threadIdx.x; i < NQ; i += blockDim.x) s_w[i] = (Real)A.qw[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Real* ue = s_u[wid];
+  for (int e = blockIdx.x * kMcWarps + wid; e < A.n_el; e += gridDim.x * kMcWarps) {
+    const double* gm = A.geom + 5LL * e;
+    const Real i00 = (Real)gm[0], i01 = (Real)gm[1], i10 = (Real)gm[2], i11 = (Real)gm[3], dj = (Real)gm[4];
+    for (int i = lane; i < N; i += 32) {
+      const int code = A.codes[(long long)e * N + i];
+      ue[i] = (Real)(code >= 0 ? A.u[code] : A.dir[-1 - code]);
+    }
+    __syncwarp();
+    if (lane < NQ) {
+      const int q = lane;
+      Real ex = Real(0), ey = Real(0), exy = Real(0);
+      for (int a = 0; a < NP; ++a) {
+        const Real r1 = s_dh1[q * NP + a], r2 = s_dh2[q * NP + a];
+        const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
+        ex += px * ue[2 * a];
+        ey += py * ue[2 * a + 1];
+        exy += py * ue[2 * a] + px * ue[2 * a + 1];
+      }
+      Real eps[3] = {ex, ey, exy};
+      if (A.epsp) {
+        const double* ep = A.epsp + ((long long)e * NQ + q) * 3;
+        eps[0] -= (Real)ep[0];
+        eps[1] -= (Real)ep[1];
+        eps[2] -= (Real)ep[2];
+      }
+      Real sig[3], Ct[6], psi;
+      mc_point(M, eps, sig, Ct, psi);
+      const Real w = dj * s_w[q];
+      Real* o = wct + ((long long)e * NQ + q) * 6;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) o[k] = w * Ct[k];
+    }
+    __syncwarp();
+  }
+}
+
+template <typename Real, int NP, int NQ, bool DIAG>
+__global__ void __launch_bounds__(32 * kMcWarps) k_mc_hvp(McArgs A, const Real* __restrict__ wct,
+                                                          Real* __restrict__ ebuf) {
+  constexpr int N = 2 * NP;
+  __shared__ Real s_dh1[NQ * NP], s_dh2[NQ * NP];
+  __shared__ Real s_x[kMcWarps][N];
+  __shared__ Real s_s[kMcWarps][NQ * 3];
+  for (int i = threadIdx.x; i < NQ * NP; i += blockDim.x) {
+    s_dh1[i] = (Real)A.dhat1[i];
+    s_dh2[i] = (Real)A.dhat2[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Real* xe = s_x[wid];
+  Real* ss = s_s[wid];
+  for (int e = blockIdx.x * kMcWarps + wid; e < A.n_el; e += gridDim.x * kMcWarps) {
+    const double* gm = A.geom + 5LL * e;
+    const Real i00 = (Real)gm[0], i01 = (Real)gm[1], i10 = (Real)gm[2], i11 = (Real)gm[3];
+    const Real* wc = wct + (long long)e * NQ * 6;
+    if (!DIAG) {
+      // tangent direction: free DOFs from x, Dirichlet DOFs zero
+      for (int i = lane; i < N; i += 32) {
+        const int code = A.codes[(long long)e * N + i];
+        xe[i] = code >= 0 ? (Real)A.u[code] : Real(0);
+      }
+      __syncwarp();
+      if (lane < NQ) {  // s_q = (w C_q) (B_q x_e)
+        const int q = lane;
+        Real ex = Real(0), ey = Real(0), exy = Real(0);
+        for (int a = 0; a < NP; ++a) {
+          const Real r1 = s_dh1[q * NP + a], r2 = s_dh2[q * NP + a];
+          const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
+          ex += px * xe[2 * a];
+          ey += py * xe[2 * a + 1];
+          exy += py * xe[2 * a] + px * xe[2 * a + 1];
+        }
+        const Real* C = wc + q * 6;
+        ss[q * 3 + 0] = C[0] * ex + C[1] * ey + C[2] * exy;
+        ss[q * 3 + 1] = C[1] * ex + C[3] * ey + C[4] * exy;
+        ss[q * 3 + 2] = C[2] * ex + C[4] * ey + C[5] * exy;
+      }
+      __syncwarp();
+    }
+    for (int i = lane; i < N; i += 32) {
+      const int a = i >> 1, c = i & 1;
+      Real acc = Real(0);
+      for (int q = 0; q < NQ; ++q) {
+        const Real r1 = s_dh1[q * NP + a], r2 = s_dh2[q * NP + a];
+        const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
+        if (DIAG) {
+          // B column (a, c): c = 0 -> (px, 0, py); c = 1 -> (0, py, px)
+          const Real* C = wc + q * 6;
+          acc += c == 0 ? px * (C[0] * px + C[2] * py) + py * (C[2] * px + C[5] * py)
+                        : py * (C[3] * py + C[4] * px) + px * (C[4] * py + C[5] * px);
+        } else {
+          acc += c == 0 ? px * ss[q * 3] + py * ss[q * 3 + 2] : py * ss[q * 3 + 1] + px * ss[q * 3 + 2];
+        }
+      }
+      ebuf[(long long)e * N + i] = acc;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Tensor-core element kernel (FP32, P2 / P4): tcgen05.mma, kind::tf32.
 //
 // For affine triangles the physical basis gradients are g_ai = sum_k J^-1_ik
@@ -878,6 +1002,10 @@ struct McHandle {
   float* dp_sbuf = nullptr;
   int n_fix = 0;
   int *fx_con = nullptr, *fx_desc = nullptr;
+  // matrix-free products: weighted tangents at the linearization point and
+  // the element vectors (allocated by the first fne_hvp_prepare)
+  void *lin_wct = nullptr, *lin_ebuf = nullptr;
+  int lin_ready = 0;
 };
 
 namespace {
@@ -1051,7 +1179,7 @@ void mc_destroy(McHandle* h) {
                   h->partials, h->counter, h->hptr, h->hidx, h->gptr, h->gidx, h->row_gpos, h->Kbuf, h->gbuf,
                   h->Phi, h->Plo, h->err, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
                   h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk, h->dp_code, h->dp_sbase, h->dp_elem_rn,
-                  h->dp_sbuf, h->fx_con, h->fx_desc};
+                  h->dp_sbuf, h->fx_con, h->fx_desc, h->lin_wct, h->lin_ebuf};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete h;
@@ -1324,6 +1452,86 @@ int mc_set_dirichlet(McHandle* h, const double* dirichlet) {
   if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("fne_set_dirichlet: ") + cudaGetErrorString(e));
   return FNE_OK;
 }
+
+namespace {
+
+template <typename Real, int NP, int NQ>
+cudaError_t mc_lin_launch(McHandle* h, int op, const double* v, double* out, cudaStream_t st) {
+  McArgs A{};
+  A.n_el = h->n_local;
+  A.codes = h->codes;
+  A.geom = h->geom;
+  A.epsp = h->epsp;
+  A.wflag = h->wflag;
+  A.dhat1 = h->dhat1;
+  A.dhat2 = h->dhat2;
+  A.qw = h->qw;
+  A.u = v;
+  A.dir = h->dir;
+  A.rhs = nullptr;
+  A.n_owned = (int)(h->hi - h->lo);
+  A.lo = h->lo;
+  Real* wct = static_cast<Real*>(h->lin_wct);
+  Real* eb = static_cast<Real*>(h->lin_ebuf);
+  const int grid = h->grid_elem, T = 32 * kMcWarps;
+  if (op == 0) {
+    k_mc_lin<Real, NP, NQ><<<grid, T, 0, st>>>(A, cast_const<Real>(h->mc), wct);
+    return cudaGetLastError();
+  }
+  if (op == 1)
+    k_mc_hvp<Real, NP, NQ, false><<<grid, T, 0, st>>>(A, wct, eb);
+  else
+    k_mc_hvp<Real, NP, NQ, true><<<grid, T, 0, st>>>(A, wct, eb);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (h->use_blk) {
+    if (h->n_rnodes == 0) return cudaSuccess;
+    const int gr = std::max(1, std::min(h->num_sms * 8, (h->n_rnodes + 255) / 256));
+    k_rowgrad<Real, 2><<<gr, 256, 0, st>>>(h->n_rnodes, h->bp_rn_inc, h->bp_inc, h->bp_rn_gpos, eb, nullptr, out);
+  } else if (h->n_rows > 0) {
+    const int gg = std::max(1, std::min(h->num_sms * 16, (h->n_rows + 255) / 256));
+    k_mc_grad_gather<Real><<<gg, 256, 0, st>>>(h->n_rows, h->gptr, h->gidx, eb, h->row_gpos, nullptr, out);
+  }
+  return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t mc_lin_dispatch(McHandle* h, int op, const double* v, double* out, cudaStream_t st) {
+  if (h->np == 3 && h->nq == 1) return mc_lin_launch<Real, 3, 1>(h, op, v, out, st);
+  if (h->np == 6 && h->nq == 7) return mc_lin_launch<Real, 6, 7>(h, op, v, out, st);
+  if (h->np == 15 && h->nq == 25) return mc_lin_launch<Real, 15, 25>(h, op, v, out, st);
+  return cudaErrorInvalidValue;
+}
+
+int mc_lin(McHandle* h, int op, const double* v, double* out, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (op == 0 && !h->lin_wct) {
+    const size_t rsz = h->precision == FNE_FP32 ? sizeof(float) : sizeof(double);
+    unsigned char *w = nullptr, *eb = nullptr;
+    int rc = mc_upload(h, &w, (const unsigned char*)nullptr, std::max<size_t>(1, (size_t)h->n_local * h->nq * 6 * rsz));
+    if (!rc) rc = mc_upload(h, &eb, (const unsigned char*)nullptr, std::max<size_t>(1, (size_t)h->n_local * h->n * rsz));
+    if (rc) {
+      if (w) cudaFree(w);
+      if (eb) cudaFree(eb);
+      return rc;
+    }
+    h->lin_wct = w;
+    h->lin_ebuf = eb;
+  }
+  if (op != 0 && !h->lin_ready)
+    return set_error(FNE_EINVAL, "matrix-free product: call fne_hvp_prepare first (no linearization point)");
+  const cudaError_t e = h->precision == FNE_FP32 ? mc_lin_dispatch<float>(h, op, v, out, st)
+                                                  : mc_lin_dispatch<double>(h, op, v, out, st);
+  if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("matrix-free product launch: ") + cudaGetErrorString(e));
+  if (op == 0) h->lin_ready = 1;
+  return FNE_OK;
+}
+
+}  // namespace
+
+int mc_hvp_prepare(McHandle* h, const double* u, void* stream) { return mc_lin(h, 0, u, nullptr, stream); }
+int mc_hvp(McHandle* h, const double* x, double* y, void* stream) { return mc_lin(h, 1, x, y, stream); }
+int mc_hvp_diagonal(McHandle* h, double* diag, void* stream) { return mc_lin(h, 2, nullptr, diag, stream); }
 
 int mc_check_status(McHandle* h) {
   if (!h->err) return FNE_OK;

@@ -177,6 +177,22 @@ typedef struct {
 int fne_create(const fne_desc* desc, fne_handle** out);
 int fne_info_get(const fne_handle* h, fne_info* info);
 /*
+ * Matrix-free Hessian products (Mohr-Coulomb handles), replacing the
+ * reference's prepare_matrix_free_operator / matrix_free_mult /
+ * matrix_free_get_diagonal (src/problems/slope_stability/jax_petsc/
+ * reordered_element_assembler.py:335-562, mode "matfree_element").
+ *   fne_hvp_prepare: linearize at u (device, [n_free] full reordered free
+ *     vector): stores the weighted consistent tangent of every quadrature
+ *     point (n_elem * nq * 6 values; allocated on the first call).
+ *   fne_hvp: y[owned] = H(u) x, x a device [n_free] tangent (its Dirichlet
+ *     components are zero by construction), y device [hi - lo].
+ *   fne_hvp_diagonal: diag[owned] = the diagonal of H(u).
+ * Stream-ordered; FNE_EINVAL for other families or before a prepare.
+ */
+int fne_hvp_prepare(fne_handle* h, const double* u, void* stream);
+int fne_hvp(fne_handle* h, const double* x, double* y, void* stream);
+int fne_hvp_diagonal(fne_handle* h, double* diag, void* stream);
+/*
  * Synchronous read of the handle's device status word (kernels that wait on
  * the tensor core record a bounded wait that gave up there instead of
  * hanging).  FNE_OK, or FNE_ETIMEOUT (the word is then cleared).  No

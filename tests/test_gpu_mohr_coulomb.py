@@ -149,3 +149,52 @@ def test_mc_tensor_core_hessian_only_and_plastic_mix():
     h = gpu.eval(torch.as_tensor(u, device="cuda"), _lib.FNE_HESS)[2]
     gpu.check_device_status()
     assert _rel(h.double().cpu().numpy(), h_ref) <= 2e-5
+
+
+@pytest.mark.parametrize("degree", [2, 4])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_matrix_free_products(degree, precision):
+    """Matrix-free H(u) x and diag H(u) against the assembled owned COO values
+    (FP64: 1e-12; FP32: 2e-5 relative to the largest entry), at a state with
+    plastic points, and against central differences of the oracle gradient."""
+    from scipy import sparse
+
+    params = meshes.slope_problem(level=2, degree=degree, lam=1.2, with_elem_B=True)
+    hd = torch.float32 if precision == "fp32" else torch.float64
+    gpu, ref = _pair(params, precision=precision, hess_dtype=hd)
+    u = 0.05 * np.random.default_rng(21).standard_normal(gpu.layout.n_free)
+    ut = torch.as_tensor(u, device="cuda")
+    h = gpu.eval(ut, _lib.FNE_HESS)[2].double().cpu().numpy()
+    A = sparse.coo_matrix((h, (gpu.layout.owned_rows, gpu.layout.owned_cols)),
+                          shape=(gpu.layout.n_free,) * 2).tocsr()
+    gpu.prepare_matrix_free_operator(ut, mode="matfree_element")
+    tol = 1e-12 if precision == "fp64" else 2e-5
+    for seed in (0, 1):
+        x = np.random.default_rng(seed).standard_normal(gpu.layout.n_free)
+        y = gpu.matrix_free_mult("matfree_element", torch.as_tensor(x, device="cuda")).cpu().numpy()
+        y_ref = A @ x
+        assert np.abs(y - y_ref).max() <= tol * np.abs(y_ref).max()
+    d = gpu.matrix_free_get_diagonal("matfree_element").cpu().numpy()
+    assert np.abs(d - A.diagonal()).max() <= tol * np.abs(A.diagonal()).max()
+    # repeat calls are bit-identical (fixed summation order)
+    y2 = gpu.matrix_free_mult("matfree_element", torch.as_tensor(x, device="cuda")).cpu().numpy()
+    assert np.array_equal(y, y2)
+    if precision == "fp64":
+        hstep = 1e-6
+        fd = (ref.gradient_fn(u + hstep * x) - ref.gradient_fn(u - hstep * x)) / (2 * hstep)
+        assert np.abs(y - fd).max() <= 1e-4 * np.abs(fd).max()
+
+
+def test_matrix_free_requires_prepare():
+    from fenics_nonlinear_energies_b200._lib import FneError
+
+    params = meshes.slope_problem(level=1, degree=2, lam=1.0)
+    from fenics_nonlinear_energies_b200.assembler import SlopeStabilityCudaAssembler
+
+    gpu = SlopeStabilityCudaAssembler(params)
+    x = torch.zeros(gpu.layout.n_free, dtype=torch.float64, device="cuda")
+    with pytest.raises(RuntimeError):
+        gpu.matrix_free_mult("matfree_element", x)
+    out = torch.empty(max(1, gpu.n_owned), dtype=torch.float64, device="cuda")
+    with pytest.raises(FneError):
+        _lib.check(_lib.lib.fne_hvp(gpu._handle, x.data_ptr(), out.data_ptr(), None))
