@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_hvp(McArgs A, const Real* 
   constexpr int N = 2 * NP;
   __shared__ Real s_dh1[NQ * NP], s_dh2[NQ * NP];
   __shared__ Real s_x[kMcWarps][N];
-  __shared__ Real s_s[kMcWarps][NQ * 3];
+  __shared__ Real s_s[kMcWarps][NQ * 4];
   for (int i = threadIdx.x; i < NQ * NP; i += blockDim.x) {
     s_dh1[i] = (Real)A.dhat1[i];
     s_dh2[i] = (Real)A.dhat2[i];
@@ -410,20 +410,30 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_hvp(McArgs A, const Real* 
         xe[i] = code >= 0 ? (Real)A.u[code] : Real(0);
       }
       __syncwarp();
-      if (lane < NQ) {  // s_q = (w C_q) (B_q x_e)
+      if (lane < NQ) {
+        // reference-gradient contraction z[d][l] = sum_b R_qbl x_(b,d); strain
+        // B_q x_e = J^-T-weighted z; s = (w C_q) strain; pulled back
+        // t[c][l] = sum_i J^-1_il s[v(c,i)], so that y_(a,c) = sum_q sum_l R_qal t[c][l]
         const int q = lane;
-        Real ex = Real(0), ey = Real(0), exy = Real(0);
+        Real z01 = Real(0), z02 = Real(0), z11 = Real(0), z12 = Real(0);
         for (int a = 0; a < NP; ++a) {
           const Real r1 = s_dh1[q * NP + a], r2 = s_dh2[q * NP + a];
-          const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
-          ex += px * xe[2 * a];
-          ey += py * xe[2 * a + 1];
-          exy += py * xe[2 * a] + px * xe[2 * a + 1];
+          const Real x0 = xe[2 * a], x1 = xe[2 * a + 1];
+          z01 += r1 * x0;
+          z02 += r2 * x0;
+          z11 += r1 * x1;
+          z12 += r2 * x1;
         }
+        const Real ex = i00 * z01 + i01 * z02, ey = i10 * z11 + i11 * z12;
+        const Real exy = i10 * z01 + i11 * z02 + i00 * z11 + i01 * z12;
         const Real* C = wc + q * 6;
-        ss[q * 3 + 0] = C[0] * ex + C[1] * ey + C[2] * exy;
-        ss[q * 3 + 1] = C[1] * ex + C[3] * ey + C[4] * exy;
-        ss[q * 3 + 2] = C[2] * ex + C[4] * ey + C[5] * exy;
+        const Real s0 = C[0] * ex + C[1] * ey + C[2] * exy;
+        const Real s1 = C[1] * ex + C[3] * ey + C[4] * exy;
+        const Real s2 = C[2] * ex + C[4] * ey + C[5] * exy;
+        ss[q * 4 + 0] = i00 * s0 + i10 * s2;  // c = 0, l = 1
+        ss[q * 4 + 1] = i01 * s0 + i11 * s2;  // c = 0, l = 2
+        ss[q * 4 + 2] = i10 * s1 + i00 * s2;  // c = 1, l = 1
+        ss[q * 4 + 3] = i11 * s1 + i01 * s2;  // c = 1, l = 2
       }
       __syncwarp();
     }
@@ -432,14 +442,14 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_hvp(McArgs A, const Real* 
       Real acc = Real(0);
       for (int q = 0; q < NQ; ++q) {
         const Real r1 = s_dh1[q * NP + a], r2 = s_dh2[q * NP + a];
-        const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
         if (DIAG) {
           // B column (a, c): c = 0 -> (px, 0, py); c = 1 -> (0, py, px)
+          const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
           const Real* C = wc + q * 6;
           acc += c == 0 ? px * (C[0] * px + C[2] * py) + py * (C[2] * px + C[5] * py)
                         : py * (C[3] * py + C[4] * px) + px * (C[4] * py + C[5] * px);
         } else {
-          acc += c == 0 ? px * ss[q * 3] + py * ss[q * 3 + 2] : py * ss[q * 3 + 1] + px * ss[q * 3 + 2];
+          acc += r1 * ss[q * 4 + 2 * c] + r2 * ss[q * 4 + 2 * c + 1];
         }
       }
       ebuf[(long long)e * N + i] = acc;
