@@ -52,7 +52,8 @@ class OracleAssembler:
         self.elem_data = {k: np.asarray(params[k], dtype=np.float64)[self.local.local_elem_idx]
                           for k in FAMILY_KEYS[family]}
         self.f_owned = self._rhs_owned()
-        self.dirichlet_only_energy = self._dirichlet_only_energy() if family == "gl" else 0.0
+        # rank 0 only (ginzburg_landau/jax_petsc/reordered_element_assembler.py:34-36)
+        self.dirichlet_only_energy = self._dirichlet_only_energy() if (family == "gl" and rank == 0) else 0.0
 
     # -- reference helpers -------------------------------------------------
     def _rhs_owned(self):
