@@ -232,3 +232,57 @@ def test_he_element_pass_matches_row_gather(precision):
     # gradient-only and Hessian-only passes agree with the fused one
     assert torch.equal(a.eval(u, _lib.FNE_GRAD)[1], ga)
     assert torch.equal(a.eval(u, _lib.FNE_HESS)[2], ha)
+
+
+@pytest.mark.parametrize("family", ["plaplace", "gl", "he", "mc"])
+@pytest.mark.parametrize("size", [2, 3])
+def test_rank_split_matches_oracle(family, size):
+    """Each rank of a size-way split (owned rows [lo, hi), overlap elements,
+    0/1 energy weights, rank-0-only constants) against the oracle of the same
+    rank: FP64 within 1e-12; the rank energies sum to the one-rank energy."""
+    from types import SimpleNamespace
+
+    from fenics_nonlinear_energies_b200.assembler import SlopeStabilityCudaAssembler
+
+    if family == "mc":
+        params = meshes.slope_problem(level=2, degree=2, lam=1.2, with_elem_B=True)
+        u = 0.05 * np.random.default_rng(31).standard_normal(int(np.asarray(params["freedofs"]).size))
+        make_gpu = lambda comm: SlopeStabilityCudaAssembler(params, comm)  # noqa: E731
+        okw = dict(block_size=2)
+    else:
+        if family == "plaplace":
+            params, _ = meshes.plaplace_problem(n=20)
+        elif family == "gl":
+            params, _ = meshes.gl_problem(n=20, seed=5)
+        else:
+            params, _ = meshes.he_beam_problem(nx=8, ny=2, nz=2)
+        cls = _asm_classes()[family]
+        make_gpu = lambda comm: cls(params, comm)  # noqa: E731
+        okw = dict(block_size=3, coordinate_key="nodes2coord", dirichlet_key="u_0_ref") if family == "he" else {}
+        n_free = int(np.asarray(params["freedofs"]).size)
+        rng = np.random.default_rng(32)
+        if family == "he":
+            y0 = np.asarray(params["u_0_ref"])[params["freedofs"]]
+            u = y0 + 1e-3 * rng.standard_normal(n_free)
+        else:
+            u = rng.uniform(-0.5, 0.5, n_free)
+    fam = "mc" if family == "mc" else family
+    total = 0.0
+    for r in range(size):
+        gpu = make_gpu(SimpleNamespace(rank=r, size=size))
+        ref = OracleAssembler(fam, params, rank=r, size=size, **okw)
+        ur = u[np.asarray(gpu.layout.perm)] if family != "he" else u
+        np.testing.assert_array_equal(gpu.layout.owned_rows, ref.layout.owned_rows)
+        e_ref, g_ref, h_ref = ref.all_in_one(ur)
+        e, g, h = gpu.eval(torch.as_tensor(ur, device="cuda"), 7)
+        scale = max(1.0, abs(e_ref))
+        assert abs(float(e.item()) - e_ref) <= 1e-12 * scale * 10
+        if g_ref.size:
+            assert _rel(g.cpu().numpy()[: gpu.n_owned], g_ref) <= FP64_TOL
+        if h_ref.size:
+            assert _rel(h.cpu().numpy(), h_ref) <= FP64_TOL
+        total += float(e.item())
+    one = OracleAssembler(fam, params, **okw)
+    u1 = u[np.asarray(one.layout.perm)] if family != "he" else u
+    e1 = one.all_in_one(u1)[0]
+    assert abs(total - e1) <= 1e-11 * max(1.0, abs(e1))
