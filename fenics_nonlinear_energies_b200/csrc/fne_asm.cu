@@ -1771,8 +1771,10 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     // entry window + row window, sized so that two CTAs fit on one SM
     const int64_t budget = std::min<int64_t>(smem_optin, (228 * 1024) / 2 - 1024) / (int64_t)real_size;
     const int64_t avail = budget - (want_push ? 0 : 12 * (int64_t)sweep_nb);
+    // two CTAs per SM when the mesh allows; small meshes get one batch per
+    // segment (more re-evaluated boundary strips, but every SM busy)
     const int n_seg = (int)std::max<int64_t>(
-        1, std::min<int64_t>(2 * n_sms, (int64_t)plan.local_elems.size() / (4 * sweep_nb)));
+        1, std::min<int64_t>(2 * n_sms, (int64_t)plan.local_elems.size() / sweep_nb));
     if (avail > 0)
       use_sweep = build_sweep_plan(plan, sweep_nb, n_seg, (int)(avail * 3 / 4), (int)(avail / 4), sweep);
     if (use_sweep && (want_push ? 0 : 12 * (int64_t)sweep_nb) + sweep.win_entries + sweep.win_rows > budget)
