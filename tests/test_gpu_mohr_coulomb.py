@@ -13,6 +13,9 @@ from fenics_nonlinear_energies_b200 import _lib, meshes
 
 pytestmark = pytest.mark.gpu
 
+FP64_TOL = 1e-12
+FP32_TOL = 2e-5
+
 
 def _rel(a, b):
     a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
@@ -198,3 +201,34 @@ def test_matrix_free_requires_prepare():
     out = torch.empty(max(1, gpu.n_owned), dtype=torch.float64, device="cuda")
     with pytest.raises(FneError):
         _lib.check(_lib.lib.fne_hvp(gpu._handle, x.data_ptr(), out.data_ptr(), None))
+
+
+@pytest.mark.parametrize("degree", [2, 4])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_mc_nonzero_previous_plastic_strain(degree, precision):
+    """A non-zero eps_p_old (strain = B u - eps_p_old at every quadrature
+    point) through the CUDA-core FP64 kernel, the tensor-core FP32 kernel and
+    the matrix-free product, against the oracle."""
+    from scipy import sparse
+
+    params = meshes.slope_problem(level=1, degree=degree, lam=1.2, with_elem_B=True)
+    rng = np.random.default_rng(41)
+    params["eps_p_old"] = 2e-4 * rng.standard_normal(params["eps_p_old"].shape)
+    hd = torch.float32 if precision == "fp32" else torch.float64
+    gpu, ref = _pair(params, precision=precision, hess_dtype=hd)
+    assert gpu.info["kernel_variant"] == (6 if precision == "fp32" else 5)
+    u = 0.03 * rng.standard_normal(gpu.layout.n_free)
+    e_ref, g_ref, h_ref = ref.all_in_one(u)
+    ut = torch.as_tensor(u, device="cuda")
+    e, g, h = gpu.eval(ut, 7)
+    tol = FP64_TOL if precision == "fp64" else FP32_TOL
+    etol = 1e-12 if precision == "fp64" else 1e-5
+    assert abs(float(e.item()) - e_ref) <= etol * _abs_scale(ref, u)
+    assert _rel(g.cpu().numpy(), g_ref) <= (tol if precision == "fp64" else 1e-4)
+    assert _rel(h.double().cpu().numpy(), h_ref) <= tol
+    gpu.prepare_matrix_free_operator(ut)
+    x = rng.standard_normal(gpu.layout.n_free)
+    A = sparse.coo_matrix((h_ref, (gpu.layout.owned_rows, gpu.layout.owned_cols)),
+                          shape=(gpu.layout.n_free,) * 2).tocsr()
+    y = gpu.matrix_free_mult("matfree_element", torch.as_tensor(x, device="cuda")).cpu().numpy()
+    assert np.abs(y - A @ x).max() <= tol * np.abs(A @ x).max()
