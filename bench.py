@@ -12,7 +12,10 @@ Other workloads (same JSON line, same timing rules; ``--workload NAME``):
 p-Laplace 128x128 P1 (FP64, zero state), Ginzburg-Landau 1024^2 in FP64,
 the Neo-Hookean beam 160x8x8 hexes x 6 tets (FP64 and FP32 Hessian) and its
 320x16x16 refinement, and the plane-strain Mohr-Coulomb slope with P4 / P2
-triangles at h = 0.08 (203,000 elements).
+triangles at h = 0.08 (203,000 elements); the matrix-free Mohr-Coulomb
+Hessian-vector product; and whole Newton solves (``*_newton_*``: metric
+"Newton s to 1e-6 rel-grad", lower is better; the roofline line is one
+device CG iteration on the Hessian at the solution, timed on its own).
 
 ``value``: device-resident inputs, CUDA events around each pass, L2 flushed
 (1 GiB write) between passes outside the timed events; its length also keeps
@@ -61,7 +64,12 @@ FLUSH_BYTES = 1 << 30
 # with the profile summary that records it.  Keyed by (workload, kernel).
 NCU_TRAFFIC = {
     ("gl1024_fp32h", "k_sweep_tri"): (213.2e6, "profiles/k_sweep_tri_gl1024_fp32.md"),
+    # one CG iteration: k_cg_spmv 117.4 MB + k_cg_update 41.9 MB
+    ("gl1024_newton_fp64", "k_cg_spmv+k_cg_update"): (159.3e6, "profiles/k_cg_gl1024_newton_fp64.md"),
 }
+
+# CG iterations timed on their own for the Newton workloads' roofline line.
+CG_TIMED_ITERATIONS = 800
 
 
 class ClockSampler:
@@ -169,7 +177,7 @@ class Workload:
 
     def __init__(self, name, family, precision, hess_fp32, conn_nodes, geom_values, geom_bytes, has_rhs, desc,
                  build, sample, op="egh"):
-        self.op = op  # "egh": fused E+grad+Hess pass; "hvp": matrix-free H(u) x
+        self.op = op  # "egh": fused E+grad+Hess pass; "hvp": matrix-free H(u) x; "newton": one Newton solve
         self.name, self.family, self.precision, self.hess_fp32 = name, family, precision, hess_fp32
         self.conn_nodes, self.geom_values, self.geom_bytes, self.has_rhs = conn_nodes, geom_values, geom_bytes, has_rhs
         self.desc, self.build, self.sample = desc, build, sample
@@ -212,7 +220,10 @@ def slope_state(params, amplitude=0.02):
     return np.stack([ux, uy], axis=1).ravel()
 
 
-def _tri(kind, n, precision, seed_from_rank=True):
+def _tri(kind, n, precision, seed_from_rank=True, start_seed=None, sample_n=None):
+    """``start_seed``: p-Laplace start U[0, 1) from this seed (zero state when
+    None); ``sample_n``: grid of the bounded CPU sample (default min(n, 512))."""
+
     def build(rank):
         import torch
 
@@ -224,18 +235,18 @@ def _tri(kind, n, precision, seed_from_rank=True):
             params, u0 = meshes.gl_problem(n=n, seed=rank)
             asm = GLCudaAssembler(params, precision=precision, hess_dtype=hd, kernel_variant=KERNEL_VARIANT["value"])
         else:
-            params, u0 = meshes.plaplace_problem(n=n, seed=None)
+            params, u0 = meshes.plaplace_problem(n=n, seed=start_seed)
             asm = PLaplaceCudaAssembler(params, precision=precision, hess_dtype=hd, kernel_variant=KERNEL_VARIANT["value"])
         return asm, _reordered(asm, u0)
 
     def sample():
         from fenics_nonlinear_energies_b200 import meshes
 
-        m = min(n, 512)
+        m = sample_n or min(n, 512)
         if kind == "gl":
             params, u0 = meshes.gl_problem(n=m, seed=0)
         else:
-            params, u0 = meshes.plaplace_problem(n=m, seed=None)
+            params, u0 = meshes.plaplace_problem(n=m, seed=start_seed)
         return kind, {}, params, u0, 2 * m * m, f"{m}x{m} P1 grid"
 
     return build, sample
@@ -339,6 +350,21 @@ WORKLOADS = {
     "mc_p2_h0.08_fp64": Workload(
         "mc_p2_h0.08_fp64", "mc", "fp64", False, 6, 5, 8, True,
         "Mohr-Coulomb slope P2 h=0.08 (203,000 elements), 7-point rule, FP64", *_mc(2, 0.08, "fp64")),
+    "plaplace128_newton_fp64": Workload(
+        "plaplace128_newton_fp64", "plaplace", "fp64", False, 3, 7, 8, True,
+        "Newton to ||g|| <= 1e-6 ||g_0||: p-Laplace p=3, f=-10, unit square 128x128 P1 triangles (32,768 "
+        "elements), start U[0,1) seed 0; Jacobi CG rtol 1e-3, golden-section line search on [-0.5, 2], FP64",
+        *_tri("plaplace", 128, "fp64", start_seed=0, sample_n=128), op="newton"),
+    "gl1024_newton_fp64": Workload(
+        "gl1024_newton_fp64", "gl", "fp64", False, 3, 7, 8, False,
+        "Newton to ||g|| <= 1e-6 ||g_0||: Ginzburg-Landau eps=0.01, 1024x1024 P1 triangles (2,097,152 "
+        "elements), u ~ U[-0.5,0.5] seeded; Jacobi CG rtol 1e-3, golden-section line search on [-0.5, 2], FP64",
+        *_tri("gl", 1024, "fp64", sample_n=96), op="newton"),
+    "gl1024_newton_fp32h": Workload(
+        "gl1024_newton_fp32h", "gl", "fp32", True, 3, 7, 4, False,
+        "Newton to ||g|| <= 1e-6 ||g_0||: Ginzburg-Landau 1024x1024 as gl1024_newton_fp64 with FP32 element "
+        "gradients / Hessians (FP32 COO values in the CG), FP64 energy, state and CG arithmetic",
+        *_tri("gl", 1024, "fp32", sample_n=96), op="newton"),
 }
 DEFAULT_WORKLOAD = "gl1024_fp32h"
 
@@ -418,10 +444,15 @@ def run_reference(args):
             out = np.zeros(xl.size)
             np.add.at(out, asm.local.elems_local_np.ravel(), ye.ravel())
             return out
+    elif w.op == "newton":
+        from oracle.newton_cpu import newton_cpu
+
+        def step():
+            return newton_cpu(asm, u, tolg_rel=1e-6)
     else:
         def step():
             return asm.all_in_one(u)
-    for _ in range(args.warmup):
+    for _ in range(min(args.warmup, 1) if w.op == "newton" else args.warmup):
         step()
     times = []
     for _ in range(args.steps):
@@ -429,18 +460,22 @@ def run_reference(args):
         step()
         times.append(time.perf_counter() - t)
     dt = sum(times) / len(times)
-    value = n_el / dt
+    newton_op = w.op == "newton"
+    value, unit = (dt, "s") if newton_op else (n_el / dt, "elements/s")
+    metric = {"hvp": "elements/s (matrix-free H(u) x)", "newton": "Newton s to 1e-6 rel-grad"}.get(
+        w.op, "elements/s (E+grad+Hess)")
+    what = ("one Newton solve to 1e-6 relative gradient (oracle assembler, NumPy/SciPy Jacobi CG, the same "
+            "golden-section line search)" if newton_op else
+            "CPU restatement of the reference JAX element kernels (torch.func float64 autodiff) + np.add.at scatter")
     line = {
-        "impl": "reference", "metric": "elements/s (matrix-free H(u) x)" if w.op == "hvp" else
-        "elements/s (E+grad+Hess)", "value": value, "unit": "elements/s",
+        "impl": "reference", "metric": metric, "value": value, "unit": unit,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "higher_is_better": not newton_op, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
         "config": {"workload": w.name, "description": w.desc, "sample": label, "elements_per_step": n_el},
-        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": int(torch.get_num_threads()),
-                         "kind": "port",
-                         "sample": f"{label} ({n_el} elements) per step; CPU restatement of the reference JAX "
-                                   "element kernels (torch.func float64 autodiff) + np.add.at scatter"},
-        "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": int(torch.get_num_threads()),
+                         "kind": "port", "sample": f"{label} ({n_el} elements) per step; {what}"},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -537,6 +572,159 @@ def run_hvp(args, w, world, rank, local):
     return 0
 
 
+class _CountingAssembler:
+    """Forwards to an assembler and counts the kernels its evaluations launch."""
+
+    def __init__(self, asm):
+        self._asm = asm
+        self.launches = 0
+
+    def eval(self, u, flags, **kw):
+        self.launches += self._asm.launches_per_eval(flags)
+        return self._asm.eval(u, flags, **kw)
+
+    def __getattr__(self, name):
+        return getattr(self._asm, name)
+
+
+def cpu_newton_baseline(w):
+    """The CPU Newton (oracle assembler + scalar CG oracle) on the workload's bounded sample."""
+    import numpy as np
+    import torch
+
+    from oracle.assembler import OracleAssembler
+    from oracle.newton_cpu import newton_cpu
+
+    family, okw, params, u, n_el, label = w.sample()
+    asm = OracleAssembler(family, params, **okw)
+    u = np.asarray(u)[np.asarray(asm.layout.perm)]
+    times = []
+    while len(times) < 5 and sum(times) < 8.0:  # repeated solves of the same start: at least ~8 s of work
+        x, info = newton_cpu(asm, u, tolg_rel=1e-6)
+        times.append(info["time_s"])
+    return {"value": sum(times) / len(times), "unit": "s", "cores": int(torch.get_num_threads()), "kind": "port",
+            "sample": f"{label} ({n_el} elements): Newton solve to 1e-6 relative gradient on the host "
+                      f"(oracle assembler, NumPy/SciPy CG, same line search), mean of {len(times)}: "
+                      f"{info['iterations']} Newton, {info['ksp_its']} CG iterations, converged={info['converged']}",
+            "newton_iterations": info["iterations"], "ksp_iterations": info["ksp_its"]}
+
+
+def run_newton(args, w, world, rank, local):
+    """One step = one Newton solve from the workload's seeded start to
+    ||g|| <= 1e-6 ||g_0|| on the device: assembly kernels, the device CG
+    (fne_cg_*) and the golden-section line search, host logic in between."""
+    import numpy as np
+    import torch
+
+    from fenics_nonlinear_energies_b200.newton import DeviceCG, newton
+
+    t_setup = time.perf_counter()
+    asm, u0 = w.build(rank)
+    t_setup = time.perf_counter() - t_setup
+    n_el = int(asm.info["n_elem"])
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    cg = DeviceCG.for_assembler(asm)
+    casm = _CountingAssembler(asm)
+    kw = dict(tolg_rel=1e-6, cg=cg)
+    u = torch.as_tensor(u0, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        newton(casm, u, **kw)
+        flush.fill_(1.0)
+    torch.cuda.synchronize()
+    casm.launches, cg.launches = 0, 0
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e2e = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    pin_u = torch.from_numpy(np.ascontiguousarray(u0)).pin_memory()
+    host_x = torch.empty(asm.n_owned, dtype=torch.float64).pin_memory()
+    infos = []
+    # The solve is host-driven (line-search decisions, one read per CG graph),
+    # so both timed loops run under the same clock sampling load on the host.
+    with ClockSampler(local) as clk:
+        _barrier(world)
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            evs[i][0].record(stream)
+            x, info = newton(casm, u, **kw)
+            evs[i][1].record(stream)
+            infos.append(info)
+        torch.cuda.synchronize()
+        _barrier(world)
+        launches = casm.launches + cg.launches
+        # e2e: start vector H2D from pinned memory, the solve, D2H of the solution
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            e2e[i][0].record(stream)
+            du = pin_u.to(dev, non_blocking=True)
+            x, _ = newton(casm, du, **kw)
+            host_x.copy_(x, non_blocking=True)
+            e2e[i][1].record(stream)
+        torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    total_s = _max_over_ranks(sum(ms) * 1e-3, world)
+    s_per_solve = total_s / args.steps
+    e2e_s = _max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e) * 1e-3, world) / args.steps
+
+    # roofline of the dominant kernel pair (one CG iteration: k_cg_spmv +
+    # k_cg_update) on the Hessian at the solution, timed on its own
+    from fenics_nonlinear_energies_b200 import _lib
+
+    asm.eval(x, _lib.FNE_HESS)
+    cg.update(asm.owned_values)
+    b = torch.as_tensor(np.random.default_rng(rank).standard_normal(asm.n_owned), device=dev)
+    cg.solve(b, rtol=0.0, maxit=64)
+    flush.fill_(2.0)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    _, cg_its = cg.solve(b, rtol=0.0, maxit=CG_TIMED_ITERATIONS)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    us_it = c0.elapsed_time(c1) * 1e3 / max(1, cg_its)
+    n, nnz = asm.n_owned, int(asm.owned_values.numel())
+    vb = asm.owned_values.element_size()
+    alg = nnz * (vb + 4) + (n + 1) * 4 + 12 * n * 8
+    peak, peak_kind = _peaks()
+    achieved = alg / (us_it * 1e-6) / 1e9
+    traffic = NCU_TRAFFIC.get((w.name, "k_cg_spmv+k_cg_update"))
+    its = [i["iterations"] for i in infos]
+    ksp = [sum(h["ksp_its"] for h in i["history"]) for i in infos]
+    if rank == 0:
+        cpu = cpu_newton_baseline(w) if (world == 1 and not args.no_cpu_baseline) else None
+        line = {
+            "metric": "Newton s to 1e-6 rel-grad", "value": s_per_solve, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": s_per_solve * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
+            "data": "synthetic (seeded start on the generated mesh)",
+            "config": {"workload": w.name, "description": w.desc, "elements": n_el, "free_dofs": asm.layout.n_free,
+                       "coo_nnz": nnz, "newton_iterations": its, "cg_iterations": ksp,
+                       "converged": [bool(i["converged"]) for i in infos], "energy": infos[-1]["energy"],
+                       "solves_per_s_all_gpus": world / s_per_solve, "setup_s": t_setup,
+                       "l2": "flushed by a 1 GiB write between solves",
+                       "parallelism": f"{world} independent replica(s), one per GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": f"{peak_kind} burst copy (hbm_gbs)",
+                         "traffic": traffic[0] if traffic else None,
+                         "traffic_source": traffic[1] if traffic else None,
+                         "algorithmic_bytes_per_launch": alg, "kernel": "k_cg_spmv+k_cg_update",
+                         "unit_of_launch": "one CG iteration (two kernels)", "us_per_cg_iteration": us_it,
+                         "cg_iterations_timed": cg_its},
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(u0.nbytes),
+                    "d2h_bytes_per_step": int(host_x.numel() * 8)},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    cg.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def run(args):
     import numpy as np
     import torch
@@ -548,6 +736,8 @@ def run(args):
     w = WORKLOADS[args.workload]
     if w.op == "hvp":
         return run_hvp(args, w, world, rank, local)
+    if w.op == "newton":
+        return run_newton(args, w, world, rank, local)
     t_setup = time.perf_counter()
     asm, u0 = w.build(rank)
     t_setup = time.perf_counter() - t_setup

@@ -89,6 +89,11 @@ def _load():
         "fne_hvp_prepare": (C.c_int, [vp, vp, vp]),
         "fne_hvp": (C.c_int, [vp, vp, vp, vp]),
         "fne_hvp_diagonal": (C.c_int, [vp, vp, vp]),
+        "fne_cg_create": (C.c_int, [C.c_int32, C.c_int64, _i64p, _i64p, C.c_int32, C.c_int32, C.POINTER(vp)]),
+        "fne_cg_set_matrix": (C.c_int, [vp, vp, vp]),
+        "fne_cg_solve": (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                   vp]),
+        "fne_cg_destroy": (C.c_int, [vp]),
         "fne_energy_p1tri_noalloc": (C.c_int, [C.c_int32, C.c_int64, vp, vp, vp, vp, vp, vp, vp, _f64p, vp,
                                                C.c_int64, C.c_int64, vp, vp]),
         "fne_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int64, C.c_int64, vp, C.c_int64, C.c_int64,

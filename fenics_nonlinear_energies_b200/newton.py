@@ -14,7 +14,8 @@ need so that Newton iterations can be counted without PETSc:
   the energy, optional stop on the energy change.
 
 The linear solve is Jacobi-preconditioned conjugate gradients on the
-assembled owned COO values (cuSPARSE SpMV through torch); CG stops at a
+assembled owned COO values (``DeviceCG``: the library's own CG kernels,
+``fne_cg_*``, every iteration on the device); CG stops at a
 negative-curvature direction and returns the last iterate (or the steepest
 descent direction), which keeps the Newton direction a descent direction for
 the non-convex Ginzburg-Landau energy.
@@ -22,9 +23,9 @@ the non-convex Ginzburg-Landau energy.
 
 from __future__ import annotations
 
+import ctypes
 import math
 import time
-import warnings
 
 import numpy as np
 import torch
@@ -105,80 +106,92 @@ def repair_linesearch_interval(f, a, b, center=0.0, center_value=None, tol=1e-6,
     return side(float(a), -1.0), side(float(b), 1.0), n_evals, repaired
 
 
-class CsrOperator:
-    """Owned COO values of an assembler viewed as a CSR matrix in reordered numbering."""
+class DeviceCG:
+    """Jacobi-preconditioned CG on an assembler's owned COO Hessian (``fne_cg_*``).
 
-    def __init__(self, assembler):
-        rows = np.asarray(assembler.layout.owned_rows, dtype=np.int64) - assembler.layout.lo
-        cols = np.asarray(assembler.layout.owned_cols, dtype=np.int64)
-        n = assembler.n_owned
-        order = np.argsort(rows, kind="stable")
-        dev = assembler.device
-        self.order = torch.as_tensor(order, device=dev)
-        counts = np.bincount(rows, minlength=n)
-        crow = np.concatenate(([0], np.cumsum(counts)))
-        self.crow = torch.as_tensor(crow, dtype=torch.int64, device=dev)
-        self.col = torch.as_tensor(cols[order], dtype=torch.int64, device=dev)
-        diag_pos = np.full(n, -1, dtype=np.int64)
-        is_diag = rows == cols
-        diag_pos[rows[is_diag]] = np.flatnonzero(is_diag)
-        self.diag_pos = torch.as_tensor(np.maximum(diag_pos, 0), device=dev)
-        self.has_diag = torch.as_tensor(diag_pos >= 0, device=dev)
-        self.n = n
-        self.A = None
-        self.dinv = None
+    The pattern is the one-rank owned COO pattern (``owned_rows - lo``,
+    ``owned_cols``); values are taken in COO order from
+    ``assembler.owned_values`` (FP32 or FP64 storage, FP64 arithmetic).  Every
+    CG iteration runs on the device; the host reads the solver state once per
+    CUDA graph of ``chunk`` iterations.
+    """
+
+    REASONS = ("converged", "non-positive curvature", "iteration limit", "zero right-hand side")
+
+    def __init__(self, n, rows, cols, *, fp32=False, device="cuda", chunk=16):
+        self._h = None
+        self.n = int(n)
+        self.device = torch.device(device)
+        self.fp32 = bool(fp32)
+        _, rp = rows_arr = _lib.i64(rows)
+        _, cp = cols_arr = _lib.i64(cols)
+        if rows_arr[0].size != cols_arr[0].size:
+            raise ValueError("rows and cols differ in length")
+        h = ctypes.c_void_p()
+        _lib.check(_lib.lib.fne_cg_create(self.n, int(rows_arr[0].size), rp, cp, int(self.fp32), int(chunk),
+                                          ctypes.byref(h)))
+        self._h = h
+        self.chunk = int(chunk)
+        self.reason = None
+        self.launches = 0  # kernels launched by update() and solve() so far
+
+    @classmethod
+    def for_assembler(cls, assembler, chunk=16):
+        lay = assembler.layout
+        rows = np.asarray(lay.owned_rows, dtype=np.int64) - lay.lo
+        return cls(assembler.n_owned, rows, lay.owned_cols, fp32=assembler.owned_values.dtype == torch.float32,
+                   device=assembler.device, chunk=chunk)
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
 
     def update(self, values):
-        v = values.double()
-        with warnings.catch_warnings():
-            warnings.simplefilter("ignore", UserWarning)  # beta-state / invariant-check notices
-            self.A = torch.sparse_csr_tensor(self.crow, self.col, v.index_select(0, self.order),
-                                             size=(self.n, self.n), check_invariants=False)
-        d = torch.where(self.has_diag, v.index_select(0, self.diag_pos), torch.ones_like(v[: self.n]))
-        d = torch.where(d.abs() > 0, d.abs(), torch.ones_like(d))
-        self.dinv = 1.0 / d
+        want = torch.float32 if self.fp32 else torch.float64
+        if values.dtype != want or not values.is_contiguous():
+            raise TypeError(f"COO values must be a contiguous {want} tensor")
+        self._values = values
+        _lib.check(_lib.lib.fne_cg_set_matrix(self._h, values.data_ptr(), self._stream()))
+        self.launches += 1
 
-    def matvec(self, x):
-        return (self.A @ x.unsqueeze(1)).squeeze(1)
+    def solve(self, b, rtol=1e-3, maxit=500, out=None):
+        """``x`` with ``A x = b`` to ``rtol`` (stopping rules of ``fne_cg_solve``); returns ``(x, iterations)``."""
+        b = b.contiguous()
+        x = torch.empty_like(b) if out is None else out
+        its, why = ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(_lib.lib.fne_cg_solve(self._h, b.data_ptr(), x.data_ptr(), float(rtol), int(maxit),
+                                         ctypes.byref(its), ctypes.byref(why), self._stream()))
+        self.reason = self.REASONS[why.value]
+        # one initialisation kernel, then graphs of `chunk` iterations of two
+        # kernels until the iteration that stopped the solve
+        self.launches += 1 + 2 * self.chunk * (-(-int(its.value) // self.chunk))
+        return x, int(its.value)
 
+    def close(self):
+        if self._h:
+            _lib.lib.fne_cg_destroy(self._h)
+            self._h = None
 
-def pcg(op, b, rtol=1e-3, maxit=500):
-    """Jacobi-preconditioned CG; stops at negative curvature.  Returns ``(x, iterations)``."""
-    x = torch.zeros_like(b)
-    r = b.clone()
-    z = op.dinv * r
-    p = z.clone()
-    rz = torch.dot(r, z)
-    bnorm = float(torch.linalg.vector_norm(b))
-    if bnorm == 0.0:
-        return x, 0
-    for it in range(1, maxit + 1):
-        Ap = op.matvec(p)
-        pAp = float(torch.dot(p, Ap))
-        if not (pAp > 0.0):
-            return (x if it > 1 else b.clone()), it
-        alpha = float(rz) / pAp
-        x.add_(p, alpha=alpha)
-        r.add_(Ap, alpha=-alpha)
-        if float(torch.linalg.vector_norm(r)) <= rtol * bnorm:
-            return x, it
-        z = op.dinv * r
-        rz_new = torch.dot(r, z)
-        p.mul_(float(rz_new) / float(rz)).add_(z)
-        rz = rz_new
-    return x, maxit
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def newton(assembler, x0, *, tolg=0.0, tolg_rel=1e-6, tolf=0.0, maxit=100, linesearch_interval=(-0.5, 2.0),
-           linesearch_tol=1e-3, ksp_rtol=1e-3, ksp_max_it=500, verbose=False):
+           linesearch_tol=1e-3, ksp_rtol=1e-3, ksp_max_it=500, verbose=False, cg=None):
     """Minimise the assembler's energy from ``x0`` (device tensor of the owned reordered DOFs).
 
     Returns ``(x, info)`` with ``info["iterations"]`` the number of Newton
     steps taken, ``info["converged"]``, the final energy and gradient norm.
+    ``cg``: a ``DeviceCG`` for this assembler's pattern to reuse across calls
+    (one is created and released per call otherwise).
     """
     dev = assembler.device
     x = torch.as_tensor(x0, dtype=torch.float64, device=dev).clone()
-    op = CsrOperator(assembler)
+    own_cg = cg is None
+    if own_cg:
+        cg = DeviceCG.for_assembler(assembler)
     flags_eg = _lib.FNE_ENERGY | _lib.FNE_GRAD
     e_buf = torch.empty(1, dtype=torch.float64, device=dev)
     g = torch.empty(assembler.n_owned, dtype=torch.float64, device=dev)
@@ -212,8 +225,8 @@ def newton(assembler, x0, *, tolg=0.0, tolg_rel=1e-6, tolf=0.0, maxit=100, lines
             break
         nit += 1
         assembler.eval(x, _lib.FNE_HESS)
-        op.update(assembler.owned_values)
-        p, ksp_its = pcg(op, -g, rtol=ksp_rtol, maxit=ksp_max_it)
+        cg.update(assembler.owned_values)
+        p, ksp_its = cg.solve(-g, rtol=ksp_rtol, maxit=ksp_max_it)
 
         def f_alpha(alpha):
             torch.add(x, p, alpha=alpha, out=x_trial)
@@ -243,4 +256,6 @@ def newton(assembler, x0, *, tolg=0.0, tolg_rel=1e-6, tolf=0.0, maxit=100, lines
     info = {"iterations": nit, "message": message, "energy": fx, "grad_norm": normg, "grad_norm0": g0,
             "converged": g0 is not None and normg < max(tolg, tolg_rel * g0) * (1.0 + 1e-12),
             "time_s": time.perf_counter() - t0, "history": history}
+    if own_cg:
+        cg.close()
     return x, info

@@ -190,10 +190,12 @@ def run_load_path(params, theta_total, steps, *, predictor=None, features=None, 
     charged.  Returns per-step records (and the solutions when ``record``).
     """
     from fenics_nonlinear_energies_b200.assembler import HECudaAssembler
+    from fenics_nonlinear_energies_b200.newton import DeviceCG
 
     kw = dict(tolg_rel=1e-6, linesearch_tol=1e-3, ksp_rtol=1e-2, ksp_max_it=2000, maxit=200)
     kw.update(newton_kw or {})
     asm = HECudaAssembler(params)
+    kw["cg"] = DeviceCG.for_assembler(asm)
     lay = asm.layout
     free = np.asarray(params["freedofs"], dtype=np.int64)
     X_free = np.asarray(params["u_0_ref"], dtype=np.float64)[free]
@@ -241,6 +243,7 @@ def run_load_path(params, theta_total, steps, *, predictor=None, features=None, 
         y = to_host(x_use)
         if record:
             sols.append(y.copy())
+    kw["cg"].close()
     asm.cleanup()
     return (recs, sols) if record else recs
 

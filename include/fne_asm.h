@@ -247,6 +247,40 @@ int fne_energy_p1tri_noalloc(int32_t family, int64_t n_elem, const int32_t* code
                              int64_t n_owned, int64_t lo, double* energy, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Newton linear solve on the device: Jacobi-preconditioned CG on the owned
+ * COO Hessian.  Replaces, for single-GPU Newton runs, the KSP solve the
+ * reference drives with the assembled matrix
+ * (core/petsc/scalar_problem_driver.py:154-226: ksp.setOperators,
+ * ksp.setTolerances(rtol, max_it), ksp.solve, ksp.getIterationNumber;
+ * hyperelasticity/jax_petsc/solver.py:257-330 the same).  Every iteration
+ * runs on the device (two kernels, in-kernel fixed-order reductions); the
+ * host reads the solver state once per CUDA graph of `chunk` iterations.
+ * ------------------------------------------------------------------------- */
+typedef struct fne_cg fne_cg;
+/* Square n x n pattern from the COO entries (rows[k], cols[k]), 0-based local
+ * indices in [0, n) (host arrays, e.g. owned_rows - lo and owned_cols of a
+ * one-rank layout); the CSR order keeps the COO order within a row.
+ * vals_fp32 = 1 stores FP32 values (the FP32-Hessian assemblers' output),
+ * 0 FP64; the arithmetic is FP64 either way.  FNE_EBOUNDS for an entry
+ * outside the block.  Allocates all device memory the solves use. */
+int fne_cg_create(int32_t n, int64_t nnz, const int64_t* rows, const int64_t* cols, int32_t vals_fp32,
+                  int32_t chunk, fne_cg** out);
+/* Takes the matrix values in COO order (device pointer, float or double as
+ * created) and the Jacobi scaling 1/|a_ii| (1 for a missing, zero or NaN
+ * diagonal).  Stream-ordered. */
+int fne_cg_set_matrix(fne_cg* cg, const void* coo_vals, void* stream);
+/* Solves A x = b (device pointers, FP64, length n) from x = 0.  Stops at the
+ * first iterate with ||r|| <= rtol ||b||, at a non-positive curvature p.Ap
+ * (returning the last iterate, or b itself at the first iteration), or after
+ * maxit iterations.  *its = iterations taken (1 for the first-iteration
+ * curvature stop, 0 for b = 0); *reason = 0 converged, 1 non-positive
+ * curvature, 2 iteration limit, 3 zero right-hand side.  Synchronises the
+ * stream once per `chunk` iterations; a handle runs one solve at a time. */
+int fne_cg_solve(fne_cg* cg, const double* b, double* x, double rtol, int32_t maxit, int32_t* its, int32_t* reason,
+                 void* stream);
+int fne_cg_destroy(fne_cg* cg);
+
+/* ---------------------------------------------------------------------------
  * Learned Newton warm start (no counterpart in the reference).  Kernels of a
  * small MLP over nodal features: BF16 operands, FP32 accumulation / master
  * weights.  All pointers are device pointers; BF16 arrays are passed as void*.

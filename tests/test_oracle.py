@@ -126,3 +126,36 @@ def test_mlp_oracle_bf16_rounding():
 
     x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, -2.5, 0.0], dtype=np.float32)
     np.testing.assert_array_equal(bf16_round(x), [1.0, 1.0, 1.0 + 2 ** -7, -2.5, 0.0])
+
+
+
+@pytest.mark.parametrize("case", ["spd", "indefinite_late", "indefinite_first", "maxit", "zero_rhs"])
+def test_scalar_cg_oracle(case):
+    from oracle import krylov
+
+    rng = np.random.default_rng(7)
+    n = 60
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    ev = np.linspace(1.0, 50.0, n)
+    if case == "indefinite_late":
+        ev[:3] = [-4.0, -2.0, -1.0]
+    if case == "indefinite_first":
+        ev[:] = -np.linspace(1.0, 5.0, n)
+    A = (Q * ev) @ Q.T
+    A = 0.5 * (A + A.T)
+    b = np.zeros(n) if case == "zero_rhs" else rng.standard_normal(n)
+    dinv = krylov.jacobi_scaling(np.diag(A))
+    rtol, maxit = (1e-10, 7) if case == "maxit" else (1e-10, 200)
+    x, it, why = krylov.pcg(A, dinv, b, rtol, maxit)
+    if case == "spd":
+        assert why == krylov.CONVERGED and it < n + 5
+        np.testing.assert_allclose(x, np.linalg.solve(A, b), rtol=1e-8, atol=1e-10)
+    elif case == "indefinite_late":
+        assert why == krylov.NEGATIVE_CURVATURE and it > 1 and (x @ b) > 0  # descent for the quadratic
+    elif case == "indefinite_first":
+        assert (it, why) == (1, krylov.NEGATIVE_CURVATURE) and np.array_equal(x, b)
+    elif case == "maxit":
+        assert (it, why) == (7, krylov.ITERATION_LIMIT)
+    else:
+        assert (it, why) == (0, krylov.ZERO_RHS) and not x.any()
+    np.testing.assert_array_equal(krylov.jacobi_scaling([2.0, -4.0, 0.0, np.nan]), [0.5, 0.25, 1.0, 1.0])
