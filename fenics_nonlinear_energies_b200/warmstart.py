@@ -219,9 +219,10 @@ def run_load_path(params, theta_total, steps, *, predictor=None, features=None, 
             params["u_0_ref"], params["nodes2coord"], theta, params["right_nodes"]))
         t0 = time.perf_counter()
         x_plain, info_plain = newton(asm, to_dev(y), **kw)
+        t_plain = time.perf_counter() - t0
         rec = {"step": k, "theta": theta, "plain_its": info_plain["iterations"],
                "plain_converged": info_plain["converged"], "plain_message": info_plain["message"],
-               "energy": info_plain["energy"]}
+               "energy": info_plain["energy"], "plain_s": t_plain}
         x_use = x_plain
         if predictor is not None:
             u_k = (y - X_free).reshape(-1, 3)
@@ -229,12 +230,14 @@ def run_load_path(params, theta_total, steps, *, predictor=None, features=None, 
             du = predictor(features.features(u_k, u_km1, dtheta, theta - dtheta, E)) * features.w
             y_pred = y + du.reshape(-1)
             x_pred, info_pred = newton(asm, to_dev(y_pred), **kw)
+            t_pred = time.perf_counter() - t0 - t_plain  # prediction (features, MLP) + Newton from it
             same = (info_pred["converged"] and info_plain["converged"] and
                     abs(info_pred["energy"] - info_plain["energy"]) <= 1e-8 * max(1.0, abs(info_plain["energy"])))
             rec.update(pred_its=info_pred["iterations"], pred_converged=info_pred["converged"],
                        pred_energy=info_pred["energy"], accepted=bool(same),
                        learned_its=info_pred["iterations"] if same else
-                       info_pred["iterations"] + info_plain["iterations"])
+                       info_pred["iterations"] + info_plain["iterations"],
+                       learned_s=t_pred if same else t_pred + t_plain)
             if same:
                 x_use = x_pred
         rec["time_s"] = time.perf_counter() - t0

@@ -74,13 +74,18 @@ def run(nx=80, ny=4, nz=4, train_paths=16, test_paths=4, steps=24, epochs=150, s
         p = sum(r["plain_its"] for r in recs)
         q = sum(r["learned_its"] for r in recs)
         a = sum(r["accepted"] for r in recs)
+        ps = sum(r["plain_s"] for r in recs)
+        qs = sum(r["learned_s"] for r in recs)
         plain_its += p
         learned_its += q
         accepted += a
         n_steps += len(recs)
+        plain_time += ps
+        learned_time += qs
         per_path.append({"theta_total": theta, "E": E, "plain_its": p, "learned_its": q, "accepted_steps": a,
+                         "plain_s": ps, "learned_s": qs,
                          "steps": len(recs), "plain_converged": all(r["plain_converged"] for r in recs)})
-        log(f"test path {j}: plain {p} learned {q} accepted {a}/{len(recs)}")
+        log(f"test path {j}: plain {p} its {ps:.2f} s, learned {q} its {qs:.2f} s, accepted {a}/{len(recs)}")
     out = {
         "mesh": {"hexes": [nx, ny, nz], "tets": 6 * nx * ny * nz},
         "steps_per_path": steps, "train_paths": train_paths, "test_paths": test_paths,
@@ -90,7 +95,9 @@ def run(nx=80, ny=4, nz=4, train_paths=16, test_paths=4, steps=24, epochs=150, s
         "generation": {"newton_its": gen_its, "steps": gen_steps, "failed_steps": gen_fail, "failure_messages": fail_msgs,
                        "time_s": gen_time},
         "test": {"plain_newton_its": plain_its, "learned_newton_its": learned_its, "accepted_steps": accepted,
-                 "steps": n_steps, "reduction": 1.0 - learned_its / max(1, plain_its), "paths": per_path},
+                 "steps": n_steps, "reduction": 1.0 - learned_its / max(1, plain_its),
+                 "plain_newton_s": plain_time, "learned_newton_s": learned_time,
+                 "time_reduction": 1.0 - learned_time / max(1e-12, plain_time), "paths": per_path},
         "tolerance": "||g|| <= 1e-6 ||g_0|| per step", "total_time_s": time.perf_counter() - t_all,
     }
     return out
