@@ -76,6 +76,7 @@ def _load():
     vp = C.c_void_p
     sig = {
         "fne_layout_build": (C.c_int, [C.POINTER(LayoutDesc), C.POINTER(vp)]),
+        "fne_layout_build_device": (C.c_int, [C.POINTER(LayoutDesc), C.POINTER(vp)]),
         "fne_layout_sizes": (C.c_int, [vp, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),
         "fne_layout_copy": (C.c_int, [vp] + [_i64p] * 8),
         "fne_layout_free": (None, [vp]),
@@ -134,8 +135,13 @@ def f64(a):
 
 
 def build_layout(*, freedofs, elems, n_total, block_size, reorder="block_xyz", coords=None,
-                 perm_override=None, adjacency=None, rank=0, size=1):
-    """C++ ``build_global_layout``; returns a dict of int64 arrays + lo/hi."""
+                 perm_override=None, adjacency=None, rank=0, size=1, device=False):
+    """``build_global_layout``; returns a dict of int64 arrays + lo/hi.
+
+    ``device=False``: the host C++ build (``fne_layout_build``);
+    ``device=True``: the same arrays built on the current CUDA device
+    (``fne_layout_build_device``) and copied back.
+    """
     keep = []
     d = LayoutDesc()
     fd, d.freedofs = i64(freedofs)
@@ -161,22 +167,32 @@ def build_layout(*, freedofs, elems, n_total, block_size, reorder="block_xyz", c
         keep += [ip, ix]
     d.comm_rank, d.comm_size = int(rank), int(size)
     h = C.c_void_p()
-    check(lib.fne_layout_build(C.byref(d), C.byref(h)))
+    check((lib.fne_layout_build_device if device else lib.fne_layout_build)(C.byref(d), C.byref(h)))
     try:
         nf, lo, hi, nnz_t, nnz_o, ne = (C.c_int64() for _ in range(6))
         check(lib.fne_layout_sizes(h, C.byref(nf), C.byref(lo), C.byref(hi), C.byref(nnz_t),
                                    C.byref(nnz_o), C.byref(ne)))
+        # one rank owns every row: the owned COO arrays are the COO arrays
+        # (copied once, the same read-only NumPy arrays under both names)
+        shared = int(size) == 1 and nnz_t.value == nnz_o.value
         out = {
             "perm": np.empty(nf.value, np.int64), "iperm": np.empty(nf.value, np.int64),
             "total_to_free_reord": np.empty(int(n_total), np.int64),
-            "coo_rows": np.empty(nnz_t.value, np.int64), "coo_cols": np.empty(nnz_t.value, np.int64),
             "owned_rows": np.empty(nnz_o.value, np.int64), "owned_cols": np.empty(nnz_o.value, np.int64),
             "elem_owner": np.empty(ne.value, np.int64),
         }
+        if shared:
+            out["coo_rows"], out["coo_cols"] = out["owned_rows"], out["owned_cols"]
+        else:
+            out["coo_rows"] = np.empty(nnz_t.value, np.int64)
+            out["coo_cols"] = np.empty(nnz_t.value, np.int64)
         ptr = lambda k: out[k].ctypes.data_as(_i64p)  # noqa: E731
         check(lib.fne_layout_copy(h, ptr("perm"), ptr("iperm"), ptr("total_to_free_reord"),
-                                  ptr("coo_rows"), ptr("coo_cols"), ptr("owned_rows"),
-                                  ptr("owned_cols"), ptr("elem_owner")))
+                                  None if shared else ptr("coo_rows"), None if shared else ptr("coo_cols"),
+                                  ptr("owned_rows"), ptr("owned_cols"), ptr("elem_owner")))
+        if shared:
+            for k in ("owned_rows", "owned_cols"):
+                out[k].flags.writeable = False
         out["lo"], out["hi"], out["n_free"] = lo.value, hi.value, nf.value
         return out
     finally:

@@ -15,7 +15,9 @@ Hessian values land in ``self.owned_values`` (a CUDA tensor, COO order of
 does (:1046-1050).
 
 Family subclasses mirror the reference's ``_make_local_element_kernels``
-implementations; the kernels themselves are in ``csrc/fne_asm.cu``.
+implementations; the kernels themselves are in ``csrc/fne_asm.cu``.  The
+layout is built on the device (``fne_layout_build_device``) unless
+``layout_on_device=False`` selects the host build; both give the same arrays.
 """
 
 from __future__ import annotations
@@ -51,7 +53,7 @@ class CudaElementAssemblerBase:
     local_elem_data_keys: tuple[str, ...] = ()
 
     def __init__(self, params, comm=None, adjacency=None, *, reorder_mode="block_xyz", perm_override=None,
-                 precision="fp64", hess_dtype=None, device=None, kernel_variant="auto",
+                 precision="fp64", hess_dtype=None, device=None, kernel_variant="auto", layout_on_device=True,
                  **_ignored_solver_kwargs):
         if not torch.cuda.is_available():
             raise RuntimeError("CudaElementAssemblerBase needs a CUDA device (no CPU fallback)")
@@ -85,6 +87,7 @@ class CudaElementAssemblerBase:
             freedofs=freedofs, elems=elems, n_total=n_total, block_size=self.block_size,
             reorder=reorder_mode, coords=np.asarray(params[self.coordinate_key], dtype=np.float64),
             perm_override=perm_override, adjacency=adjacency, rank=self.rank, size=self.size,
+            device=bool(layout_on_device),
         )
         self._setup_timings["global_layout"] = time.perf_counter() - t0
         self.layout = SimpleNamespace(**lay)

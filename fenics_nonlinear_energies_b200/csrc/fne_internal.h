@@ -7,7 +7,28 @@
 
 #include "../../include/fne_asm.h"
 
+// Result of fne_layout_build (host vectors) or fne_layout_build_device (the
+// same arrays in device memory; the host vectors stay empty).
+struct fne_layout {
+  int64_t n_total = 0, n_free = 0, lo = 0, hi = 0, n_elem = 0;
+  std::vector<int64_t> perm, iperm, t2f, coo_rows, coo_cols, owned_rows, owned_cols, elem_owner;
+  bool on_device = false;
+  struct {
+    int64_t nnz_total = 0, nnz_owned = 0;
+    int64_t *perm = nullptr, *iperm = nullptr, *t2f = nullptr, *coo_rows = nullptr, *coo_cols = nullptr,
+            *owned_rows = nullptr, *owned_cols = nullptr, *elem_owner = nullptr;
+    bool owned_is_coo = false;  // one rank: the owned arrays alias the COO arrays
+  } dev;
+};
+
 namespace fne {
+
+// Device layout arrays: D2H copy into caller buffers / release.
+int layout_device_copy(const fne_layout* L, int64_t* perm, int64_t* iperm, int64_t* t2f, int64_t* coo_rows,
+                       int64_t* coo_cols, int64_t* owned_rows, int64_t* owned_cols, int64_t* elem_owner);
+void layout_device_release(fne_layout* L);
+// Host-side argument checks shared by the host and device layout builds.
+int layout_check_desc(const fne_layout_desc* d);
 
 // Thread-local last-error message (fne_last_error()).
 int set_error(int code, const std::string& msg);

@@ -82,14 +82,9 @@ void element_adjacency(int64_t n_total, int64_t n_free, const int64_t* freedofs,
 
 using namespace fne;
 
-struct fne_layout {
-  int64_t n_total = 0, n_free = 0, lo = 0, hi = 0, n_elem = 0;
-  std::vector<int64_t> perm, iperm, t2f, coo_rows, coo_cols, owned_rows, owned_cols, elem_owner;
-};
+namespace fne {
 
-extern "C" int fne_layout_build(const fne_layout_desc* d, fne_layout** out) {
-  if (!d || !out) return set_error(FNE_EINVAL, "fne_layout_build: null argument");
-  *out = nullptr;
+int layout_check_desc(const fne_layout_desc* d) {
   const int bs = d->block_size;
   if (bs < 1 || d->n_free < 0 || d->n_total < d->n_free || d->ndof_e < 1 || d->n_elem < 0 ||
       d->comm_size < 1 || d->comm_rank < 0 || d->comm_rank >= d->comm_size)
@@ -105,6 +100,16 @@ extern "C" int fne_layout_build(const fne_layout_desc* d, fne_layout** out) {
   for (int64_t i = 0; i < d->n_elem * (int64_t)d->ndof_e; ++i)
     if (d->elems[i] < 0 || d->elems[i] >= d->n_total)
       return set_error(FNE_EBOUNDS, "fne_layout_build: element DOF out of range");
+  return FNE_OK;
+}
+
+}  // namespace fne
+
+extern "C" int fne_layout_build(const fne_layout_desc* d, fne_layout** out) {
+  if (!d || !out) return set_error(FNE_EINVAL, "fne_layout_build: null argument");
+  *out = nullptr;
+  const int bs = d->block_size;
+  if (const int rc = layout_check_desc(d); rc != FNE_OK) return rc;
 
   auto* L = new (std::nothrow) fne_layout();
   if (!L) return set_error(FNE_ENOMEM, "fne_layout_build: out of host memory");
@@ -219,8 +224,8 @@ extern "C" int fne_layout_sizes(const fne_layout* L, int64_t* n_free, int64_t* l
   if (n_free) *n_free = L->n_free;
   if (lo) *lo = L->lo;
   if (hi) *hi = L->hi;
-  if (nnz_total) *nnz_total = (int64_t)L->coo_rows.size();
-  if (nnz_owned) *nnz_owned = (int64_t)L->owned_rows.size();
+  if (nnz_total) *nnz_total = L->on_device ? L->dev.nnz_total : (int64_t)L->coo_rows.size();
+  if (nnz_owned) *nnz_owned = L->on_device ? L->dev.nnz_owned : (int64_t)L->owned_rows.size();
   if (n_elem) *n_elem = L->n_elem;
   return FNE_OK;
 }
@@ -229,6 +234,8 @@ extern "C" int fne_layout_copy(const fne_layout* L, int64_t* perm, int64_t* iper
                                int64_t* coo_rows, int64_t* coo_cols, int64_t* owned_rows,
                                int64_t* owned_cols, int64_t* elem_owner) {
   if (!L) return set_error(FNE_EINVAL, "fne_layout_copy: null layout");
+  if (L->on_device) return layout_device_copy(L, perm, iperm, t2f, coo_rows, coo_cols, owned_rows, owned_cols,
+                                              elem_owner);
   auto cp = [](int64_t* dst, const std::vector<int64_t>& v) {
     if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int64_t));
   };
@@ -243,4 +250,7 @@ extern "C" int fne_layout_copy(const fne_layout* L, int64_t* perm, int64_t* iper
   return FNE_OK;
 }
 
-extern "C" void fne_layout_free(fne_layout* L) { delete L; }
+extern "C" void fne_layout_free(fne_layout* L) {
+  if (L && L->on_device) layout_device_release(L);
+  delete L;
+}

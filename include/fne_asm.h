@@ -26,6 +26,11 @@
  *                        in layout.owned_rows/owned_cols order
  *   fne_set_dirichlet    update_dirichlet (:1560-1566)
  *   fne_destroy          cleanup (:1777-1783)
+ *   fne_layout_build_device  fne_layout_build on the GPU (same arrays)
+ *   fne_hvp*             matrix-free Mohr-Coulomb operator,
+ *                        src/problems/slope_stability/jax_petsc/reordered_element_assembler.py:335-440, 527-562
+ *   fne_cg_*             the Newton step's KSP solve on the assembled matrix (Jacobi CG),
+ *                        src/core/petsc/scalar_problem_driver.py:154-226
  */
 #ifndef FNE_ASM_H
 #define FNE_ASM_H
@@ -87,6 +92,14 @@ typedef struct {
 typedef struct fne_layout fne_layout;
 
 int fne_layout_build(const fne_layout_desc* desc, fne_layout** out);
+/* The same layout built on the current CUDA device, array for array
+ * identical: stable radix sorts of the blocks' coordinates (z, y, x) and a
+ * radix sort + unique of the element DOF-pair keys row * n_free + col.
+ * Inputs are host arrays, checked as fne_layout_build checks them; the
+ * arrays stay in device memory until fne_layout_copy (D2H) and
+ * fne_layout_free.  Needs about 16 * n_elem * ndof_e^2 bytes of device
+ * memory for the pair keys when no adjacency is given. */
+int fne_layout_build_device(const fne_layout_desc* desc, fne_layout** out);
 /* Sizes of the arrays fne_layout_copy fills. */
 int fne_layout_sizes(const fne_layout* lay, int64_t* n_free, int64_t* lo, int64_t* hi,
                      int64_t* nnz_total, int64_t* nnz_owned, int64_t* n_elem);
