@@ -335,6 +335,9 @@ WORKLOADS = {
     "mc_p4_h0.08_fp32": Workload(
         "mc_p4_h0.08_fp32", "mc", "fp32", True, 15, 5, 8, True,
         "Mohr-Coulomb slope P4 h=0.08 (203,000 elements), FP32 element grad/Hessian", *_mc(4, 0.08, "fp32")),
+    "mc_p4_h0.16_fp64": Workload(
+        "mc_p4_h0.16_fp64", "mc", "fp64", False, 15, 5, 8, True,
+        "Mohr-Coulomb slope P4 h=0.16 (about 51,000 elements), FP64 (profiling size)", *_mc(4, 0.16, "fp64")),
     "mc_p4_h0.16_fp32": Workload(
         "mc_p4_h0.16_fp32", "mc", "fp32", True, 15, 5, 8, True,
         "Mohr-Coulomb slope P4 h=0.16 (about 51,000 elements), FP32 element grad/Hessian (profiling size)",
@@ -369,7 +372,7 @@ WORKLOADS = {
 DEFAULT_WORKLOAD = "gl1024_fp32h"
 
 KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri", 5: "k_mc_elem+k_node_gather",
-                6: "k_mc_tc+k_fixup2", 7: "k_he_elem+k_node_gather", 8: "k_push_tri"}
+                6: "k_mc_tc+k_fixup2", 7: "k_he_elem+k_node_gather", 8: "k_push_tri", 9: "k_mc_dmma+k_fixup2"}
 
 
 def algorithmic_bytes(w, asm, n_el):

@@ -171,10 +171,15 @@ class CudaElementAssemblerBase:
     def launches_per_eval(self, flags):
         """Kernel launches one ``eval(u, flags)`` issues: one fused kernel for the
         triangle families and the tet row-gather kernel; element kernel plus one
-        node-block gather for Mohr-Coulomb and the element-parallel tet pass."""
-        if self.info["kernel_variant"] not in (5, 6, 7) or flags == _lib.FNE_ENERGY:
+        node-block gather for the element-parallel tet pass; for Mohr-Coulomb
+        the element kernel, the Hessian gather or shared-block fix-up, and the
+        gradient rows."""
+        kv = self.info["kernel_variant"]
+        if flags == _lib.FNE_ENERGY or kv not in (5, 6, 7, 9):
             return 1
-        return 2
+        if kv == 7:
+            return 2
+        return 1 + bool(flags & _lib.FNE_HESS) + bool(flags & _lib.FNE_GRAD)
 
     # ---- vector helpers -----------------------------------------------------
     def _stream(self):

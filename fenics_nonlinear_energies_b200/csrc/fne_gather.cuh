@@ -161,25 +161,36 @@ __global__ void __launch_bounds__(256) k_node_gather(NodeGatherArgs G, const Rea
 }
 
 // Shared-block fix-up for bs = 2 (direct-write epilogue): one thread per
-// shared output block sums its contributions (buffer slots listed in element
-// order) and writes the block's two rows.
-template <typename HOut>
+// shared output block sums its contributions (buffer slots of 4 values,
+// listed in element order) and writes the block's two rows.  SB: the
+// buffer's value type (float: tensor-core path; double: FP64 DMMA path).
+template <typename HOut, typename SB>
 __global__ void __launch_bounds__(256) k_fixup2(int n_blk, const int4* __restrict__ desc,
-                                                const int* __restrict__ slots, const float4* __restrict__ sbuf,
+                                                const int* __restrict__ slots, const SB* __restrict__ sbuf,
                                                 HOut* __restrict__ out) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n_blk; b += gridDim.x * blockDim.x) {
     const int4 ds = __ldg(desc + b);
     const int cnt = ds.w & 0xFFFF;
     const unsigned dm = (unsigned)(ds.w >> 16) & 3u;
-    float a00 = 0.f, a01 = 0.f, a10 = 0.f, a11 = 0.f;
+    SB a00 = 0, a01 = 0, a10 = 0, a11 = 0;
     for (int j = 0; j < cnt; ++j) {
-      const float4 v = __ldg(sbuf + __ldg(slots + ds.z + j));
-      a00 += v.x;
-      a01 += v.y;
-      a10 += v.z;
-      a11 += v.w;
+      const long long sl = __ldg(slots + ds.z + j);
+      if constexpr (sizeof(SB) == 4) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(sbuf) + sl);
+        a00 += v.x;
+        a01 += v.y;
+        a10 += v.z;
+        a11 += v.w;
+      } else {
+        const double2 v0 = __ldg(reinterpret_cast<const double2*>(sbuf) + 2 * sl);
+        const double2 v1 = __ldg(reinterpret_cast<const double2*>(sbuf) + 2 * sl + 1);
+        a00 += v0.x;
+        a01 += v0.y;
+        a10 += v1.x;
+        a11 += v1.y;
+      }
     }
-    const float r0[2] = {a00, a01}, r1[2] = {a10, a11};
+    const SB r0[2] = {a00, a01}, r1[2] = {a10, a11};
     int k = 0;
 #pragma unroll
     for (int d = 0; d < 2; ++d)

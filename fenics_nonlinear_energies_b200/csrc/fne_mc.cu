@@ -943,6 +943,331 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 P2 / P4: the same contraction K[(a,b),(c,d,e)] = P[(a,b),(q,k,l)] ·
+// Ã[(q,k,l),(c,d,e)] as the tensor-core kernel, in FP64 on the DMMA units
+// (mma.sync m16n8k4 f64) with the direct-write epilogue straight from the
+// accumulator registers.  One MMA K step of 4 is one quadrature point, and
+// P[(a,b),(q,k,l)] = R_qak R_qbl, so the A fragments are formed from the
+// reference gradient tables in registers (no P in shared memory).  Each
+// tile of TE elements: return map per (quadrature point, element) -> Ã and
+// the gradient helper in shared memory; warp task (16 node pairs,
+// 8 elements) runs NQ MMA steps of four n8 tiles (one per (c, d) component)
+// and writes its blocks; the element gradient follows on the CUDA cores.
+// Two CTAs per SM, so one CTA's return map overlaps the other's MMAs.
+// ---------------------------------------------------------------------------
+template <int NP, int NQ>
+struct McTileD {
+  static constexpr int NPAIR = NP * (NP + 1) / 2;
+  static constexpr int MT = (NPAIR + 15) / 16;          // m16 tiles of node pairs
+  static constexpr int KK = 4 * NQ;                      // (q, k, l)
+  static constexpr int TE = 16;                          // elements per tile
+  static constexpr int N = 4 * TE;                       // column (c * 2 + d) * TE + e
+  static constexpr int NS = N + 4;                       // B row stride (doubles), = 4 (mod 16)
+  static constexpr int THREADS = 256;
+  static constexpr int MIN_BLOCKS = 2;
+  static constexpr int NWARPS = THREADS / 32;
+  static constexpr int NTASK = MT * 2;                   // (m16 tile, element half)
+  static constexpr int R16(int b) { return (b + 15) / 16 * 16; }
+  static constexpr int OFF_B = 0;
+  static constexpr int OFF_S = OFF_B + R16(KK * NS * 8);             // [NQ][TE] 4 doubles
+  static constexpr int OFF_R = OFF_S + NQ * TE * 32;                 // dh1, dh2 [NQ * NP], qw [NQ]
+  static constexpr int OFF_U = OFF_R + R16((2 * NQ * NP + NQ) * 8);  // [TE][2 NP]
+  static constexpr int OFF_G = OFF_U + R16(TE * 2 * NP * 8);         // [TE][5]
+  static constexpr int OFF_PLAN = OFF_G + R16(TE * 5 * 8);           // [TE][NP * NP] uint16 codes
+  static constexpr int PLAN_WORDS = (TE * NP * NP + 1) / 2;
+  static constexpr int OFF_ROW = OFF_PLAN + R16(PLAN_WORDS * 4);     // [TE][NP][2] row starts
+  static constexpr int OFF_SB = OFF_ROW + R16(TE * NP * 2 * 4);      // [TE] shared-slot bases
+  static constexpr int SMEM = OFF_SB + R16(TE * 4);
+};
+
+struct McDmArgs {
+  const uint16_t* code;
+  const int* sbase;
+  const int* elem_rn;
+  const int* rn_row;
+  double* sbuf;      // shared-block buffer, 4 doubles per slot
+};
+
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, {%0, %1, %2, %3};\n"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a0), "d"(a1), "d"(b0));
+}
+
+template <int NP, int NQ, int WANT>
+__global__ void __launch_bounds__(McTileD<NP, NQ>::THREADS, McTileD<NP, NQ>::MIN_BLOCKS)
+    k_mc_dmma(McArgs A, McConstR<double> C, McDmArgs T, double* __restrict__ hout, double* __restrict__ gbuf,
+              double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ eout) {
+  using G = McTileD<NP, NQ>;
+  constexpr int N2 = 2 * NP, TE = G::TE, NS = G::NS, NPAIR = G::NPAIR, NT = G::THREADS;
+  constexpr int NN = NP * NP;
+  constexpr int UPT = (TE * N2 + NT - 1) / NT;
+  constexpr int GPT = (TE * 5 + NT - 1) / NT;
+  constexpr int RPT = (TE * NP + NT - 1) / NT;
+  constexpr int WPT = (G::PLAN_WORDS + NT - 1) / NT;
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* sB = reinterpret_cast<double*>(smem + G::OFF_B);
+  double2* sS = reinterpret_cast<double2*>(smem + G::OFF_S);  // [NQ][TE] x 2 double2
+  double* sD1 = reinterpret_cast<double*>(smem + G::OFF_R);
+  double* sD2 = sD1 + NQ * NP;
+  double* sW = sD2 + NQ * NP;
+  double* sU = reinterpret_cast<double*>(smem + G::OFF_U);
+  double* sGm = reinterpret_cast<double*>(smem + G::OFF_G);
+  uint32_t* sPlanW = reinterpret_cast<uint32_t*>(smem + G::OFF_PLAN);
+  const uint16_t* sPlan = reinterpret_cast<const uint16_t*>(smem + G::OFF_PLAN);
+  int* sRow = reinterpret_cast<int*>(smem + G::OFF_ROW);
+  int* sSb = reinterpret_cast<int*>(smem + G::OFF_SB);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gq = lane >> 2, tq = lane & 3;  // MMA fragment group / thread in group
+
+  for (int i = tid; i < NQ * NP; i += NT) {
+    sD1[i] = A.dhat1[i];
+    sD2[i] = A.dhat2[i];
+  }
+  for (int i = tid; i < NQ; i += NT) sW[i] = A.qw[i];
+  const int n_tiles = (A.n_el + TE - 1) / TE;
+
+  int cv[UPT], rnv[RPT], rsv[RPT][2], sbv = 0;
+  uint32_t pw[WPT];
+  double uv[UPT], gv[GPT];
+  auto fetch_codes = [&](int tile) {
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+      const int i = tid + k * NT, el = i / N2;
+      const int e = tile * TE + el;
+      cv[k] = (tile < n_tiles && i < TE * N2 && e < A.n_el) ? __ldg(A.codes + (long long)e * N2 + (i - el * N2))
+                                                             : INT_MIN;
+    }
+#pragma unroll
+    for (int k = 0; k < GPT; ++k) {
+      const int i = tid + k * NT, el = i / 5;
+      const int e = tile * TE + el;
+      gv[k] = (tile < n_tiles && i < TE * 5 && e < A.n_el) ? __ldg(A.geom + (long long)tile * TE * 5 + i) : 0.0;
+    }
+    const int ne_t = tile < n_tiles ? min(TE, A.n_el - tile * TE) : 0;
+    const int nw = (ne_t * NN + 1) / 2;
+    const uint32_t* cw = reinterpret_cast<const uint32_t*>(T.code) + (long long)tile * TE * NN / 2;
+#pragma unroll
+    for (int k = 0; k < WPT; ++k) {
+      const int i = tid + k * NT;
+      pw[k] = i < nw ? __ldg(cw + i) : 0xFFFFFFFFu;
+    }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const int i = tid + k * NT;
+      rnv[k] = i < ne_t * NP ? __ldg(T.elem_rn + (long long)tile * TE * NP + i) : -1;
+    }
+    sbv = tid < ne_t ? __ldg(T.sbase + (long long)tile * TE + tid) : 0;
+  };
+  auto fetch_values = [&]() {
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+      const int c = cv[k];
+      uv[k] = c == INT_MIN ? 0.0 : (c >= 0 ? __ldg(A.u + c) : __ldg(A.dir + (-1 - c)));
+    }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const int rn = rnv[k];
+      rsv[k][0] = rn >= 0 ? __ldg(T.rn_row + 2LL * rn) : -1;
+      rsv[k][1] = rn >= 0 ? __ldg(T.rn_row + 2LL * rn + 1) : -1;
+    }
+  };
+  auto stash = [&]() {
+#pragma unroll
+    for (int k = 0; k < UPT; ++k)
+      if (tid + k * NT < TE * N2) sU[tid + k * NT] = uv[k];
+#pragma unroll
+    for (int k = 0; k < GPT; ++k)
+      if (tid + k * NT < TE * 5) sGm[tid + k * NT] = gv[k];
+#pragma unroll
+    for (int k = 0; k < WPT; ++k)
+      if (tid + k * NT < G::PLAN_WORDS) sPlanW[tid + k * NT] = pw[k];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k)
+      if (tid + k * NT < TE * NP) {
+        sRow[2 * (tid + k * NT)] = rsv[k][0];
+        sRow[2 * (tid + k * NT) + 1] = rsv[k][1];
+      }
+    if (tid < TE) sSb[tid] = sbv;
+  };
+  // one directed block (ra -> cb) of element el: into the COO rows or the
+  // shared-block buffer
+  auto put = [&](int el, int ra, int cb, double w00, double w01, double w10, double w11) {
+    const unsigned code = sPlan[el * NN + ra * NP + cb];
+    if (code == 0xFFFFu) return;
+    if (code & 0x8000u) {
+      double2* sb = reinterpret_cast<double2*>(T.sbuf) + 2 * ((long long)sSb[el] + (code & 0x7FFFu));
+      sb[0] = make_double2(w00, w01);
+      sb[1] = make_double2(w10, w11);
+      return;
+    }
+    const int off = (int)(code & 0xFFFu);
+    const unsigned dm = (code >> 12) & 3u;
+    const double w[2][2] = {{w00, w01}, {w10, w11}};
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int rs = sRow[(el * NP + ra) * 2 + c];
+      if (rs < 0) continue;
+      int k = 0;
+#pragma unroll
+      for (int d = 0; d < 2; ++d)
+        if ((dm >> d) & 1u) hout[rs + off + k++] = w[c][d];
+    }
+  };
+
+  double eacc = 0.0;
+  fetch_codes(blockIdx.x);
+  fetch_values();
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int e0 = tile * TE;
+    const int ne = min(TE, A.n_el - e0);
+    stash();
+    __syncthreads();
+    // (1) constitutive update per (quadrature point, element) -> Ã (rows
+    // q * 4 + k * 2 + l, columns (c * 2 + d) * TE + el) and the gradient helper
+    for (int p = tid; p < TE * NQ; p += NT) {
+      const int q = p / TE, el = p - q * TE;
+      double at[4][4];
+      double2 s01 = make_double2(0.0, 0.0), s23 = make_double2(0.0, 0.0);
+      if (el < ne) {
+        const double* gm = sGm + el * 5;
+        const double i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
+        const double* ue = sU + el * N2;
+        double ex = 0.0, ey = 0.0, exy = 0.0;
+#pragma unroll 5
+        for (int a = 0; a < NP; ++a) {
+          const double r1 = sD1[q * NP + a], r2 = sD2[q * NP + a];
+          const double px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
+          const double ux = ue[2 * a], uy = ue[2 * a + 1];
+          ex += px * ux;
+          ey += py * uy;
+          exy += py * ux + px * uy;
+        }
+        double eps[3] = {ex, ey, exy};
+        if (A.epsp) {
+          const double* ep = A.epsp + ((long long)(e0 + el) * NQ + q) * 3;
+          eps[0] -= ep[0];
+          eps[1] -= ep[1];
+          eps[2] -= ep[2];
+        }
+        double sig[3], Ct[6], psi;
+        mc_point(C, eps, sig, Ct, psi);
+        const double w = gm[4] * sW[q];
+        if ((WANT & MW_E) && A.wflag[e0 + el]) eacc += w * psi;
+        const double Cf[3][3] = {{Ct[0], Ct[1], Ct[2]}, {Ct[1], Ct[3], Ct[4]}, {Ct[2], Ct[4], Ct[5]}};
+        const int vci[2][2] = {{0, 2}, {2, 1}};
+        const double Mx[2][2] = {{i00, i01}, {i10, i11}};
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll
+          for (int d = 0; d < 2; ++d) {
+            double Acd[2][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+              for (int j = 0; j < 2; ++j) Acd[i][j] = w * Cf[vci[c][i]][vci[d][j]];
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+#pragma unroll
+              for (int l = 0; l < 2; ++l)
+                at[c * 2 + d][k * 2 + l] = Mx[0][k] * (Acd[0][0] * Mx[0][l] + Acd[0][1] * Mx[1][l]) +
+                                           Mx[1][k] * (Acd[1][0] * Mx[0][l] + Acd[1][1] * Mx[1][l]);
+          }
+        }
+        s01 = make_double2(w * (Mx[0][0] * sig[0] + Mx[1][0] * sig[2]), w * (Mx[0][1] * sig[0] + Mx[1][1] * sig[2]));
+        s23 = make_double2(w * (Mx[0][0] * sig[2] + Mx[1][0] * sig[1]), w * (Mx[0][1] * sig[2] + Mx[1][1] * sig[1]));
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int kl = 0; kl < 4; ++kl) at[j][kl] = 0.0;
+      }
+      sS[2 * (q * TE + el)] = s01;
+      sS[2 * (q * TE + el) + 1] = s23;
+#pragma unroll
+      for (int kl = 0; kl < 4; ++kl)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) sB[(q * 4 + kl) * NS + j * TE + el] = at[j][kl];
+    }
+    __syncthreads();
+    // next tile's gather codes and geometry in flight during the MMAs
+    fetch_codes(tile + gridDim.x);
+    // (2) warp task (16 node pairs, 8 elements): NQ steps of four m16n8k4
+    // MMAs (one n8 tile per (c, d) component), then the blocks from registers
+    for (int task = warp; task < G::NTASK; task += G::NWARPS) {
+      const int mt = task >> 1, hf = task & 1;
+      // node pairs of this lane's fragment rows (pairs beyond NPAIR compute
+      // with pair 0 and are not stored)
+      int pa_[2], pb_[2];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int m = mt * 16 + gq + 8 * r;
+        int a = 0, b = m < NPAIR ? m : 0;
+        while (a < NP && b >= NP - a) {
+          b -= NP - a;
+          ++a;
+        }
+        pa_[r] = a;
+        pb_[r] = a + b;
+      }
+      // A fragment (row m, column q * 4 + tq): R_q[pa][k] * R_q[pb][l], k = tq / 2, l = tq % 2
+      const double* ra0 = ((tq >> 1) ? sD2 : sD1) + pa_[0];
+      const double* rb0 = ((tq & 1) ? sD2 : sD1) + pb_[0];
+      const double* ra1 = ((tq >> 1) ? sD2 : sD1) + pa_[1];
+      const double* rb1 = ((tq & 1) ? sD2 : sD1) + pb_[1];
+      double acc[4][4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[j][r] = 0.0;
+      const double* pb = sB + tq * NS + hf * 8 + gq;
+#pragma unroll 5
+      for (int q = 0; q < NQ; ++q) {
+        const double a0 = ra0[q * NP] * rb0[q * NP], a1 = ra1[q * NP] * rb1[q * NP];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_16x8x4(acc[j], a0, a1, pb[q * 4 * NS + j * TE]);
+      }
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int m = mt * 16 + gq + 8 * r;
+        if (m >= NPAIR) continue;
+#pragma unroll
+        for (int x = 0; x < 2; ++x) {
+          const int el = hf * 8 + 2 * tq + x;
+          if (el >= ne) continue;
+          const double v0 = acc[0][2 * r + x], v1 = acc[1][2 * r + x];
+          const double v2 = acc[2][2 * r + x], v3 = acc[3][2 * r + x];
+          put(el, pa_[r], pb_[r], v0, v1, v2, v3);                      // K[(a,c),(b,d)], (c,d) row-major
+          if (pa_[r] != pb_[r]) put(el, pb_[r], pa_[r], v0, v2, v1, v3);  // transposed block (b, a)
+        }
+      }
+    }
+    // (3) element gradient
+    if (WANT & MW_G) {
+      for (int i = tid; i < TE * N2; i += NT) {
+        const int el = i / N2, r = i - el * N2, a = r >> 1, c = r & 1;
+        if (el >= ne) continue;
+        double acc = 0.0;
+#pragma unroll 5
+        for (int q = 0; q < NQ; ++q) {
+          const double2 s = sS[2 * (q * TE + el) + c];
+          acc += sD1[q * NP + a] * s.x + sD2[q * NP + a] * s.y;
+        }
+        gbuf[(long long)(e0 + el) * N2 + r] = acc;
+      }
+    }
+    fetch_values();
+    __syncthreads();
+  }
+  if (WANT & MW_E) {
+    if (A.rhs)
+      for (int i = blockIdx.x * NT + threadIdx.x; i < A.n_owned; i += gridDim.x * NT)
+        eacc -= A.rhs[i] * A.u[A.lo + i];
+    mc_energy_finalize(eacc, partials, counter, eout);
+  }
+}
+
 // COO values: position p sums its element-matrix entries in element order.
 template <typename Real, typename HOut>
 __global__ void k_mc_gather(int n, const int* __restrict__ ptr, const int* __restrict__ idx,
@@ -995,7 +1320,9 @@ struct McHandle {
   // fix-up plan over the shared blocks
   uint16_t* dp_code = nullptr;
   int *dp_sbase = nullptr, *dp_elem_rn = nullptr;
-  float* dp_sbuf = nullptr;
+  void* dp_sbuf = nullptr;  // 4 floats (tensor-core path) or 4 doubles (DMMA path) per slot
+  // FP64 DMMA path (P2 / P4)
+  int dm = 0, grid_dm = 1;
   int n_fix = 0;
   int *fx_con = nullptr, *fx_desc = nullptr;
   // matrix-free products: weighted tangents at the linearization point and
@@ -1030,11 +1357,15 @@ cudaError_t mc_gathers(McHandle* h, int flags, const Real* K, const Real* g, dou
     if (h->n_rnodes == 0) return cudaSuccess;
     HOut* H = static_cast<HOut*>(hess);
     if (flags & MW_H) {
-      if (h->tc) {  // direct-write epilogue: only the shared blocks remain
+      if (h->tc || h->dm) {  // direct-write epilogue: only the shared blocks remain
         if (h->n_fix > 0) {
           const int gf = std::max(1, std::min(h->num_sms * 16, (h->n_fix + 255) / 256));
-          k_fixup2<HOut><<<gf, 256, 0, st>>>(h->n_fix, reinterpret_cast<const int4*>(h->fx_desc), h->fx_con,
-                                             reinterpret_cast<const float4*>(h->dp_sbuf), H);
+          if (h->dm)
+            k_fixup2<HOut, double><<<gf, 256, 0, st>>>(h->n_fix, reinterpret_cast<const int4*>(h->fx_desc),
+                                                       h->fx_con, static_cast<const double*>(h->dp_sbuf), H);
+          else
+            k_fixup2<HOut, float><<<gf, 256, 0, st>>>(h->n_fix, reinterpret_cast<const int4*>(h->fx_desc),
+                                                      h->fx_con, static_cast<const float*>(h->dp_sbuf), H);
         }
       } else {
         NodeGatherArgs G{h->n_rnodes, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
@@ -1082,7 +1413,8 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
   if constexpr (sizeof(Real) == 4 && NP > 3) {
     if (h->tc && (flags & MW_H)) {
       using G = McTile<NP, NQ>;
-      McTcArgs T{h->Phi, h->Plo, h->err, h->dp_code, h->dp_sbase, h->dp_elem_rn, h->bp_rn_row, h->dp_sbuf};
+      McTcArgs T{h->Phi, h->Plo, h->err, h->dp_code, h->dp_sbase, h->dp_elem_rn, h->bp_rn_row,
+                 static_cast<float*>(h->dp_sbuf)};
       float* g = static_cast<float*>(h->gbuf);
       HOut* H = static_cast<HOut*>(hess);
       const McConstR<float> Mf = cast_const<float>(h->mc);
@@ -1093,6 +1425,22 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
         default: k_mc_tc<NP, NQ, 7, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
       }
       return mc_gathers<float, HOut, NP>(h, flags, static_cast<const float*>(nullptr), g, grad, hess, st);
+    }
+  }
+  if constexpr (sizeof(Real) == 8 && NP > 3) {
+    if (h->dm && (flags & MW_H)) {
+      using G = McTileD<NP, NQ>;
+      McDmArgs T{h->dp_code, h->dp_sbase, h->dp_elem_rn, h->bp_rn_row, static_cast<double*>(h->dp_sbuf)};
+      double* g = static_cast<double*>(h->gbuf);
+      double* H = static_cast<double*>(hess);
+      const McConstR<double> Md = cast_const<double>(h->mc);
+      switch (flags) {
+        case 4: k_mc_dmma<NP, NQ, 4><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
+        case 5: k_mc_dmma<NP, NQ, 5><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
+        case 6: k_mc_dmma<NP, NQ, 6><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
+        default: k_mc_dmma<NP, NQ, 7><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
+      }
+      return mc_gathers<double, double, NP>(h, flags, static_cast<const double*>(nullptr), g, grad, hess, st);
     }
   }
   switch (flags) {
@@ -1164,6 +1512,25 @@ int mc_tc_prepare(McHandle* h, const double* tables, std::vector<float>& phi, st
                                     cudaGetErrorString(e));
   const int n_tiles = (h->n_local + G::TE - 1) / G::TE;
   h->grid_tc = std::max(1, std::min(n_tiles, h->num_sms * G::MIN_BLOCKS));
+  return FNE_OK;
+}
+
+// FP64 DMMA kernel: grid (two CTAs per SM) and the shared-memory opt-in.
+template <int NP, int NQ>
+int mc_dm_prepare(McHandle* h) {
+  using G = McTileD<NP, NQ>;
+  cudaError_t e = cudaSuccess;
+  auto opt_in = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+  };
+  opt_in((const void*)k_mc_dmma<NP, NQ, 4>);
+  opt_in((const void*)k_mc_dmma<NP, NQ, 5>);
+  opt_in((const void*)k_mc_dmma<NP, NQ, 6>);
+  opt_in((const void*)k_mc_dmma<NP, NQ, 7>);
+  if (e != cudaSuccess)
+    return set_error(FNE_ECUDA, std::string("Mohr-Coulomb: FP64 DMMA kernel shared memory: ") + cudaGetErrorString(e));
+  const int n_tiles = (h->n_local + G::TE - 1) / G::TE;
+  h->grid_dm = std::max(1, std::min({n_tiles, h->num_sms * G::MIN_BLOCKS, h->n_partials}));
   return FNE_OK;
 }
 
@@ -1389,27 +1756,41 @@ int mc_create(const fne_desc* d, McHandle** out) {
   // tensor-core path: FP32 P2 / P4 on a node-blocked pattern unless CUDA
   // cores are requested; its epilogue writes the COO values directly
   h->tc = d->precision == FNE_FP32 && np > 3 && d->kernel_variant != 1 && use_blk;
+  // FP64 DMMA path: FP64 P2 / P4 on a node-blocked pattern, same epilogue
+  h->dm = d->precision == FNE_FP64 && np > 3 && d->kernel_variant != 1 && use_blk;
   DirectPlan dp;
-  if (h->tc && build_direct_plan(bp, nl, np, 2, dp) != FNE_OK) h->tc = 0;
+  if ((h->tc || h->dm) && build_direct_plan(bp, nl, np, 2, dp) != FNE_OK) h->tc = h->dm = 0;
   {
     unsigned char* kb = nullptr;
-    if (!h->tc) MC_TRY(mc_upload(h, &kb, (const unsigned char*)nullptr, (size_t)nl * npair * 4 * rsz));
+    if (!h->tc && !h->dm) MC_TRY(mc_upload(h, &kb, (const unsigned char*)nullptr, (size_t)nl * npair * 4 * rsz));
     h->Kbuf = kb;
     unsigned char* gb = nullptr;
     MC_TRY(mc_upload(h, &gb, (const unsigned char*)nullptr, (size_t)nl * n * rsz));
     h->gbuf = gb;
   }
   h->n_contrib = use_blk ? (int64_t)bp.con.size() : (int64_t)hptr[d->nnz];
-  if (h->tc) {
-    dp.code.push_back(0xFFFF);  // the kernel reads codes in 32-bit words
+  if (h->tc || h->dm) {
+    dp.code.push_back(0xFFFF);  // the kernels read codes in 32-bit words
     dp.code.push_back(0xFFFF);
     MC_TRY(mc_upload(h, &h->dp_code, dp.code.data(), dp.code.size()));
     MC_TRY(mc_upload(h, &h->dp_sbase, dp.sbase.data(), dp.sbase.size()));
     MC_TRY(mc_upload(h, &h->dp_elem_rn, bp.elem_rn.data(), bp.elem_rn.size()));
-    MC_TRY(mc_upload(h, &h->dp_sbuf, (const float*)nullptr, (size_t)std::max<int64_t>(1, dp.n_slots) * 4));
+    unsigned char* sb = nullptr;
+    MC_TRY(mc_upload(h, &sb, (const unsigned char*)nullptr,
+                     (size_t)std::max<int64_t>(1, dp.n_slots) * 4 * (h->dm ? sizeof(double) : sizeof(float))));
+    h->dp_sbuf = sb;
     h->n_fix = (int)(dp.fdesc.size() / 4);
     MC_TRY(mc_upload(h, &h->fx_con, dp.fix.con.data(), dp.fix.con.size()));
     MC_TRY(mc_upload(h, &h->fx_desc, dp.fdesc.data(), dp.fdesc.size()));
+  }
+  if (h->dm) {
+    const int rc_dm = np == 15 ? mc_dm_prepare<15, 25>(h) : mc_dm_prepare<6, 7>(h);
+    if (rc_dm) {
+      mc_destroy(h);
+      return rc_dm;
+    }
+  }
+  if (h->tc) {
     std::vector<float> phi, plo;
     int rc_tc = np == 15 ? mc_tc_prepare<15, 25>(h, d->e3, phi, plo) : mc_tc_prepare<6, 7>(h, d->e3, phi, plo);
     if (rc_tc) {
@@ -1546,7 +1927,7 @@ void mc_info(const McHandle* h, fne_info* info) {
   info->n_incidences = h->n_contrib;
   info->device_bytes = h->device_bytes;
   info->max_row_len = 0;
-  info->kernel_variant = h->tc ? 6 : 5;
+  info->kernel_variant = h->tc ? 6 : h->dm ? 9 : 5;
 }
 
 }  // namespace fne

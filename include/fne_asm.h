@@ -166,8 +166,9 @@ typedef struct {
                                  * (push; not bit-reproducible).
                                  * P1 tets: 0/1 = row-gather; 2 = element-
                                  * parallel pass + node-block gather.
-                                 * Mohr-Coulomb: 0 = automatic (tensor cores for
-                                 * FP32 P2/P4, CUDA cores otherwise);
+                                 * Mohr-Coulomb: 0 = automatic (tcgen05 tensor
+                                 * cores for FP32 P2/P4, FP64 DMMA tensor cores
+                                 * for FP64 P2/P4, CUDA cores for P1);
                                  * 1 = CUDA cores only.                        */
 } fne_desc;
 
@@ -184,7 +185,8 @@ typedef struct {
                            * 3 incidence-parallel, 4 banded sweep,
                            * 5 Mohr-Coulomb CUDA cores, 6 Mohr-Coulomb tcgen05,
                            * 7 element-parallel tets + node-block gather,
-                           * 8 banded sweep, push variant */
+                           * 8 banded sweep, push variant,
+                           * 9 Mohr-Coulomb FP64 DMMA (mma.sync f64) */
 } fne_info;
 
 int fne_create(const fne_desc* desc, fne_handle** out);

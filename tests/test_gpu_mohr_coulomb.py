@@ -42,18 +42,52 @@ def _abs_scale(ref, u):
     return float(np.abs(e).sum() + abs(ref.f_owned @ np.asarray(u)[: ref.f_owned.size]))
 
 
+@pytest.mark.parametrize("variant", ["auto", "cuda_cores"])
 @pytest.mark.parametrize("degree,level", [(2, 1), (4, 1), (2, 2)])
 @pytest.mark.parametrize("scale", [0.0, 0.05])
-def test_mc_fp64_matches_oracle(degree, level, scale):
+def test_mc_fp64_matches_oracle(degree, level, scale, variant):
+    """FP64 P2 / P4: the DMMA tensor-core kernel (automatic) and the CUDA-core
+    kernel, both at the FP64 bar."""
     params = meshes.slope_problem(level=level, degree=degree, lam=1.2, with_elem_B=True)
-    gpu, ref = _pair(params)
+    gpu, ref = _pair(params, kernel_variant=variant)
     u = scale * np.random.default_rng(degree + level).standard_normal(gpu.layout.n_free)
     e_ref, g_ref, h_ref = ref.all_in_one(u)
     e, g, h = gpu.eval(torch.as_tensor(u, device="cuda"), 7)
     assert abs(float(e.item()) - e_ref) <= 1e-12 * max(_abs_scale(ref, u), 1.0)
     assert _rel(g.cpu().numpy(), g_ref) <= 1e-12
     assert _rel(h.cpu().numpy(), h_ref) <= 1e-12
-    assert gpu.info["kernel_variant"] == 5
+    assert gpu.info["kernel_variant"] == (9 if variant == "auto" else 5)
+
+
+@pytest.mark.parametrize("degree", [2, 4])
+def test_mc_fp64_dmma_path(degree):
+    """The FP64 DMMA kernel against the FP64 CUDA-core kernel (same
+    arithmetic up to summation order), bit-repeatable, with every flag
+    combination (energy / gradient passes of the automatic path agree)."""
+    params = meshes.slope_problem(level=2, degree=degree, lam=1.2, with_elem_B=True)
+    gpu, ref = _pair(params)
+    cc, _ = _pair(params, kernel_variant="cuda_cores")
+    assert gpu.info["kernel_variant"] == 9 and cc.info["kernel_variant"] == 5
+    u = 0.05 * np.random.default_rng(13).standard_normal(gpu.layout.n_free)
+    ut = torch.as_tensor(u, device="cuda")
+    e, g, h = [t.clone() for t in gpu.eval(ut, 7)]
+    ec, gc, hc = [t.clone() for t in cc.eval(ut, 7)]
+    assert _rel(h.cpu().numpy(), hc.cpu().numpy()) <= 1e-13
+    assert _rel(g.cpu().numpy(), gc.cpu().numpy()) <= 1e-13
+    assert abs(float(e.item()) - float(ec.item())) <= 1e-13 * _abs_scale(ref, u)
+    e2, g2, h2 = gpu.eval(ut, 7)
+    assert torch.equal(h, h2) and torch.equal(g, g2) and torch.equal(e, e2)
+    # other flag sets are other template instances (the compiler may contract
+    # multiply-adds differently): agreement to rounding
+    for flags in (_lib.FNE_HESS, _lib.FNE_HESS | _lib.FNE_ENERGY, _lib.FNE_HESS | _lib.FNE_GRAD):
+        ef, gf, hf = gpu.eval(ut, flags)
+        assert _rel(hf.cpu().numpy(), h.cpu().numpy()) <= 1e-14
+        if flags & _lib.FNE_GRAD:
+            assert _rel(gf.cpu().numpy(), g.cpu().numpy()) <= 1e-14
+        if flags & _lib.FNE_ENERGY:
+            assert abs(float(ef.item()) - float(e.item())) <= 1e-14 * _abs_scale(ref, u)
+    assert abs(float(gpu.eval(ut, _lib.FNE_ENERGY)[0].item()) - float(e.item())) <= 1e-13 * _abs_scale(ref, u)
+    assert _rel(gpu.eval(ut, _lib.FNE_GRAD)[1].cpu().numpy(), g.cpu().numpy()) <= 1e-13
 
 
 def test_mc_plastic_points_present():
@@ -216,7 +250,7 @@ def test_mc_nonzero_previous_plastic_strain(degree, precision):
     params["eps_p_old"] = 2e-4 * rng.standard_normal(params["eps_p_old"].shape)
     hd = torch.float32 if precision == "fp32" else torch.float64
     gpu, ref = _pair(params, precision=precision, hess_dtype=hd)
-    assert gpu.info["kernel_variant"] == (6 if precision == "fp32" else 5)
+    assert gpu.info["kernel_variant"] == (6 if precision == "fp32" else 9)
     u = 0.03 * rng.standard_normal(gpu.layout.n_free)
     e_ref, g_ref, h_ref = ref.all_in_one(u)
     ut = torch.as_tensor(u, device="cuda")
