@@ -176,8 +176,9 @@ class Workload:
     """
 
     def __init__(self, name, family, precision, hess_fp32, conn_nodes, geom_values, geom_bytes, has_rhs, desc,
-                 build, sample, op="egh"):
+                 build, sample, op="egh", newton_kw=None):
         self.op = op  # "egh": fused E+grad+Hess pass; "hvp": matrix-free H(u) x; "newton": one Newton solve
+        self.newton_kw = dict(newton_kw or {})  # Newton settings of the "newton" workloads
         self.name, self.family, self.precision, self.hess_fp32 = name, family, precision, hess_fp32
         self.conn_nodes, self.geom_values, self.geom_bytes, self.has_rhs = conn_nodes, geom_values, geom_bytes, has_rhs
         self.desc, self.build, self.sample = desc, build, sample
@@ -279,6 +280,42 @@ def _he(nx, ny, nz, precision, theta=4.0 * 3.141592653589793 / 24.0):
     return build, sample
 
 
+def _he_newton(nx, ny, nz, precision, theta=4.0 * 3.141592653589793 / 24.0):
+    """First load step of the twisted beam: Dirichlet right face rotated by
+    ``theta``, Newton from the reference configuration."""
+
+    def rotated(params):
+        from fenics_nonlinear_energies_b200 import meshes
+
+        return meshes.rotate_right_face_from_reference(params["u_0_ref"], params["nodes2coord"], theta,
+                                                       params["right_nodes"])
+
+    def build(rank):
+        import torch
+
+        from fenics_nonlinear_energies_b200 import meshes
+        from fenics_nonlinear_energies_b200.assembler import HECudaAssembler
+
+        params, _ = meshes.he_beam_problem(nx=nx, ny=ny, nz=nz)
+        hd = torch.float32 if precision == "fp32" else torch.float64
+        asm = HECudaAssembler(params, precision=precision, hess_dtype=hd, kernel_variant=KERNEL_VARIANT["value"])
+        rot = rotated(params)
+        asm.update_dirichlet(rot)
+        return asm, _reordered(asm, rot[params["freedofs"]])
+
+    def sample():
+        from fenics_nonlinear_energies_b200 import meshes
+
+        sx = max(1, nx // 8)
+        params, _ = meshes.he_beam_problem(nx=sx, ny=ny, nz=nz)
+        rot = rotated(params)
+        params = dict(params, u_0_ref=rot)
+        return "he", {"block_size": 3, "coordinate_key": "nodes2coord", "dirichlet_key": "u_0_ref"}, params, \
+            rot[params["freedofs"]], 6 * sx * ny * nz, f"{sx}x{ny}x{nz}-hex beam"
+
+    return build, sample
+
+
 def _mc(degree, h, precision):
     def build(rank):
         import torch
@@ -363,6 +400,12 @@ WORKLOADS = {
         "Newton to ||g|| <= 1e-6 ||g_0||: Ginzburg-Landau eps=0.01, 1024x1024 P1 triangles (2,097,152 "
         "elements), u ~ U[-0.5,0.5] seeded; Jacobi CG rtol 1e-3, golden-section line search on [-0.5, 2], FP64",
         *_tri("gl", 1024, "fp64", sample_n=96), op="newton"),
+    "he160x8x8_newton_fp64": Workload(
+        "he160x8x8_newton_fp64", "he", "fp64", False, 4, 13, 8, False,
+        "Newton to ||g|| <= 1e-6 ||g_0||: Neo-Hookean beam 160x8x8 hexes x 6 tets (61,440), E=10, nu=0.3, "
+        "first load step (right face rotated by 4pi/24) from the reference configuration; Jacobi CG rtol 1e-2, "
+        "golden-section line search on [-0.5, 2], FP64", *_he_newton(160, 8, 8, "fp64"), op="newton",
+        newton_kw={"ksp_rtol": 1e-2, "ksp_max_it": 2000, "maxit": 200}),
     "gl1024_newton_fp32h": Workload(
         "gl1024_newton_fp32h", "gl", "fp32", True, 3, 7, 4, False,
         "Newton to ||g|| <= 1e-6 ||g_0||: Ginzburg-Landau 1024x1024 as gl1024_newton_fp64 with FP32 element "
@@ -451,7 +494,7 @@ def run_reference(args):
         from oracle.newton_cpu import newton_cpu
 
         def step():
-            return newton_cpu(asm, u, tolg_rel=1e-6)
+            return newton_cpu(asm, u, tolg_rel=1e-6, **w.newton_kw)
     else:
         def step():
             return asm.all_in_one(u)
@@ -603,7 +646,7 @@ def cpu_newton_baseline(w):
     u = np.asarray(u)[np.asarray(asm.layout.perm)]
     times = []
     while len(times) < 5 and sum(times) < 8.0:  # repeated solves of the same start: at least ~8 s of work
-        x, info = newton_cpu(asm, u, tolg_rel=1e-6)
+        x, info = newton_cpu(asm, u, tolg_rel=1e-6, **w.newton_kw)
         times.append(info["time_s"])
     return {"value": sum(times) / len(times), "unit": "s", "cores": int(torch.get_num_threads()), "kind": "port",
             "sample": f"{label} ({n_el} elements): Newton solve to 1e-6 relative gradient on the host "
@@ -629,7 +672,7 @@ def run_newton(args, w, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     cg = DeviceCG.for_assembler(asm)
     casm = _CountingAssembler(asm)
-    kw = dict(tolg_rel=1e-6, cg=cg)
+    kw = dict(tolg_rel=1e-6, cg=cg, **w.newton_kw)
     u = torch.as_tensor(u0, device=dev)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     for _ in range(args.warmup):
