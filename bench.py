@@ -893,7 +893,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel-variant", default="auto", choices=["auto", "row_gather", "incidence", "element", "cuda_cores", "push"])
+    ap.add_argument("--kernel-variant", default="auto", choices=["auto", "row_gather", "incidence", "element", "cuda_cores", "push",
+                                                                  "row_lanes_2", "row_lanes_4", "row_lanes_8"])
     args = ap.parse_args()
     KERNEL_VARIANT["value"] = args.kernel_variant
     if args.warmup < 3 and args.impl == "b200":

@@ -61,7 +61,7 @@ class Info(C.Structure):
     _fields_ = [
         ("n_rows", C.c_int64), ("nnz", C.c_int64), ("n_elem", C.c_int64),
         ("n_incidences", C.c_int64), ("device_bytes", C.c_int64),
-        ("max_row_len", C.c_int32), ("kernel_variant", C.c_int32),
+        ("max_row_len", C.c_int32), ("kernel_variant", C.c_int32), ("row_lanes", C.c_int32),
     ]
 
 

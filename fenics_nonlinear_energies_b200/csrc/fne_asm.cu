@@ -565,29 +565,37 @@ __global__ void __launch_bounds__(kTriRows) k_rows_tri(RowArgs A, const Chunk* _
   if (WANT & W_E) energy_finalize(eacc, eo);
 }
 
-template <typename Real, int WANT, typename HOut>
+template <typename Real, int WANT, typename HOut, int G>
 __global__ void __launch_bounds__(kTetRows) k_rows_tet(RowArgs A, const Chunk* __restrict__ R, Phys P,
                                                        double* __restrict__ grad, HOut* __restrict__ hess,
                                                        EnergyOut eo) {
+  // G lanes per output row (consecutive threads): lane s takes the row's
+  // incident elements s, s + G, ... into its own shared-memory slice of the
+  // CTA's rows; the slices are summed in lane order at the end and the
+  // gradient over the lanes by a fixed shuffle tree (deterministic).
+  constexpr int RP = kTetRows / G;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Real* sacc = reinterpret_cast<Real*>(smem_raw);
-  const int r0 = blockIdx.x * blockDim.x;
-  const int r = r0 + threadIdx.x;
-  const int rend = min(r0 + (int)blockDim.x, A.n_rows);
+  const int r0 = blockIdx.x * RP;
+  const int sub = threadIdx.x % G;
+  const int r = r0 + threadIdx.x / G;
+  const int rend = min(r0 + RP, A.n_rows);
   const int cs = A.row_ptr[r0];
   const int clen = A.row_ptr[rend] - cs;
+  Real* slice = sacc + sub * clen;
   if (WANT & W_H) {
-    for (int j = threadIdx.x; j < clen; j += blockDim.x) sacc[j] = Real(0);
+    for (int j = threadIdx.x; j < G * clen; j += blockDim.x) sacc[j] = Real(0);
     __syncthreads();
   }
   double eacc = 0.0;
+  Real g = Real(0);
+  int c = 0, gp = 0;
   if (r < A.n_rows) {
     const int node = A.row_node[r];
-    const int c = A.row_comp[r];
+    c = A.row_comp[r];
     const int base = A.row_ptr[r] - cs;
     const int ib = A.inc_ptr[node], ie = A.inc_ptr[node + 1];
-    Real g = Real(0);
-    for (int i = ib; i < ie; ++i) {
+    for (int i = ib + sub; i < ie; i += G) {
       const int el = __ldg(A.inc_elem + i);
       const unsigned info = __ldg(A.inc_info + i);
       TetElem<Real> t;
@@ -612,21 +620,30 @@ __global__ void __launch_bounds__(kTetRows) k_rows_tet(RowArgs A, const Chunk* _
         for (int b = 0; b < 4; ++b) {
           const unsigned off = (info >> (kOffShift + kOffBits * b)) & 127u;
           if (off != kNoCol) {
-            sacc[base + off] += h[b][0];
-            sacc[base + off + 1] += h[b][1];
-            sacc[base + off + 2] += h[b][2];
+            slice[base + off] += h[b][0];
+            slice[base + off + 1] += h[b][1];
+            slice[base + off + 2] += h[b][2];
           }
         }
       }
       if ((WANT & W_E) && c == 0 && (info & kEnergyFlag)) eacc += he_energy<Real>(P, yd, t);
     }
-    const int gp = A.row_gpos[r];
-    if (WANT & W_G) grad[gp] = (double)g - (A.rhs ? A.rhs[gp] : 0.0);
-    if ((WANT & W_E) && A.rhs) eacc -= A.rhs[gp] * A.u[A.lo + gp];
+    gp = A.row_gpos[r];
   }
+  if (WANT & W_G) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o, G);
+    if (r < A.n_rows && sub == 0) grad[gp] = (double)g - (A.rhs ? A.rhs[gp] : 0.0);
+  }
+  if ((WANT & W_E) && A.rhs && r < A.n_rows && sub == 0) eacc -= A.rhs[gp] * A.u[A.lo + gp];
   if (WANT & W_H) {
     __syncthreads();
-    for (int j = threadIdx.x; j < clen; j += blockDim.x) hess[cs + j] = (HOut)sacc[j];
+    for (int j = threadIdx.x; j < clen; j += blockDim.x) {
+      Real v = sacc[j];
+#pragma unroll
+      for (int s2 = 1; s2 < G; ++s2) v += sacc[s2 * clen + j];
+      hess[cs + j] = (HOut)v;
+    }
   }
   if (WANT & W_E) energy_finalize(eacc, eo);
 }
@@ -1349,6 +1366,7 @@ struct fne_handle {
   int family = 0, precision = 0, hess_fp32 = 0, npe = 0, bs = 0;
   int64_t n_total = 0, n_free = 0, lo = 0, hi = 0, nnz = 0;
   int n_rows = 0, n_local = 0, n_dir_only = 0, rows_per_cta = 0, grid_rows = 0;
+  int tet_lanes = 1;  // lanes per output row of the tet row kernel (1, 2, 4, 8)
   int64_t n_inc = 0;
   int max_row_len = 0;
   size_t smem_bytes = 0;
@@ -1553,8 +1571,8 @@ cudaError_t launch_tri_t(fne_handle* h, int want, const RowArgs& A, const IncArg
   return cudaErrorInvalidValue;
 }
 
-template <typename Real, typename HOut>
-cudaError_t launch_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
+template <typename Real, typename HOut, int G>
+cudaError_t launch_tet_g(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
                          cudaStream_t st, bool set_attr) {
   HOut* H = static_cast<HOut*>(hess);
   const dim3 grid(h->grid_rows), block(kTetRows);
@@ -1562,9 +1580,9 @@ cudaError_t launch_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad
 #define FNE_TET_CASE(W)                                                                                       \
   case W:                                                                                                     \
     if (set_attr)                                                                                             \
-      return cudaFuncSetAttribute(k_rows_tet<Real, W, HOut>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+      return cudaFuncSetAttribute(k_rows_tet<Real, W, HOut, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                   (int)h->smem_bytes);                                                        \
-    k_rows_tet<Real, W, HOut><<<grid, block, sm, st>>>(A, h->rec, h->phys, grad, H, eo);                       \
+    k_rows_tet<Real, W, HOut, G><<<grid, block, sm, st>>>(A, h->rec, h->phys, grad, H, eo);                    \
     return cudaGetLastError();
   switch (want) {
     FNE_TET_CASE(2)
@@ -1576,6 +1594,17 @@ cudaError_t launch_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad
   }
 #undef FNE_TET_CASE
   return cudaErrorInvalidValue;
+}
+
+template <typename Real, typename HOut>
+cudaError_t launch_tet_t(fne_handle* h, int want, const RowArgs& A, double* grad, void* hess, EnergyOut eo,
+                         cudaStream_t st, bool set_attr) {
+  switch (h->tet_lanes) {
+    case 2: return launch_tet_g<Real, HOut, 2>(h, want, A, grad, hess, eo, st, set_attr);
+    case 4: return launch_tet_g<Real, HOut, 4>(h, want, A, grad, hess, eo, st, set_attr);
+    case 8: return launch_tet_g<Real, HOut, 8>(h, want, A, grad, hess, eo, st, set_attr);
+    default: return launch_tet_g<Real, HOut, 1>(h, want, A, grad, hess, eo, st, set_attr);
+  }
 }
 
 template <typename Real, typename HOut>
@@ -1850,14 +1879,25 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     h->inc_max_len = inc.max_len;
     h->smem_bytes = (size_t)h->inc_max_rows * (sizeof(int) + real_size) + (size_t)inc.max_len * real_size;
   } else {
-    h->rows_per_cta = is_tri(d->family) ? kTriRows : kTetRows;
+    // tets: G lanes per row (kernel_variant 1 = one lane, 4 / 5 / 6 = 2 / 4 / 8
+    // lanes; automatic: the fewest lanes giving at least 1024 row lanes per SM)
+    h->tet_lanes = 1;
+    if (!is_tri(d->family)) {
+      if (d->kernel_variant >= 4 && d->kernel_variant <= 6) {
+        h->tet_lanes = 1 << (d->kernel_variant - 3);
+      } else if (d->kernel_variant != 1) {
+        while (h->tet_lanes < 8 && (int64_t)plan.n_rows * h->tet_lanes < (int64_t)h->num_sms * 1024)
+          h->tet_lanes *= 2;
+      }
+    }
+    h->rows_per_cta = is_tri(d->family) ? kTriRows : kTetRows / h->tet_lanes;
     h->grid_rows = (h->n_rows + h->rows_per_cta - 1) / h->rows_per_cta;
     int64_t max_cta = 0;
     for (int c = 0; c < h->grid_rows; ++c) {
       const int a = c * h->rows_per_cta, b = std::min(h->n_rows, a + h->rows_per_cta);
       max_cta = std::max<int64_t>(max_cta, plan.row_ptr[b] - plan.row_ptr[a]);
     }
-    h->smem_bytes = (size_t)max_cta * real_size;
+    h->smem_bytes = (size_t)max_cta * h->tet_lanes * real_size;
   }
   if (h->smem_bytes > 227 * 1024) {
     free_handle(h);
@@ -1994,6 +2034,7 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   info->kernel_variant = is_tri(h->family) ? (h->use_push ? 8 : (h->use_sweep ? 4 : (h->use_inc ? 3 : 1)))
                                            : (h->use_elem2 ? 7 : 2);
   if (h->use_elem2) info->n_incidences = h->e2_contrib;
+  info->row_lanes = h->tet_lanes;
   return FNE_OK;
 }
 

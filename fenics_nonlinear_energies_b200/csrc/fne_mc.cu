@@ -1928,6 +1928,7 @@ void mc_info(const McHandle* h, fne_info* info) {
   info->device_bytes = h->device_bytes;
   info->max_row_len = 0;
   info->kernel_variant = h->tc ? 6 : h->dm ? 9 : 5;
+  info->row_lanes = 1;
 }
 
 }  // namespace fne

@@ -164,8 +164,11 @@ typedef struct {
                                  * 1 = row-gather; 2 = incidence-parallel;
                                  * 3 = banded sweep with shared-memory atomics
                                  * (push; not bit-reproducible).
-                                 * P1 tets: 0/1 = row-gather; 2 = element-
-                                 * parallel pass + node-block gather.
+                                 * P1 tets: 0 = row-gather with automatic lanes
+                                 * per row; 1 = row-gather, one lane per row;
+                                 * 2 = element-parallel pass + node-block
+                                 * gather; 4 / 5 / 6 = row-gather with 2 / 4 / 8
+                                 * lanes per row.
                                  * Mohr-Coulomb: 0 = automatic (tcgen05 tensor
                                  * cores for FP32 P2/P4, FP64 DMMA tensor cores
                                  * for FP64 P2/P4, CUDA cores for P1);
@@ -187,6 +190,7 @@ typedef struct {
                            * 7 element-parallel tets + node-block gather,
                            * 8 banded sweep, push variant,
                            * 9 Mohr-Coulomb FP64 DMMA (mma.sync f64) */
+  int32_t row_lanes;      /* lanes per output row of the tet row kernel, else 1 */
 } fne_info;
 
 int fne_create(const fne_desc* desc, fne_handle** out);

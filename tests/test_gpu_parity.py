@@ -234,6 +234,34 @@ def test_he_element_pass_matches_row_gather(precision):
     assert torch.equal(a.eval(u, _lib.FNE_HESS)[2], ha)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("variant", ["row_gather", "row_lanes_2", "row_lanes_4", "row_lanes_8"])
+def test_he_row_lanes(variant, precision):
+    """The tet row kernel with 1, 2, 4 or 8 lanes per output row (each lane
+    its own shared-memory slice, summed in lane order) against the oracle,
+    bit-repeatable; the automatic choice gives a small beam several lanes."""
+    params, y0 = meshes.he_beam_problem(nx=10, ny=3, nz=3)
+    hd = torch.float32 if precision == "fp32" else torch.float64
+    gpu, ref = _make("he", params, precision=precision, hess_dtype=hd, kernel_variant=variant)
+    lanes = {"row_gather": 1, "row_lanes_2": 2, "row_lanes_4": 4, "row_lanes_8": 8}[variant]
+    assert gpu.info["kernel_variant"] == 2 and gpu.info["row_lanes"] == lanes
+    u = y0 + 1e-3 * np.random.default_rng(12).standard_normal(y0.size)
+    ut = torch.as_tensor(u, device="cuda")
+    if precision == "fp64":
+        _check(gpu, ref, u, FP64_TOL, energy_scale=_abs_energy_scale(ref, u))
+    else:
+        e_ref, g_ref, h_ref = ref.all_in_one(u)
+        e, g, h = gpu.eval(ut, 7)
+        assert abs(float(e.item()) - e_ref) <= 1e-6 * _abs_energy_scale(ref, u)
+        assert _rel(g.cpu().numpy(), g_ref) <= 1e-4
+        assert _rel(h.double().cpu().numpy(), h_ref) <= FP32_TOL
+    e1, g1, h1 = [t.clone() for t in gpu.eval(ut, 7)]
+    e2, g2, h2 = gpu.eval(ut, 7)
+    assert torch.equal(h1, h2) and torch.equal(g1, g2) and torch.equal(e1, e2)
+    auto, _ = _make("he", params, precision=precision, hess_dtype=hd)
+    assert auto.info["row_lanes"] == 8  # 1,000-odd rows: far below 1024 row lanes per SM
+
+
 @pytest.mark.parametrize("family", ["plaplace", "gl", "he", "mc"])
 @pytest.mark.parametrize("size", [2, 3])
 def test_rank_split_matches_oracle(family, size):
