@@ -1880,14 +1880,15 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     h->smem_bytes = (size_t)h->inc_max_rows * (sizeof(int) + real_size) + (size_t)inc.max_len * real_size;
   } else {
     // tets: G lanes per row (kernel_variant 1 = one lane, 4 / 5 / 6 = 2 / 4 / 8
-    // lanes; automatic: the fewest lanes giving at least 1024 row lanes per SM)
+    // lanes; automatic: the fewest lanes giving at least 1024 (FP64) or 512
+    // (FP32) row lanes per SM -- measured on the 61,440- and 491,520-tet beams)
     h->tet_lanes = 1;
     if (!is_tri(d->family)) {
       if (d->kernel_variant >= 4 && d->kernel_variant <= 6) {
         h->tet_lanes = 1 << (d->kernel_variant - 3);
       } else if (d->kernel_variant != 1) {
-        while (h->tet_lanes < 8 && (int64_t)plan.n_rows * h->tet_lanes < (int64_t)h->num_sms * 1024)
-          h->tet_lanes *= 2;
+        const int64_t want = (int64_t)h->num_sms * (f32 ? 512 : 1024);
+        while (h->tet_lanes < 8 && (int64_t)plan.n_rows * h->tet_lanes < want) h->tet_lanes *= 2;
       }
     }
     h->rows_per_cta = is_tri(d->family) ? kTriRows : kTetRows / h->tet_lanes;
