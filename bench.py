@@ -17,6 +17,10 @@ Hessian-vector product; and whole Newton solves (``*_newton_*``: metric
 "Newton s to 1e-6 rel-grad", lower is better; the roofline line is one
 device CG iteration on the Hessian at the solution, timed on its own).
 
+``--pass energy`` times the energy-only pass instead (the line-search
+callback, ``energy_fn``): algorithmic bytes are the connectivity, geometry
+and state reads only.
+
 ``value``: device-resident inputs, CUDA events around each pass, L2 flushed
 (1 GiB write) between passes outside the timed events; its length also keeps
 the GPU busy while the host enqueues the timed pass, so no launch gap
@@ -418,17 +422,23 @@ KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tr
                 6: "k_mc_tc+k_fixup2", 7: "k_he_elem+k_node_gather", 8: "k_push_tri", 9: "k_mc_dmma+k_fixup2"}
 
 
-def algorithmic_bytes(w, asm, n_el):
+def algorithmic_bytes(w, asm, n_el, energy_only=False):
     """Bytes one pass must move: node-level connectivity (int32), per-element
     geometry, the free state u (FP64), the load vector where the family has one,
-    the owned gradient write (FP64) and the owned COO value write."""
+    and -- unless energy only -- the owned gradient write (FP64) and the owned
+    COO value write."""
     n_free = asm.layout.n_free
     nnz = int(asm.owned_values.numel())
     hb = 4 if w.hess_fp32 else 8
-    b = n_el * (4 * w.conn_nodes + w.geom_bytes * w.geom_values) + n_free * 8 + asm.n_owned * 8 + nnz * hb
+    b = n_el * (4 * w.conn_nodes + w.geom_bytes * w.geom_values) + n_free * 8
+    if not energy_only:
+        b += asm.n_owned * 8 + nnz * hb
     if w.has_rhs:
         b += asm.n_owned * 8
     return b
+
+
+ENERGY_KERNELS = {"plaplace": "k_energy_tri", "gl": "k_energy_tri", "he": "k_energy_tet", "mc": "k_mc_elem (energy)"}
 
 
 # ---------------------------------------------------------------------------
@@ -445,20 +455,22 @@ def _oracle_sample(w, min_seconds=8.0, max_passes=5):
     return asm, u, n_el, label, min_seconds, max_passes, int(torch.get_num_threads())
 
 
-def cpu_port_baseline(w):
+def cpu_port_baseline(w, energy_only=False):
     """The oracle (CPU restatement of the reference path) on a bounded sample."""
     asm, u, n_el, label, min_s, max_p, cores = _oracle_sample(w)
-    asm.all_in_one(u)  # warm-up
+    step = (lambda: asm.energy_fn(u)) if energy_only else (lambda: asm.all_in_one(u))  # noqa: E731
+    step()  # warm-up
     times = []
-    while len(times) < max_p and sum(times) < min_s:
+    while len(times) < (20 if energy_only else max_p) and sum(times) < min_s:
         t = time.perf_counter()
-        asm.all_in_one(u)
+        step()
         times.append(time.perf_counter() - t)
     dt = sum(times) / len(times)
+    what = ("energy passes of the CPU restatement (the reference element energy, NumPy float64)" if energy_only
+            else "fused E+grad+Hess passes of the CPU restatement (torch.func float64 autodiff of the reference "
+                 "element energy + np.add.at scatter)")
     return {"value": n_el / dt, "unit": "elements/s", "cores": cores, "kind": "port",
-            "sample": f"{label} ({n_el} elements), {len(times)} fused E+grad+Hess passes of the CPU "
-                      "restatement (torch.func float64 autodiff of the reference element energy + np.add.at "
-                      "scatter)", "seconds_per_pass": dt}
+            "sample": f"{label} ({n_el} elements), {len(times)} {what}", "seconds_per_pass": dt}
 
 
 def run_reference(args):
@@ -790,7 +802,8 @@ def run(args):
     n_el = int(asm.info["n_elem"])
     dev = torch.device("cuda", local)
     u = torch.as_tensor(u0, device=dev)
-    flags = _lib.FNE_ENERGY | _lib.FNE_GRAD | _lib.FNE_HESS
+    energy_only = args.pass_ == "energy"
+    flags = _lib.FNE_ENERGY if energy_only else _lib.FNE_ENERGY | _lib.FNE_GRAD | _lib.FNE_HESS
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     launches_per_pass = asm.launches_per_eval(flags)
@@ -824,38 +837,41 @@ def run(args):
     host_e = torch.empty(1, dtype=torch.float64).pin_memory()
     dev_u = torch.empty_like(u)
     e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for _ in range(args.warmup):
+    def e2e_pass():
         dev_u.copy_(pin_u, non_blocking=True)
         e, g, h = asm.eval(dev_u, flags)
-        host_e.copy_(e, non_blocking=True), host_g.copy_(g, non_blocking=True), host_h.copy_(h, non_blocking=True)
+        host_e.copy_(e, non_blocking=True)
+        if not energy_only:
+            host_g.copy_(g, non_blocking=True)
+            host_h.copy_(h, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_pass()
     torch.cuda.synchronize()
     _barrier(world)
     for i in range(args.steps):
         flush.fill_(float(i))
         e2e_ev[i][0].record(stream)
-        dev_u.copy_(pin_u, non_blocking=True)
-        e, g, h = asm.eval(dev_u, flags)
-        host_e.copy_(e, non_blocking=True)
-        host_g.copy_(g, non_blocking=True)
-        host_h.copy_(h, non_blocking=True)
+        e2e_pass()
         e2e_ev[i][1].record(stream)
     torch.cuda.synchronize()
     e2e_s = _max_over_ranks(sum(a.elapsed_time(b) for a, b in e2e_ev) * 1e-3, world)
     e2e_value = world * n_el * args.steps / e2e_s
 
     # roofline of the pass (one kernel launch per pass for the P1 families)
-    alg_bytes = algorithmic_bytes(w, asm, n_el)
+    alg_bytes = algorithmic_bytes(w, asm, n_el, energy_only)
     peak, peak_kind = _peaks()
     avg_launch_s = (sum(kernel_ms) / len(kernel_ms)) * 1e-3
     achieved = alg_bytes / avg_launch_s / 1e9
-    kname = KERNEL_NAMES.get(asm.info["kernel_variant"], "?")
+    kname = ENERGY_KERNELS[w.family] if energy_only else KERNEL_NAMES.get(asm.info["kernel_variant"], "?")
     traffic = NCU_TRAFFIC.get((w.name, kname))
     nnz = int(asm.owned_values.numel())
 
     if rank == 0:
-        cpu = cpu_port_baseline(w) if (world == 1 and not args.no_cpu_baseline) else None
+        cpu = cpu_port_baseline(w, energy_only) if (world == 1 and not args.no_cpu_baseline) else None
         line = {
-            "metric": "elements/s (E+grad+Hess)", "value": value, "unit": "elements/s", "n_gpus": world,
+            "metric": "elements/s (energy)" if energy_only else "elements/s (E+grad+Hess)", "value": value,
+            "unit": "elements/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
             "data": "synthetic (seeded / closed-form state on the generated mesh)",
@@ -872,7 +888,8 @@ def run(args):
                          "launches_per_pass": launches_per_pass},
             "e2e": {"value": e2e_value, "unit": "elements/s",
                     "h2d_bytes_per_step": int(u0.nbytes),
-                    "d2h_bytes_per_step": int(8 + host_g.numel() * 8 + host_h.numel() * host_h.element_size())},
+                    "d2h_bytes_per_step": 8 if energy_only else
+                    int(8 + host_g.numel() * 8 + host_h.numel() * host_h.element_size())},
             "gpu_launches": args.steps * launches_per_pass,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
@@ -893,6 +910,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pass", dest="pass_", default="egh", choices=["egh", "energy"],
+                    help="egh: fused energy + gradient + Hessian pass (default); energy: the energy-only pass "
+                         "(the line-search callback)")
     ap.add_argument("--kernel-variant", default="auto", choices=["auto", "row_gather", "incidence", "element", "cuda_cores", "push",
                                                                   "row_lanes_2", "row_lanes_4", "row_lanes_8"])
     args = ap.parse_args()

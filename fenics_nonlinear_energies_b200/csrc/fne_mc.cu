@@ -944,6 +944,103 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
 }
 
 // ---------------------------------------------------------------------------
+// Energy and / or gradient without the Hessian (the line-search and gradient
+// callbacks): tiles of 32 elements; the tile's gathered nodal values and
+// geometry are staged in shared memory, then threads run over (quadrature
+// point, element): strain from the reference tables and J^-1, return map
+// (the tangent it would also form is not used and is compiled out), energy
+// density, and for the gradient the pulled-back helper s[c][k] =
+// w sum_i J^-1_ik sigma[v(c, i)]; the element gradient g_(a,c) = sum_q R_qak
+// s_q[c][k] follows per (element, DOF).
+// ---------------------------------------------------------------------------
+constexpr int kEgTile = 32, kEgThreads = 256;
+
+template <typename Real, int NP, int NQ, int WANT>
+__global__ void __launch_bounds__(kEgThreads) k_mc_eg(McArgs A, McConstR<Real> M, Real* __restrict__ gbuf,
+                                                      double* __restrict__ partials, unsigned* __restrict__ counter,
+                                                      double* __restrict__ eout) {
+  constexpr int TE = kEgTile, N2 = 2 * NP, NT = kEgThreads;
+  constexpr int US = N2 + 1;  // odd row stride of the staged nodal values: no bank conflicts
+  __shared__ Real sD1[NQ * NP], sD2[NQ * NP], sW[NQ];
+  __shared__ Real sU[TE * US];
+  __shared__ Real sGm[TE * 5];
+  __shared__ Real sS[(WANT & MW_G) ? NQ * TE * 4 : 1];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < NQ * NP; i += NT) {
+    sD1[i] = (Real)A.dhat1[i];
+    sD2[i] = (Real)A.dhat2[i];
+  }
+  for (int i = tid; i < NQ; i += NT) sW[i] = (Real)A.qw[i];
+  double eacc = 0.0;
+  const int n_tiles = (A.n_el + TE - 1) / TE;
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int e0 = tile * TE;
+    const int ne = min(TE, A.n_el - e0);
+    __syncthreads();  // previous tile's readers are done (and the tables are loaded)
+    for (int i = tid; i < ne * N2; i += NT) {
+      const int code = __ldg(A.codes + (long long)e0 * N2 + i);
+      sU[(i / N2) * US + i % N2] = (Real)(code >= 0 ? __ldg(A.u + code) : __ldg(A.dir + (-1 - code)));
+    }
+    for (int i = tid; i < ne * 5; i += NT) sGm[i] = (Real)__ldg(A.geom + (long long)e0 * 5 + i);
+    __syncthreads();
+    for (int p = tid; p < TE * NQ; p += NT) {
+      const int q = p / TE, el = p - q * TE;
+      if (el >= ne) continue;
+      const Real* gm = sGm + el * 5;
+      const Real i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
+      const Real* ue = sU + el * US;
+      Real ex = Real(0), ey = Real(0), exy = Real(0);
+#pragma unroll 5
+      for (int a = 0; a < NP; ++a) {
+        const Real r1 = sD1[q * NP + a], r2 = sD2[q * NP + a];
+        const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
+        const Real ux = ue[2 * a], uy = ue[2 * a + 1];
+        ex += px * ux;
+        ey += py * uy;
+        exy += py * ux + px * uy;
+      }
+      Real eps[3] = {ex, ey, exy};
+      if (A.epsp) {
+        const double* ep = A.epsp + ((long long)(e0 + el) * NQ + q) * 3;
+        eps[0] -= (Real)ep[0];
+        eps[1] -= (Real)ep[1];
+        eps[2] -= (Real)ep[2];
+      }
+      Real sig[3], Ct[6], psi;
+      mc_point(M, eps, sig, Ct, psi);
+      const Real w = gm[4] * sW[q];
+      if ((WANT & MW_E) && A.wflag[e0 + el]) eacc += (double)(w * psi);
+      if (WANT & MW_G) {
+        Real* sg = sS + (q * TE + el) * 4;
+        sg[0] = w * (i00 * sig[0] + i10 * sig[2]);
+        sg[1] = w * (i01 * sig[0] + i11 * sig[2]);
+        sg[2] = w * (i00 * sig[2] + i10 * sig[1]);
+        sg[3] = w * (i01 * sig[2] + i11 * sig[1]);
+      }
+    }
+    if (WANT & MW_G) {
+      __syncthreads();
+      for (int i = tid; i < ne * N2; i += NT) {
+        const int el = i / N2, r = i - el * N2, a = r >> 1, c = r & 1;
+        Real acc = Real(0);
+#pragma unroll 5
+        for (int q = 0; q < NQ; ++q) {
+          const Real* sg = sS + (q * TE + el) * 4 + 2 * c;
+          acc += sD1[q * NP + a] * sg[0] + sD2[q * NP + a] * sg[1];
+        }
+        gbuf[(long long)(e0 + el) * N2 + r] = acc;
+      }
+    }
+  }
+  if (WANT & MW_E) {
+    if (A.rhs)
+      for (int i = blockIdx.x * NT + threadIdx.x; i < A.n_owned; i += gridDim.x * NT)
+        eacc -= A.rhs[i] * A.u[A.lo + i];
+    mc_energy_finalize(eacc, partials, counter, eout);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // FP64 P2 / P4: the same contraction K[(a,b),(c,d,e)] = P[(a,b),(q,k,l)] ·
 // Ã[(q,k,l),(c,d,e)] as the tensor-core kernel, in FP64 on the DMMA units
 // (mma.sync m16n8k4 f64) with the direct-write epilogue straight from the
@@ -1323,6 +1420,8 @@ struct McHandle {
   void* dp_sbuf = nullptr;  // 4 floats (tensor-core path) or 4 doubles (DMMA path) per slot
   // FP64 DMMA path (P2 / P4)
   int dm = 0, grid_dm = 1;
+  // tiled energy / gradient kernel for the calls without the Hessian
+  int use_eg = 0, grid_eg = 1;
   int n_fix = 0;
   int *fx_con = nullptr, *fx_desc = nullptr;
   // matrix-free products: weighted tangents at the linearization point and
@@ -1442,6 +1541,16 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
       }
       return mc_gathers<double, double, NP>(h, flags, static_cast<const double*>(nullptr), g, grad, hess, st);
     }
+  }
+  if (!(flags & MW_H) && h->use_eg) {  // energy / gradient callbacks
+    const int ge = h->grid_eg;
+    switch (flags) {
+      case 1: k_mc_eg<Real, NP, NQ, 1><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
+      case 2: k_mc_eg<Real, NP, NQ, 2><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
+      case 3: k_mc_eg<Real, NP, NQ, 3><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
+      default: return cudaErrorInvalidValue;
+    }
+    return mc_gathers<Real, HOut, NP>(h, flags, K, g, grad, hess, st);
   }
   switch (flags) {
     case 1: k_mc_elem<Real, NP, NQ, 1><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
@@ -1711,6 +1820,10 @@ int mc_create(const fne_desc* d, McHandle** out) {
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev);
   h->grid_elem = (int)std::max<int64_t>(1, std::min<int64_t>(h->num_sms * 8, (nl + kMcWarps - 1) / kMcWarps));
   h->n_partials = h->grid_elem;
+  // energy / gradient calls: the tiled kernel unless the CUDA-core kernel is requested
+  h->use_eg = d->kernel_variant != 1;
+  h->grid_eg = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)h->num_sms * 4, (nl + kEgTile - 1) / kEgTile,
+                                                            (int64_t)h->n_partials}));
   const size_t rsz = d->precision == FNE_FP32 ? sizeof(float) : sizeof(double);
   int rc = FNE_OK;
 #define MC_TRY(x)      \

@@ -141,8 +141,11 @@ def test_mc_energy_only_and_repeatability():
     e1, g1, h1 = [t.clone() for t in gpu.eval(u, 7)]
     e2, g2, h2 = [t.clone() for t in gpu.eval(u, 7)]
     assert torch.equal(h1, h2) and torch.equal(g1, g2) and torch.equal(e1, e2)
+    # the energy-only pass is the tiled energy / gradient kernel: same value
+    # to rounding (other summation order)
     e_only = gpu.eval(u, _lib.FNE_ENERGY)[0].clone()
-    assert torch.equal(e_only, e1)
+    assert abs(float(e_only.item()) - float(e1.item())) <= 1e-14 * max(1.0, abs(float(e1.item())))
+    assert torch.equal(e_only, gpu.eval(u, _lib.FNE_ENERGY)[0])
 
 
 @pytest.mark.parametrize("degree", [2, 4])
@@ -266,3 +269,34 @@ def test_mc_nonzero_previous_plastic_strain(degree, precision):
                           shape=(gpu.layout.n_free,) * 2).tocsr()
     y = gpu.matrix_free_mult("matfree_element", torch.as_tensor(x, device="cuda")).cpu().numpy()
     assert np.abs(y - A @ x).max() <= tol * np.abs(A @ x).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("degree", [1, 2, 4])
+def test_mc_energy_gradient_kernel(degree, precision):
+    """Energy-only, gradient-only and energy + gradient calls (the tiled
+    energy / gradient kernel) against the oracle, against the CUDA-core
+    kernel, with a non-zero previous plastic strain, bit-repeatable."""
+    params = meshes.slope_problem(level=1, degree=degree, lam=1.2, with_elem_B=True)
+    rng = np.random.default_rng(17 + degree)
+    params["eps_p_old"] = 1e-4 * rng.standard_normal(params["eps_p_old"].shape)
+    hd = torch.float32 if precision == "fp32" else torch.float64
+    gpu, ref = _pair(params, precision=precision, hess_dtype=hd)
+    cc, _ = _pair(params, precision=precision, hess_dtype=hd, kernel_variant="cuda_cores")
+    u = 0.04 * rng.standard_normal(gpu.layout.n_free)
+    ut = torch.as_tensor(u, device="cuda")
+    e_ref, g_ref, _ = ref.all_in_one(u)
+    scale = _abs_scale(ref, u)
+    etol, gtol = (1e-12, 1e-12) if precision == "fp64" else (1e-5, 1e-4)
+    e1 = float(gpu.eval(ut, _lib.FNE_ENERGY)[0].item())
+    g2 = gpu.eval(ut, _lib.FNE_GRAD)[1].clone()
+    e3, g3, _ = gpu.eval(ut, _lib.FNE_ENERGY | _lib.FNE_GRAD)
+    assert abs(e1 - e_ref) <= etol * scale and abs(float(e3.item()) - e_ref) <= etol * scale
+    assert _rel(g2.cpu().numpy(), g_ref) <= gtol and _rel(g3.cpu().numpy(), g_ref) <= gtol
+    ec = float(cc.eval(ut, _lib.FNE_ENERGY)[0].item())
+    gc = cc.eval(ut, _lib.FNE_GRAD)[1]
+    ctol = 1e-13 if precision == "fp64" else 1e-5
+    assert abs(e1 - ec) <= ctol * scale
+    assert _rel(g2.cpu().numpy(), gc.cpu().numpy()) <= ctol
+    assert torch.equal(gpu.eval(ut, _lib.FNE_GRAD)[1], g2)
+    assert float(gpu.eval(ut, _lib.FNE_ENERGY)[0].item()) == e1
