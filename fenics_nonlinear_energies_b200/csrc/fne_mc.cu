@@ -755,17 +755,19 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
         const float* gm = sGm + el * 5;
         const float i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
         const float* ue = sU + el * N2;
-        float ex = 0.f, ey = 0.f, exy = 0.f;
+        float gx1 = 0.f, gx2 = 0.f, gy1 = 0.f, gy2 = 0.f;  // reference-gradient contractions
 #pragma unroll 5
         for (int a = 0; a < NP; ++a) {
           const float r1 = sD1[q * NP + a], r2 = sD2[q * NP + a];
-          const float px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
           const float ux = ue[2 * a], uy = ue[2 * a + 1];
-          ex += px * ux;
-          ey += py * uy;
-          exy += py * ux + px * uy;
+          gx1 += r1 * ux;
+          gx2 += r2 * ux;
+          gy1 += r1 * uy;
+          gy2 += r2 * uy;
         }
-        float eps[3] = {ex, ey, exy};
+        const float uxx = i00 * gx1 + i01 * gx2, uxy = i10 * gx1 + i11 * gx2;
+        const float uyx = i00 * gy1 + i01 * gy2, uyy = i10 * gy1 + i11 * gy2;
+        float eps[3] = {uxx, uyy, uxy + uyx};
         if (A.epsp) {
           const double* ep = A.epsp + ((long long)(e0 + el) * NQ + q) * 3;
           eps[0] -= (float)ep[0];
@@ -989,17 +991,21 @@ __global__ void __launch_bounds__(kEgThreads) k_mc_eg(McArgs A, McConstR<Real> M
       const Real* gm = sGm + el * 5;
       const Real i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
       const Real* ue = sU + el * US;
-      Real ex = Real(0), ey = Real(0), exy = Real(0);
+      // reference-gradient contractions first (4 multiply-adds per node),
+      // then J^-1: grad u = [[i00 Gx1 + i01 Gx2, ...]]
+      Real gx1 = Real(0), gx2 = Real(0), gy1 = Real(0), gy2 = Real(0);
 #pragma unroll 5
       for (int a = 0; a < NP; ++a) {
         const Real r1 = sD1[q * NP + a], r2 = sD2[q * NP + a];
-        const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
         const Real ux = ue[2 * a], uy = ue[2 * a + 1];
-        ex += px * ux;
-        ey += py * uy;
-        exy += py * ux + px * uy;
+        gx1 += r1 * ux;
+        gx2 += r2 * ux;
+        gy1 += r1 * uy;
+        gy2 += r2 * uy;
       }
-      Real eps[3] = {ex, ey, exy};
+      const Real uxx = i00 * gx1 + i01 * gx2, uxy = i10 * gx1 + i11 * gx2;  // d ux / dx, d ux / dy
+      const Real uyx = i00 * gy1 + i01 * gy2, uyy = i10 * gy1 + i11 * gy2;  // d uy / dx, d uy / dy
+      Real eps[3] = {uxx, uyy, uxy + uyx};
       if (A.epsp) {
         const double* ep = A.epsp + ((long long)(e0 + el) * NQ + q) * 3;
         eps[0] -= (Real)ep[0];
@@ -1231,17 +1237,19 @@ __global__ void __launch_bounds__(McTileD<NP, NQ>::THREADS, McTileD<NP, NQ>::MIN
         const double* gm = sGm + el * 5;
         const double i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
         const double* ue = sU + el * N2;
-        double ex = 0.0, ey = 0.0, exy = 0.0;
+        double gx1 = 0.0, gx2 = 0.0, gy1 = 0.0, gy2 = 0.0;  // reference-gradient contractions
 #pragma unroll 5
         for (int a = 0; a < NP; ++a) {
           const double r1 = sD1[q * NP + a], r2 = sD2[q * NP + a];
-          const double px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
           const double ux = ue[2 * a], uy = ue[2 * a + 1];
-          ex += px * ux;
-          ey += py * uy;
-          exy += py * ux + px * uy;
+          gx1 += r1 * ux;
+          gx2 += r2 * ux;
+          gy1 += r1 * uy;
+          gy2 += r2 * uy;
         }
-        double eps[3] = {ex, ey, exy};
+        const double uxx = i00 * gx1 + i01 * gx2, uxy = i10 * gx1 + i11 * gx2;
+        const double uyx = i00 * gy1 + i01 * gy2, uyy = i10 * gy1 + i11 * gy2;
+        double eps[3] = {uxx, uyy, uxy + uyx};
         if (A.epsp) {
           const double* ep = A.epsp + ((long long)(e0 + el) * NQ + q) * 3;
           eps[0] -= ep[0];
