@@ -123,12 +123,12 @@ class DeviceCG:
         self.n = int(n)
         self.device = torch.device(device)
         self.fp32 = bool(fp32)
-        _, rp = rows_arr = _lib.i64(rows)
-        _, cp = cols_arr = _lib.i64(cols)
-        if rows_arr[0].size != cols_arr[0].size:
+        rows_np, rp = _lib.i64(rows)  # the arrays stay referenced until the call returns
+        cols_np, cp = _lib.i64(cols)
+        if rows_np.size != cols_np.size:
             raise ValueError("rows and cols differ in length")
         h = ctypes.c_void_p()
-        _lib.check(_lib.lib.fne_cg_create(self.n, int(rows_arr[0].size), rp, cp, int(self.fp32), int(chunk),
+        _lib.check(_lib.lib.fne_cg_create(self.n, int(rows_np.size), rp, cp, int(self.fp32), int(chunk),
                                           ctypes.byref(h)))
         self._h = h
         self.chunk = int(chunk)
