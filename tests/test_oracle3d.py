@@ -1,0 +1,127 @@
+"""CPU checks of the 3-D Mohr-Coulomb oracle (``oracle/energies3d.py``).
+
+The reference pins its 3-D density the same way (finite differences of the
+autodiff stress / tangent, ``tests/test_slope_stability_3d.py:434-523``):
+elastic closed form, central differences of sigma = dpsi/deps and
+D = dsigma/deps inside every branch, branch coverage, continuity of psi
+across the yield surface, and an element-level check on a P1 tetrahedron.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import energies3d as E3
+
+LAME, SHEAR = 2.0e4 * 0.3 / (1.3 * 0.4), 2.0e4 / 2.6  # E = 2e4, nu = 0.3
+BULK = LAME + 2.0 * SHEAR / 3.0
+
+
+def _params(c_bar, sin_phi, n):
+    return [np.full(n, v) for v in (c_bar, sin_phi, SHEAR, BULK, LAME)]
+
+
+def test_elastic_branch_closed_form():
+    rng = np.random.default_rng(0)
+    eps = 1e-4 * rng.standard_normal((5, 6))
+    sig, D, psi, br = E3.mc_stress_tangent(eps, *_params(1e6, 0.5, 5))
+    assert (br == 0).all()
+    np.testing.assert_allclose(psi, E3.elastic_density(eps, SHEAR, LAME), rtol=1e-13)
+    I1 = eps[:, :3].sum(1)
+    sig_ref = np.concatenate([LAME * I1[:, None] + 2 * SHEAR * eps[:, :3], SHEAR * eps[:, 3:]], axis=1)
+    np.testing.assert_allclose(sig, sig_ref, rtol=1e-12, atol=1e-12 * np.abs(sig_ref).max())
+    D_ref = np.zeros((6, 6))
+    D_ref[:3, :3] = LAME
+    D_ref += np.diag([2 * SHEAR] * 3 + [SHEAR] * 3)
+    for i in range(5):
+        np.testing.assert_allclose(D[i], D_ref, rtol=1e-12, atol=1e-9)
+
+
+def _sample_branches(n=4000, seed=1):
+    rng = np.random.default_rng(seed)
+    dev = rng.standard_normal((n, 6)) * 1e-3
+    vol = rng.uniform(-1.0, 4.0, size=(n, 1)) * 1e-3
+    eps = dev.copy()
+    eps[:, :3] += vol
+    c = rng.uniform(0.1, 20.0, size=n)
+    sp = rng.uniform(0.2, 0.7, size=n)
+    _, br = E3.mc_density(eps, c, sp, SHEAR, BULK, LAME)
+    return eps, c, sp, br
+
+
+def test_every_branch_is_reached():
+    _, _, _, br = _sample_branches()
+    counts = np.bincount(br, minlength=5)
+    assert (counts > 0).all(), counts
+
+
+@pytest.mark.parametrize("branch", [1, 2, 3, 4])
+def test_stress_and_tangent_by_central_differences(branch):
+    eps, c, sp, br = _sample_branches()
+    idx = np.flatnonzero(br == branch)[:3]
+    h = 1e-8
+    for i in idx:
+        e0 = eps[i]
+        prm = [c[i], sp[i], SHEAR, BULK, LAME]
+        sig, D, psi, b = E3.mc_stress_tangent(e0[None], *prm)
+        assert b[0] == branch
+        ok = True
+        fd_sig = np.zeros(6)
+        fd_D = np.zeros((6, 6))
+        for k in range(6):
+            dk = np.zeros(6)
+            dk[k] = h
+            (pp, bp), (pm, bm) = E3.mc_density(e0 + dk, *prm), E3.mc_density(e0 - dk, *prm)
+            ok &= bool(bp[()] == branch and bm[()] == branch)
+            fd_sig[k] = (pp - pm) / (2 * h)
+            sp_, _, _, _ = E3.mc_stress_tangent((e0 + dk)[None], *prm)
+            sm_, _, _, _ = E3.mc_stress_tangent((e0 - dk)[None], *prm)
+            fd_D[:, k] = (sp_[0] - sm_[0]) / (2 * h)
+        if not ok:  # a difference step crossed a branch boundary
+            continue
+        # the apex potential is linear in I1 (zero tangent): absolute scale = the elastic modulus
+        scale = LAME + 2.0 * SHEAR
+        np.testing.assert_allclose(sig[0], fd_sig, rtol=2e-5, atol=2e-5 * np.abs(sig[0]).max())
+        np.testing.assert_allclose(D[0], fd_D, rtol=5e-4, atol=5e-4 * np.abs(D[0]).max() + 1e-8 * scale)
+        np.testing.assert_allclose(D[0], D[0].T, atol=1e-9 * max(np.abs(D[0]).max(), scale))
+
+
+def test_potential_continuous_across_yield_surface():
+    """psi is C1 across the elastic / plastic boundary: along a strain ray the
+    values just inside and just outside agree to the step."""
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        d = rng.standard_normal(6)
+        prm = [rng.uniform(0.5, 5.0), rng.uniform(0.2, 0.6), SHEAR, BULK, LAME]
+        ts = np.linspace(0.0, 5e-3, 4001)
+        psi, br = E3.mc_density(ts[:, None] * d[None], *prm)
+        cross = np.flatnonzero((br[:-1] == 0) & (br[1:] != 0))
+        if cross.size == 0:
+            continue
+        j = cross[0]
+        jump = abs(psi[j + 1] - psi[j])
+        slope = abs(psi[j] - psi[j - 1])
+        assert jump <= 3.0 * slope + 1e-12
+
+
+def test_p1_tet_element_derivatives():
+    X = np.array([[0.0, 0.0, 0.0], [1.0, 0.1, 0.0], [0.2, 1.1, 0.1], [0.1, 0.3, 0.9]])
+    M = np.concatenate([np.ones((4, 1)), X], axis=1)
+    grads = np.linalg.inv(M)[1:]                       # (3, 4): d phi_a / d x_k
+    vol = abs(np.linalg.det(M)) / 6.0
+    dphix, dphiy, dphiz = (grads[k][None, :] for k in range(3))
+    qw = np.array([vol])
+    prm = [np.array([60.0]), np.array([0.45]), np.array([SHEAR]), np.array([BULK]), np.array([LAME])]
+    rng = np.random.default_rng(4)
+    u = 2e-3 * rng.standard_normal(12)
+    e, g, H, br = E3.element_derivatives(u, dphix, dphiy, dphiz, qw, *prm)
+    assert br[0] == 2  # a return branch with a full-rank tangent at this load (left edge)
+    h = 1e-8
+    fd_g = np.array([(E3.element_derivatives(u + h * np.eye(12)[i], dphix, dphiy, dphiz, qw, *prm)[0] -
+                      E3.element_derivatives(u - h * np.eye(12)[i], dphix, dphiy, dphiz, qw, *prm)[0]) / (2 * h)
+                     for i in range(12)])
+    np.testing.assert_allclose(g, fd_g, rtol=1e-5, atol=1e-5 * np.abs(g).max())
+    d = rng.standard_normal(12)
+    gp = E3.element_derivatives(u + h * d, dphix, dphiy, dphiz, qw, *prm)[1]
+    gm = E3.element_derivatives(u - h * d, dphix, dphiy, dphiz, qw, *prm)[1]
+    np.testing.assert_allclose(H @ d, (gp - gm) / (2 * h), rtol=5e-4, atol=5e-4 * np.abs(H @ d).max())
+    np.testing.assert_allclose(H, H.T, atol=1e-9 * np.abs(H).max())
