@@ -421,3 +421,78 @@ def slope_elem_B(params):
     B[:, :, 2, 0::2] = gy
     B[:, :, 2, 1::2] = gx
     return B
+
+
+# ---------------------------------------------------------------------------
+# Tetrahedral Lagrange elements (3-D slope family)
+# ---------------------------------------------------------------------------
+# Node order of src/problems/slope_stability_3d/support/simplex_lagrange.py:
+# vertices, then the interior points of the edges (0,1), (1,2), (0,2), (1,3),
+# (2,3), (0,3) from the first vertex towards the second, then the interior
+# points of the faces (0,1,2), (0,1,3), (0,2,3), (1,2,3), then the cell
+# interior.  Each node is a tuple of barycentric counts summing to p.
+TET_EDGES = ((0, 1), (1, 2), (0, 2), (1, 3), (2, 3), (0, 3))
+TET_FACES = ((0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3))
+
+
+def _tri_interior_counts(p):
+    return [(a, b, p - a - b) for a in range(p - 2, 0, -1) for b in range(p - a - 1, 0, -1) if p - a - b > 0]
+
+
+def tet_lagrange_counts(p):
+    """Barycentric count tuples (c0, c1, c2, c3) of the degree-p nodes, in node order."""
+    p = int(p)
+    if p < 1:
+        raise ValueError("degree must be >= 1")
+    out = [tuple(p if i == v else 0 for i in range(4)) for v in range(4)]
+    for i, j in TET_EDGES:
+        for k in range(1, p):
+            c = [0, 0, 0, 0]
+            c[i], c[j] = p - k, k
+            out.append(tuple(c))
+    for face in TET_FACES:
+        for tri in _tri_interior_counts(p):
+            c = [0, 0, 0, 0]
+            for local, vertex in enumerate(face):
+                c[vertex] = tri[local]
+            out.append(tuple(c))
+    out += [(a, b, c, p - a - b - c) for a in range(p - 3, 0, -1) for b in range(p - a - 2, 0, -1)
+            for c in range(p - a - b - 1, 0, -1) if p - a - b - c > 0]
+    return out
+
+
+def tet_lagrange_points(p):
+    """Reference coordinates (3, n_p) of the nodes: (c1, c2, c3) / p."""
+    return np.array([[c[1], c[2], c[3]] for c in tet_lagrange_counts(p)], dtype=np.float64).T / float(p)
+
+
+def tet_lagrange_tabulate(p, xi):
+    """Values (n_p, nq) and reference derivatives d/dxi_k (3 x (n_p, nq)) of the
+    degree-p basis at ``xi`` (3, nq).  Basis of node c: prod_i L_{c_i}(lambda_i)
+    with L_m(l) = prod_{j<m} (p l - j) / (j + 1) (barycentric Lagrange form);
+    d/dxi_k = d/dlambda_k - d/dlambda_0."""
+    p = int(p)
+    xi = np.asarray(xi, dtype=np.float64)
+    lam = np.stack([1.0 - xi[0] - xi[1] - xi[2], xi[0], xi[1], xi[2]])   # (4, nq)
+
+    def factor(m, l):
+        val, der = np.ones_like(l), np.zeros_like(l)
+        for j in range(m):
+            f = (p * l - j) / (j + 1)
+            der = der * f + val * (p / (j + 1))
+            val = val * f
+        return val, der
+
+    counts = tet_lagrange_counts(p)
+    phi = np.empty((len(counts), xi.shape[1]))
+    dlam = np.empty((4, len(counts), xi.shape[1]))
+    for n, c in enumerate(counts):
+        vals, ders = zip(*(factor(c[i], lam[i]) for i in range(4)))
+        phi[n] = vals[0] * vals[1] * vals[2] * vals[3]
+        for i in range(4):
+            term = ders[i]
+            for j in range(4):
+                if j != i:
+                    term = term * vals[j]
+            dlam[i, n] = term
+    return phi, dlam[1] - dlam[0], dlam[2] - dlam[0], dlam[3] - dlam[0]

@@ -102,3 +102,32 @@ def test_mc_oracle_gravity_load_matches_reference_rule():
     area = float(np.sum(p["det_j"]) / 2.0)
     assert math.isclose(total, -p["gamma"] * area, rel_tol=1e-12)
     assert asm.f_owned.size == asm.layout.hi - asm.layout.lo
+
+
+@pytest.mark.parametrize("p", [1, 2, 4])
+def test_tet_lagrange_tabulation(p):
+    """Tetrahedral Lagrange basis: node count, the simplex_lagrange node order
+    (P2 golden: vertices, then edge midpoints of (0,1), (1,2), (0,2), (1,3),
+    (2,3), (0,3)), Kronecker property, partition of unity, and derivatives by
+    central differences."""
+    from fenics_nonlinear_energies_b200 import meshes
+
+    counts = meshes.tet_lagrange_counts(p)
+    assert len(counts) == (p + 1) * (p + 2) * (p + 3) // 6 and len(set(counts)) == len(counts)
+    if p == 2:
+        assert counts == [(2, 0, 0, 0), (0, 2, 0, 0), (0, 0, 2, 0), (0, 0, 0, 2), (1, 1, 0, 0), (0, 1, 1, 0),
+                          (1, 0, 1, 0), (0, 1, 0, 1), (0, 0, 1, 1), (1, 0, 0, 1)]
+    pts = meshes.tet_lagrange_points(p)
+    phi, d1, d2, d3 = meshes.tet_lagrange_tabulate(p, pts)
+    np.testing.assert_allclose(phi, np.eye(len(counts)), atol=1e-12)
+    rng = np.random.default_rng(p)
+    x = rng.dirichlet(np.ones(4), size=7).T[1:]          # interior points (3, 7)
+    phi, d1, d2, d3 = meshes.tet_lagrange_tabulate(p, x)
+    np.testing.assert_allclose(phi.sum(0), 1.0, atol=1e-12)
+    for k, dk in enumerate((d1, d2, d3)):
+        np.testing.assert_allclose(dk.sum(0), 0.0, atol=1e-10)
+        h = 1e-6
+        e = np.zeros((3, 1))
+        e[k] = h
+        fd = (meshes.tet_lagrange_tabulate(p, x + e)[0] - meshes.tet_lagrange_tabulate(p, x - e)[0]) / (2 * h)
+        np.testing.assert_allclose(dk, fd, atol=1e-7 * max(1.0, np.abs(dk).max()))
