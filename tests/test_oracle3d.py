@@ -125,3 +125,23 @@ def test_p1_tet_element_derivatives():
     gm = E3.element_derivatives(u - h * d, dphix, dphiy, dphiz, qw, *prm)[1]
     np.testing.assert_allclose(H @ d, (gp - gm) / (2 * h), rtol=5e-4, atol=5e-4 * np.abs(H @ d).max())
     np.testing.assert_allclose(H, H.T, atol=1e-9 * np.abs(H).max())
+
+
+@pytest.mark.parametrize("branch", [0, 1, 2, 3, 4])
+def test_spectral_chain_rule_matches_autodiff(branch):
+    """The eigenvalue chain rule a device kernel evaluates (d lambda = v v^T,
+    second derivatives with the 1/(lambda_k - lambda_j) eigenvector terms)
+    against autodiff through eigvalsh, in every branch."""
+    from oracle import spectral3d
+
+    eps, c, sp, br = _sample_branches()
+    idx = np.flatnonzero(br == branch)[:4]
+    assert idx.size > 0
+    for i in idx:
+        prm = [c[i], sp[i], SHEAR, BULK, LAME]
+        sig_a, D_a, _, b = E3.mc_stress_tangent(eps[i][None], *prm)
+        sig_s, D_s, bs = spectral3d.stress_tangent_spectral(eps[i], *prm)
+        assert b[0] == bs == branch
+        scale = LAME + 2.0 * SHEAR
+        np.testing.assert_allclose(sig_s, sig_a[0], rtol=1e-9, atol=1e-11 * scale * np.abs(eps[i]).max())
+        np.testing.assert_allclose(D_s, D_a[0], rtol=1e-7, atol=1e-9 * scale)
