@@ -496,3 +496,100 @@ def tet_lagrange_tabulate(p, xi):
                     term = term * vals[j]
             dlam[i, n] = term
     return phi, dlam[1] - dlam[0], dlam[2] - dlam[0], dlam[3] - dlam[0]
+
+
+def gauss_jacobi_tet(n):
+    """Collapsed (Stroud conical product) Gauss-Jacobi rule with ``n**3`` points,
+    exact to degree 2n-1 on the reference tetrahedron (volume 1/6):
+    x = a (1-b)(1-c), y = b (1-c), z = c with Jacobian (1-b)(1-c)^2."""
+    from scipy.special import roots_jacobi
+
+    tc, wc = roots_jacobi(n, 2.0, 0.0)
+    tb, wb = roots_jacobi(n, 1.0, 0.0)
+    ta, wa = roots_jacobi(n, 0.0, 0.0)
+    c, b, a = (tc + 1.0) / 2.0, (tb + 1.0) / 2.0, (ta + 1.0) / 2.0
+    pts, w = [], []
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                pts.append((a[k] * (1.0 - b[j]) * (1.0 - c[i]), b[j] * (1.0 - c[i]), c[i]))
+                w.append(wc[i] * wb[j] * wa[k] / 64.0)
+    return np.array(pts).T, np.array(w)
+
+
+def slope3d_problem(nx=8, ny=2, nz=4, *, degree=2, length=40.0, width=10.0, h_left=20.0, h_right=10.0,
+                    x1=15.0, x2=25.0, E=2.0e4, nu=0.3, c0=6.0, phi_deg=45.0, psi_deg=0.0, lam=1.0,
+                    gamma=20.0, quad_n=None):
+    """Synthetic 3-D slope: x in [0, length], y in [0, width], z in [0, H(x)] with
+    H = h_left up to x1, linear to h_right at x2, h_right after; a structured
+    nx x ny x nz hex grid mapped to that profile, every hex split into six
+    tetrahedra (positively oriented), P1 or P2 nodes in the tetrahedral
+    Lagrange order of ``tet_lagrange_counts``.  Fixed: all components at
+    z = 0, u_x at x = 0 and x = length, u_y at y = 0 and y = width.  Davis-B
+    reduced strength at ``lam``; gravity ``gamma`` along -z.  Returns the
+    element data the 3-D density needs per element and quadrature point."""
+    if degree not in (1, 2):
+        raise ValueError("degree must be 1 or 2")
+    xs = np.linspace(0.0, length, nx + 1)
+    hx = np.interp(xs, [0.0, x1, x2, length], [h_left, h_left, h_right, h_right])
+    nid = np.arange((nx + 1) * (ny + 1) * (nz + 1)).reshape(nx + 1, ny + 1, nz + 1)
+    I, J, K = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    verts = np.stack([xs[I], width * J / ny, hx[I] * K / nz], axis=-1).reshape(-1, 3)
+    kuhn = ((0, 1, 3, 7), (0, 1, 5, 7), (0, 2, 3, 7), (0, 2, 6, 7), (0, 4, 5, 7), (0, 4, 6, 7))
+    tets = []
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                c = [nid[i + (m & 1), j + ((m >> 1) & 1), k + ((m >> 2) & 1)] for m in range(8)]
+                for t in kuhn:
+                    v = [c[m] for m in t]
+                    if np.linalg.det(verts[v[1:]] - verts[v[0]]) < 0.0:
+                        v[2], v[3] = v[3], v[2]
+                    tets.append(v)
+    tets = np.array(tets, dtype=np.int64)
+    nodes = verts
+    if degree == 2:
+        edge_id = {}
+        mids = []
+        conn = np.empty((tets.shape[0], 10), dtype=np.int64)
+        conn[:, :4] = tets
+        for e, t in enumerate(tets):
+            for q, (a, b) in enumerate(TET_EDGES):
+                key = (min(t[a], t[b]), max(t[a], t[b]))
+                if key not in edge_id:
+                    edge_id[key] = verts.shape[0] + len(mids)
+                    mids.append(0.5 * (verts[t[a]] + verts[t[b]]))
+                conn[e, 4 + q] = edge_id[key]
+        nodes = np.concatenate([verts, np.array(mids)])
+        tets = conn
+    n_nodes = nodes.shape[0]
+    fixed = np.zeros((n_nodes, 3), dtype=bool)
+    tol = 1e-9
+    fixed[np.abs(nodes[:, 2]) < tol, :] = True
+    fixed[(np.abs(nodes[:, 0]) < tol) | (np.abs(nodes[:, 0] - length) < tol), 0] = True
+    fixed[(np.abs(nodes[:, 1]) < tol) | (np.abs(nodes[:, 1] - width) < tol), 1] = True
+    freedofs = np.flatnonzero(~fixed.ravel()).astype(np.int64)
+    xi, wq = gauss_jacobi_tet(quad_n or (degree + 1))
+    _, d1, d2, d3 = tet_lagrange_tabulate(degree, xi)           # (n_p, nq)
+    X = nodes[tets[:, :4]]                                     # (E, 4, 3)
+    Jm = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)  # dx / dxi (E, 3, 3)
+    det = np.linalg.det(Jm)
+    Jinv = np.linalg.inv(Jm)                                   # dxi / dx
+    R = np.stack([d1, d2, d3], axis=0)                         # (3, n_p, nq)
+    G = np.einsum("eki,kpq->eiqp", Jinv, R)                     # (E, 3, nq, n_p): d phi_p / d x_i
+    c_bar, phi_red = davis_b_reduction(c0, phi_deg, psi_deg, lam)
+    lame = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    shear = E / (2.0 * (1.0 + nu))
+    bulk = lame + 2.0 * shear / 3.0
+    ne, nq = tets.shape[0], wq.size
+    full = lambda v: np.full((ne, nq), float(v))  # noqa: E731
+    phi_vals = tet_lagrange_tabulate(degree, xi)[0]            # (n_p, nq)
+    load = np.zeros(3 * n_nodes)
+    np.add.at(load, 3 * tets + 2, -gamma * np.einsum("e,q,pq->ep", np.abs(det), wq, phi_vals))
+    elems = (3 * tets[:, :, None] + np.arange(3)).reshape(ne, -1)
+    return {
+        "nodes": nodes, "elems_scalar": tets, "elems": elems, "freedofs": freedofs, "u_0": np.zeros(3 * n_nodes),
+        "dphix": G[:, 0], "dphiy": G[:, 1], "dphiz": G[:, 2], "quad_weight": np.abs(det)[:, None] * wq[None, :],
+        "c_bar": full(2.0 * c_bar * math.cos(math.radians(phi_red))), "sin_phi": full(math.sin(math.radians(phi_red))),
+        "shear": full(shear), "bulk": full(bulk), "lame": full(lame), "force": load,
+    }

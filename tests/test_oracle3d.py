@@ -145,3 +145,68 @@ def test_spectral_chain_rule_matches_autodiff(branch):
         scale = LAME + 2.0 * SHEAR
         np.testing.assert_allclose(sig_s, sig_a[0], rtol=1e-9, atol=1e-11 * scale * np.abs(eps[i]).max())
         np.testing.assert_allclose(D_s, D_a[0], rtol=1e-7, atol=1e-9 * scale)
+
+
+def test_tet_quadrature_exactness():
+    from math import factorial
+
+    from fenics_nonlinear_energies_b200 import meshes
+
+    for n in (2, 3, 4):
+        xi, w = meshes.gauss_jacobi_tet(n)
+        assert abs(w.sum() - 1.0 / 6.0) < 1e-15
+        for a in range(2 * n):
+            for b in range(2 * n - a):
+                for c in range(2 * n - a - b):
+                    exact = factorial(a) * factorial(b) * factorial(c) / factorial(a + b + c + 3)
+                    assert abs(np.sum(w * xi[0] ** a * xi[1] ** b * xi[2] ** c) - exact) < 1e-15
+
+
+def test_slope3d_mesh_and_assembly():
+    """Synthetic P2 tet slope: counts, volume, orientation; global energy,
+    gradient and Hessian assembled from the 3-D oracle, checked by central
+    differences along random directions (the layout of the future family)."""
+    from fenics_nonlinear_energies_b200 import meshes
+
+    p = meshes.slope3d_problem(nx=2, ny=1, nz=1, degree=2, lam=1.5, quad_n=2)  # 8 points: enough for FD checks
+    nv = 3 * 2 * 2
+    assert p["elems_scalar"].shape == (12, 10)
+    assert p["nodes"].shape[0] == nv + len({tuple(sorted(e)) for t in p["elems_scalar"][:, :4]
+                                            for e in [(t[a], t[b]) for a, b in meshes.TET_EDGES]})
+    # straight-sided slope over two x cells: H = 20 at x = 0, 15 at x = 20, 10 at x = 40
+    assert abs(p["quad_weight"].sum() - 10.0 * (20.0 * 17.5 + 20.0 * 12.5)) < 1e-9
+    X = p["nodes"][p["elems_scalar"][:, :4]]
+    assert (np.linalg.det(np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], 1)) > 0).all()
+    free, elems = p["freedofs"], p["elems"]
+    prm = [p[k] for k in ("c_bar", "sin_phi", "shear", "bulk", "lame")]
+
+    def assemble(u_free, want_h=True):
+        u = p["u_0"].copy()
+        u[free] = u_free
+        n = u.size
+        e_tot, g, H = 0.0, np.zeros(n), np.zeros((n, n)) if want_h else None
+        for e in range(elems.shape[0]):
+            args = (p["dphix"][e], p["dphiy"][e], p["dphiz"][e], p["quad_weight"][e], *[a[e] for a in prm])
+            if want_h:
+                ee, ge, He, _ = E3.element_derivatives(u[elems[e]], *args)
+                H[np.ix_(elems[e], elems[e])] += He
+            else:
+                eps = E3.strain6(u[elems[e]], *args[:3])
+                ee = float(np.sum(args[3] * E3.mc_density(eps, *[a for a in args[4:]])[0]))
+                ge = 0.0
+            e_tot += ee
+            if want_h:
+                np.add.at(g, elems[e], ge)
+        e_tot -= p["force"] @ u
+        return e_tot, (g - p["force"])[free], (H[np.ix_(free, free)] if want_h else None)
+
+    rng = np.random.default_rng(7)
+    u = 3e-3 * rng.standard_normal(free.size)
+    e0, g0, H0 = assemble(u)
+    np.testing.assert_allclose(H0, H0.T, atol=1e-9 * np.abs(H0).max())
+    d = rng.standard_normal(free.size)
+    h = 1e-7
+    fd = (assemble(u + h * d, False)[0] - assemble(u - h * d, False)[0]) / (2 * h)
+    assert abs(fd - g0 @ d) <= 1e-5 * abs(g0 @ d) + 1e-9
+    gp, gm = assemble(u + h * d)[1], assemble(u - h * d)[1]
+    np.testing.assert_allclose(H0 @ d, (gp - gm) / (2 * h), rtol=1e-3, atol=1e-4 * np.abs(H0 @ d).max())
