@@ -64,13 +64,14 @@ def _branch_F(branch, c_bar, sin_phi, shear, bulk, lame, tiny):
     return F
 
 
-def stress_tangent_spectral(eps6, c_bar, sin_phi, shear, bulk, lame, tiny=E3.TINY):
-    """(sigma (6,), D (6, 6), branch) at one strain by the spectral chain rule."""
+def stress_tangent_spectral(eps6, c_bar, sin_phi, shear, bulk, lame, tiny=E3.TINY, eigh=np.linalg.eigh):
+    """(sigma (6,), D (6, 6), branch) at one strain by the spectral chain rule;
+    ``eigh``: the symmetric eigen-decomposition used (LAPACK or ``jacobi_eigh3``)."""
     eps6 = np.asarray(eps6, dtype=np.float64)
     _, br = E3.mc_density(eps6[None], c_bar, sin_phi, shear, bulk, lame, tiny)
     br = int(br[0])
     A = np.einsum("m,mij->ij", eps6, _DA) + tiny * np.diag([0.0, 1.0, 2.0])
-    w, V = np.linalg.eigh(A)
+    w, V = eigh(A)
     order = [2, 1, 0]                       # descending: lambda_1 >= lambda_2 >= lambda_3
     lam, V = w[order], V[:, order]
     g = np.einsum("ik,mij,jk->km", V, _DA, V)            # g[k, m] = v_k^T dA_m v_k
@@ -89,3 +90,31 @@ def stress_tangent_spectral(eps6, c_bar, sin_phi, shear, bulk, lame, tiny=E3.TIN
     sigma = F_e + g.T @ F_l
     D = F_ee + g.T @ F_le + F_le.T @ g + g.T @ F_ll @ g + np.einsum("k,kmn->mn", F_l, Hk)
     return sigma, D, br
+
+
+def jacobi_eigh3(A, sweeps=6):
+    """Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations
+    (the textbook method: for each off-diagonal (p, q), the rotation that
+    zeroes it, t = sgn(theta) / (|theta| + sqrt(theta^2 + 1)) with
+    theta = (a_qq - a_pp) / (2 a_pq)), a fixed number of sweeps -- the form a
+    device kernel evaluates per quadrature point without data-dependent loop
+    counts.  Returns (w ascending, V) like numpy.linalg.eigh."""
+    a = np.array(A, dtype=np.float64, copy=True)
+    V = np.eye(3)
+    for _ in range(sweeps):
+        for p, q in ((0, 1), (0, 2), (1, 2)):
+            apq = a[p, q]
+            if apq == 0.0:
+                continue
+            theta = (a[q, q] - a[p, p]) / (2.0 * apq)
+            t = np.copysign(1.0, theta) / (abs(theta) + np.sqrt(theta * theta + 1.0))
+            c = 1.0 / np.sqrt(t * t + 1.0)
+            s = t * c
+            R = np.eye(3)
+            R[p, p] = R[q, q] = c
+            R[p, q], R[q, p] = s, -s
+            a = R.T @ a @ R
+            V = V @ R
+    w = np.diag(a).copy()
+    order = np.argsort(w)
+    return w[order], V[:, order]

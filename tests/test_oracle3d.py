@@ -140,11 +140,12 @@ def test_spectral_chain_rule_matches_autodiff(branch):
     for i in idx:
         prm = [c[i], sp[i], SHEAR, BULK, LAME]
         sig_a, D_a, _, b = E3.mc_stress_tangent(eps[i][None], *prm)
-        sig_s, D_s, bs = spectral3d.stress_tangent_spectral(eps[i], *prm)
-        assert b[0] == bs == branch
         scale = LAME + 2.0 * SHEAR
-        np.testing.assert_allclose(sig_s, sig_a[0], rtol=1e-9, atol=1e-11 * scale * np.abs(eps[i]).max())
-        np.testing.assert_allclose(D_s, D_a[0], rtol=1e-7, atol=1e-9 * scale)
+        for eigh in (np.linalg.eigh, spectral3d.jacobi_eigh3):   # LAPACK and the kernel's Jacobi sweeps
+            sig_s, D_s, bs = spectral3d.stress_tangent_spectral(eps[i], *prm, eigh=eigh)
+            assert b[0] == bs == branch
+            np.testing.assert_allclose(sig_s, sig_a[0], rtol=1e-9, atol=1e-11 * scale * np.abs(eps[i]).max())
+            np.testing.assert_allclose(D_s, D_a[0], rtol=1e-7, atol=1e-9 * scale)
 
 
 def test_tet_quadrature_exactness():
@@ -210,3 +211,22 @@ def test_slope3d_mesh_and_assembly():
     assert abs(fd - g0 @ d) <= 1e-5 * abs(g0 @ d) + 1e-9
     gp, gm = assemble(u + h * d)[1], assemble(u - h * d)[1]
     np.testing.assert_allclose(H0 @ d, (gp - gm) / (2 * h), rtol=1e-3, atol=1e-4 * np.abs(H0 @ d).max())
+
+
+def test_jacobi_eigh3_matches_lapack():
+    """Fixed-sweep cyclic Jacobi on symmetric 3x3 matrices (random, repeated and
+    tie-broken nearly repeated eigenvalues, diagonal) against LAPACK."""
+    from oracle import spectral3d
+
+    rng = np.random.default_rng(11)
+    mats = [(lambda M: 0.5 * (M + M.T))(rng.standard_normal((3, 3))) * 10.0 ** rng.uniform(-4, 2) for _ in range(200)]
+    Q = np.linalg.qr(rng.standard_normal((3, 3)))[0]
+    mats += [Q @ np.diag([1e-3, 1e-3, -2e-3]) @ Q.T, Q @ np.diag([5e-4] * 3) @ Q.T,
+             np.diag([3.0, 1.0, 2.0]), Q @ np.diag([1e-3, 1e-3 + 1e-15, 1e-3 + 2e-15]) @ Q.T]
+    for A in mats:
+        w, V = spectral3d.jacobi_eigh3(A)
+        w_ref = np.linalg.eigvalsh(A)
+        scale = max(np.abs(w_ref).max(), 1e-300)
+        np.testing.assert_allclose(w, w_ref, rtol=0, atol=1e-14 * scale)
+        np.testing.assert_allclose(V.T @ V, np.eye(3), atol=1e-13)
+        np.testing.assert_allclose(V @ np.diag(w) @ V.T, A, atol=1e-13 * scale)
