@@ -107,7 +107,8 @@ def jacobi_eigh3(A, sweeps=6):
             if apq == 0.0:
                 continue
             theta = (a[q, q] - a[p, p]) / (2.0 * apq)
-            t = np.copysign(1.0, theta) / (abs(theta) + np.sqrt(theta * theta + 1.0))
+            # t -> 1 / (2 theta) for large theta (no overflow of theta^2)
+            t = 0.5 / theta if abs(theta) > 1e100 else np.copysign(1.0, theta) / (abs(theta) + np.sqrt(theta * theta + 1.0))
             c = 1.0 / np.sqrt(t * t + 1.0)
             s = t * c
             R = np.eye(3)
