@@ -98,3 +98,13 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 12
     for n in sorted(names):
         assert hasattr(_lib.lib, n), n
+
+
+@pytest.mark.parametrize("reorder", ["none", "block_xyz"])
+@pytest.mark.parametrize("size", [1, 2, 3])
+def test_slope3d_p2_layout(reorder, size):
+    """The 3-D family's layout (P2 tetrahedra, 3 DOFs per node, 30 DOFs per
+    element) through the same C++ builder, bit for bit against the oracle."""
+    p = meshes.slope3d_problem(nx=3, ny=2, nz=2, degree=2)
+    for rank in range(size):
+        _compare(p, bs=3, coord_key="nodes", dir_key="u_0", reorder=reorder, rank=rank, size=size)
