@@ -509,6 +509,9 @@ def run_reference(args):
 
         def step():
             return newton_cpu(asm, u, tolg_rel=1e-6, **w.newton_kw)
+    elif args.pass_ == "energy":
+        def step():
+            return asm.energy_fn(u)
     else:
         def step():
             return asm.all_in_one(u)
@@ -522,10 +525,12 @@ def run_reference(args):
     dt = sum(times) / len(times)
     newton_op = w.op == "newton"
     value, unit = (dt, "s") if newton_op else (n_el / dt, "elements/s")
+    energy_op = w.op == "egh" and args.pass_ == "energy"
     metric = {"hvp": "elements/s (matrix-free H(u) x)", "newton": "Newton s to 1e-6 rel-grad"}.get(
-        w.op, "elements/s (E+grad+Hess)")
+        w.op, "elements/s (energy)" if energy_op else "elements/s (E+grad+Hess)")
     what = ("one Newton solve to 1e-6 relative gradient (oracle assembler, NumPy/SciPy Jacobi CG, the same "
             "golden-section line search)" if newton_op else
+            "energy pass of the CPU restatement of the reference element energy" if energy_op else
             "CPU restatement of the reference JAX element kernels (torch.func float64 autodiff) + np.add.at scatter")
     line = {
         "impl": "reference", "metric": metric, "value": value, "unit": unit,
