@@ -1,0 +1,217 @@
+// One quadrature point of the 3-D Mohr-Coulomb density: energy, stress and
+// consistent tangent in strain space, as host/device code (the reference
+// density is src/problems/slope_stability_3d/jax/jax_energy_3d.py:38-191;
+// its derivatives there come from JAX autodiff through eigvalsh).
+//
+// Strain eps = [xx, yy, zz, xy, yz, xz] with engineering shears.  With
+// A = tensor(eps) + tiny diag(0, 1, 2), lambda_1 >= lambda_2 >= lambda_3 its
+// eigenvalues, I1 = eps_xx + eps_yy + eps_zz and
+// Q = eps_xx^2 + eps_yy^2 + eps_zz^2 + (xy^2 + yz^2 + xz^2) / 2, every
+// branch potential is a quadratic form in z = (lambda_1, lambda_2,
+// lambda_3, I1) plus mu Q (elastic and smooth branches), built from terms
+// -n^2 / (2 d) with n = a.z - c linear:
+//   elastic  lame/2 I1^2 + mu Q
+//   smooth   lame/2 I1^2 + mu Q - f^2 / (2 d_s),     f = 2mu((1+s)l1 - (1-s)l3) + 2 lame s I1 - c
+//   left     lame/2 I1^2 + mu(l3^2 + (l1+l2)^2/2) - n_l^2 / (2 d_l)
+//   right    lame/2 I1^2 + mu(l1^2 + (l2+l3)^2/2) - n_r^2 / (2 d_r)
+//   apex     K/2 I1^2 - n_a^2 / (2 d_a)
+// (each d through the reference's signed tiny guard).  The branch is picked
+// from the primal values in the reference's order.  Stress and tangent
+// follow by the chain rule with the eigenvalue derivatives
+//   d lambda_k / dA = v_k v_k^T,
+//   d2 lambda_k / dA dA[X, Y] = 2 sum_{j != k} (v_k^T X v_j)(v_j^T Y v_k) / (lambda_k - lambda_j),
+// eigenvectors from a fixed six-sweep cyclic Jacobi solve.
+#pragma once
+
+#include <cmath>
+
+#ifdef __CUDACC__
+#define FNE_HD __host__ __device__ __forceinline__
+#else
+#define FNE_HD inline
+#endif
+
+namespace fne {
+namespace mc3d {
+
+// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations (fixed sweep
+// count); w descending, V columns the eigenvectors.
+FNE_HD void eigh3(const double A0[3][3], double w[3], double V[3][3]) {
+  double a[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      a[i][j] = A0[i][j];
+      V[i][j] = i == j ? 1.0 : 0.0;
+    }
+  const int P[3] = {0, 0, 1}, Qi[3] = {1, 2, 2};
+  for (int sweep = 0; sweep < 6; ++sweep) {
+    for (int r = 0; r < 3; ++r) {
+      const int p = P[r], q = Qi[r];
+      const double apq = a[p][q];
+      if (apq == 0.0) continue;
+      const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+      const double t = fabs(theta) > 1e100 ? 0.5 / theta
+                                            : (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+      const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+      // a <- R^T a R with R = identity except R_pp = R_qq = c, R_pq = s, R_qp = -s
+      for (int k = 0; k < 3; ++k) {  // columns p, q
+        const double akp = a[k][p], akq = a[k][q];
+        a[k][p] = c * akp - s * akq;
+        a[k][q] = s * akp + c * akq;
+      }
+      for (int k = 0; k < 3; ++k) {  // rows p, q
+        const double apk = a[p][k], aqk = a[q][k];
+        a[p][k] = c * apk - s * aqk;
+        a[q][k] = s * apk + c * aqk;
+      }
+      for (int k = 0; k < 3; ++k) {
+        const double vkp = V[k][p], vkq = V[k][q];
+        V[k][p] = c * vkp - s * vkq;
+        V[k][q] = s * vkp + c * vkq;
+      }
+    }
+  }
+  // sort descending (three elements)
+  int o[3] = {0, 1, 2};
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2 - i; ++j)
+      if (a[o[j]][o[j]] < a[o[j + 1]][o[j + 1]]) {
+        const int tmp = o[j];
+        o[j] = o[j + 1];
+        o[j + 1] = tmp;
+      }
+  double Vs[3][3];
+  for (int k = 0; k < 3; ++k) {
+    w[k] = a[o[k]][o[k]];
+    for (int i = 0; i < 3; ++i) Vs[i][k] = V[i][o[k]];
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int k = 0; k < 3; ++k) V[i][k] = Vs[i][k];
+}
+
+FNE_HD double safe_denom(double x, double tiny) {
+  return fabs(x) < tiny ? (x >= 0.0 ? tiny : -tiny) : x;
+}
+
+// psi, sigma[6], D[6][6] at strain e[6].  Returns the branch (0 elastic,
+// 1 smooth, 2 left edge, 3 right edge, 4 apex).
+FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K, double lame, double tiny,
+                 double& psi, double sig[6], double D[6][6]) {
+  // dA / d eps_m: (i, j) entries with weight (1 for normals, 1/2 for the shears)
+  const double A[3][3] = {{e[0] + 0.0 * tiny, 0.5 * e[3], 0.5 * e[5]},
+                          {0.5 * e[3], e[1] + tiny, 0.5 * e[4]},
+                          {0.5 * e[5], 0.5 * e[4], e[2] + 2.0 * tiny}};
+  double lam[3], V[3][3];
+  eigh3(A, lam, V);
+  const double l1 = lam[0], l2 = lam[1], l3 = lam[2];
+  const double I1 = e[0] + e[1] + e[2];
+  const double Qv = e[0] * e[0] + e[1] * e[1] + e[2] * e[2] + 0.5 * (e[3] * e[3] + e[4] * e[4] + e[5] * e[5]);
+  // branch tests (primal values, the reference's order)
+  const double f_tr = 2.0 * mu * ((1.0 + sp) * l1 - (1.0 - sp) * l3) + 2.0 * lame * sp * I1 - c_bar;
+  const double g_sl = (l1 - l2) / fmax(tiny, 1.0 + sp), g_sr = (l2 - l3) / fmax(tiny, 1.0 - sp);
+  const double g_la = (l1 + l2 - 2.0 * l3) / fmax(tiny, 3.0 - sp), g_ra = (2.0 * l1 - l2 - l3) / fmax(tiny, 3.0 + sp);
+  const double d_s = safe_denom(4.0 * lame * sp * sp + 4.0 * mu * (1.0 + sp * sp), tiny);
+  const double d_l = safe_denom(4.0 * lame * sp * sp + mu * (1.0 + sp) * (1.0 + sp) + 2.0 * mu * (1.0 - sp) * (1.0 - sp), tiny);
+  const double d_r = safe_denom(4.0 * lame * sp * sp + 2.0 * mu * (1.0 + sp) * (1.0 + sp) + mu * (1.0 - sp) * (1.0 - sp), tiny);
+  const double d_a = safe_denom(4.0 * K * sp * sp, tiny);
+  // linear forms n = a.z - c over z = (l1, l2, l3, I1)
+  const double as[4] = {2.0 * mu * (1.0 + sp), 0.0, -2.0 * mu * (1.0 - sp), 2.0 * lame * sp};
+  const double al[4] = {mu * (1.0 + sp), mu * (1.0 + sp), -2.0 * mu * (1.0 - sp), 2.0 * lame * sp};
+  const double ar[4] = {2.0 * mu * (1.0 + sp), -mu * (1.0 - sp), -mu * (1.0 - sp), 2.0 * lame * sp};
+  const double aa[4] = {0.0, 0.0, 0.0, 2.0 * K * sp};
+  auto lin = [&](const double a[4]) { return a[0] * l1 + a[1] * l2 + a[2] * l3 + a[3] * I1 - c_bar; };
+  const double lam_s = f_tr / d_s, lam_l = lin(al) / d_l, lam_r = lin(ar) / d_r;
+  int br;
+  if (f_tr <= 0.0) br = 0;
+  else if (lam_s <= fmin(g_sl, g_sr)) br = 1;
+  else if (g_sl < g_sr && lam_l >= g_sl && lam_l <= g_la) br = 2;
+  else if (g_sl > g_sr && lam_r >= g_sr && lam_r <= g_ra) br = 3;
+  else br = 4;
+  // F(z) = 1/2 z^T M z + q^T z (+ const) + wQ Q: value, gradient Fz[4], Hessian Fzz[4][4]
+  double Fz[4] = {0, 0, 0, 0}, Fzz[4][4] = {{0}};
+  double wQ = 0.0;
+  psi = 0.0;
+  auto add_quad = [&](int i, int j, double coef) {  // + coef/2 (z_i + z_j)^2 style terms via M entries
+    Fzz[i][j] += coef;
+    if (i != j) Fzz[j][i] += coef;
+  };
+  const double z[4] = {l1, l2, l3, I1};
+  auto add_neg_sq = [&](const double a[4], double d) {  // - n^2 / (2 d), n = a.z - c
+    const double n = lin(a);
+    psi -= 0.5 * n * n / d;
+    for (int i = 0; i < 4; ++i) {
+      Fz[i] -= n / d * a[i];
+      for (int j = 0; j < 4; ++j) Fzz[i][j] -= a[i] * a[j] / d;
+    }
+  };
+  if (br == 4) {
+    psi = 0.5 * K * I1 * I1;
+    Fz[3] += K * I1;
+    add_quad(3, 3, K);
+    add_neg_sq(aa, d_a);
+  } else {
+    psi = 0.5 * lame * I1 * I1;
+    Fz[3] += lame * I1;
+    add_quad(3, 3, lame);
+    if (br <= 1) {
+      psi += mu * Qv;
+      wQ = mu;
+      if (br == 1) add_neg_sq(as, d_s);
+    } else if (br == 2) {  // mu (l3^2 + (l1 + l2)^2 / 2)
+      psi += mu * (l3 * l3 + 0.5 * (l1 + l2) * (l1 + l2));
+      Fz[2] += 2.0 * mu * l3;
+      Fz[0] += mu * (l1 + l2);
+      Fz[1] += mu * (l1 + l2);
+      add_quad(2, 2, 2.0 * mu);
+      add_quad(0, 0, mu);
+      add_quad(1, 1, mu);
+      add_quad(0, 1, mu);
+      add_neg_sq(al, d_l);
+    } else {  // mu (l1^2 + (l2 + l3)^2 / 2)
+      psi += mu * (l1 * l1 + 0.5 * (l2 + l3) * (l2 + l3));
+      Fz[0] += 2.0 * mu * l1;
+      Fz[1] += mu * (l2 + l3);
+      Fz[2] += mu * (l2 + l3);
+      add_quad(0, 0, 2.0 * mu);
+      add_quad(1, 1, mu);
+      add_quad(2, 2, mu);
+      add_quad(1, 2, mu);
+      add_neg_sq(ar, d_r);
+    }
+  }
+  (void)z;
+  // d z / d eps: eigenvalues g_k[m] = v_k^T dA_m v_k, I1 = (1, 1, 1, 0, 0, 0)
+  const int mi[6] = {0, 1, 2, 0, 1, 0}, mj[6] = {0, 1, 2, 1, 2, 2};
+  const double mw[6] = {1.0, 1.0, 1.0, 0.5, 0.5, 0.5};
+  // X[k][l][m] = v_k^T dA_m v_l
+  double X[3][3][6];
+  for (int k = 0; k < 3; ++k)
+    for (int l = 0; l < 3; ++l)
+      for (int m = 0; m < 6; ++m) {
+        const int i = mi[m], j = mj[m];
+        X[k][l][m] = i == j ? V[i][k] * V[i][l] : mw[m] * (V[i][k] * V[j][l] + V[j][k] * V[i][l]);
+      }
+  double dz[4][6];
+  for (int k = 0; k < 3; ++k)
+    for (int m = 0; m < 6; ++m) dz[k][m] = X[k][k][m];
+  for (int m = 0; m < 6; ++m) dz[3][m] = m < 3 ? 1.0 : 0.0;
+  for (int m = 0; m < 6; ++m) {
+    double s = wQ * (m < 3 ? 2.0 * e[m] : e[m]);
+    for (int a = 0; a < 4; ++a) s += Fz[a] * dz[a][m];
+    sig[m] = s;
+  }
+  for (int m = 0; m < 6; ++m)
+    for (int n = 0; n < 6; ++n) {
+      double s = (m == n) ? wQ * (m < 3 ? 2.0 : 1.0) : 0.0;
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) s += Fzz[a][b] * dz[a][m] * dz[b][n];
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+          if (j != k) s += Fz[k] * 2.0 * X[k][j][m] * X[j][k][n] / (lam[k] - lam[j]);
+      D[m][n] = s;
+    }
+  return br;
+}
+
+}  // namespace mc3d
+}  // namespace fne

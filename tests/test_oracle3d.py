@@ -230,3 +230,59 @@ def test_jacobi_eigh3_matches_lapack():
         np.testing.assert_allclose(w, w_ref, rtol=0, atol=1e-14 * scale)
         np.testing.assert_allclose(V.T @ V, np.eye(3), atol=1e-13)
         np.testing.assert_allclose(V @ np.diag(w) @ V.T, A, atol=1e-13 * scale)
+
+
+@pytest.fixture(scope="module")
+def mc3d_host(tmp_path_factory):
+    """The device header's point function compiled for the host with g++."""
+    import ctypes
+    import os
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    d = tmp_path_factory.mktemp("mc3d")
+    src = d / "shim.cpp"
+    src.write_text('#include "fne_mc3d_point.cuh"\n'
+                   'extern "C" int mc3d_point_host(const double* e, double c, double sp, double mu, double K,\n'
+                   '                               double lame, double tiny, double* psi, double* sig, double* D) {\n'
+                   '  double Dm[6][6];\n'
+                   '  const int br = fne::mc3d::point(e, c, sp, mu, K, lame, tiny, *psi, sig, Dm);\n'
+                   '  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) D[i * 6 + j] = Dm[i][j];\n'
+                   '  return br;\n}\n')
+    lib = d / "libmc3d.so"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I",
+                    os.path.join(root, "fenics_nonlinear_energies_b200", "csrc"), str(src), "-o", str(lib)],
+                   check=True)
+    so = ctypes.CDLL(str(lib))
+    dp = ctypes.POINTER(ctypes.c_double)
+    so.mc3d_point_host.restype = ctypes.c_int
+    so.mc3d_point_host.argtypes = [dp] + [ctypes.c_double] * 6 + [dp, dp, dp]
+
+    def call(e, c, sp, mu, K, lame, tiny=E3.TINY):
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        psi = np.zeros(1)
+        sig = np.zeros(6)
+        D = np.zeros(36)
+        br = so.mc3d_point_host(e.ctypes.data_as(dp), c, sp, mu, K, lame, tiny, psi.ctypes.data_as(dp),
+                                sig.ctypes.data_as(dp), D.ctypes.data_as(dp))
+        return br, psi[0], sig, D.reshape(6, 6)
+
+    return call
+
+
+@pytest.mark.parametrize("branch", [0, 1, 2, 3, 4])
+def test_device_point_function_on_host(mc3d_host, branch):
+    """fne_mc3d_point.cuh (the future kernel's per-point code: Jacobi eigen
+    solve, branch potentials as quadratic forms, spectral chain rule), compiled
+    for the host, against the oracle: branch, psi, sigma and D."""
+    eps, c, sp, br = _sample_branches()
+    idx = np.flatnonzero(br == branch)[:5]
+    scale = LAME + 2.0 * SHEAR
+    for i in idx:
+        b, psi, sig, D = mc3d_host(eps[i], c[i], sp[i], SHEAR, BULK, LAME)
+        assert b == branch
+        psi_ref, _ = E3.mc_density(eps[i][None], c[i], sp[i], SHEAR, BULK, LAME)
+        assert abs(psi - psi_ref[0]) <= 1e-12 * max(1.0, abs(psi_ref[0]))
+        sig_a, D_a, _, _ = E3.mc_stress_tangent(eps[i][None], c[i], sp[i], SHEAR, BULK, LAME)
+        np.testing.assert_allclose(sig, sig_a[0], rtol=1e-9, atol=1e-11 * scale * np.abs(eps[i]).max())
+        np.testing.assert_allclose(D, D_a[0], rtol=1e-7, atol=1e-9 * scale)
