@@ -108,3 +108,22 @@ def test_slope3d_p2_layout(reorder, size):
     p = meshes.slope3d_problem(nx=3, ny=2, nz=2, degree=2)
     for rank in range(size):
         _compare(p, bs=3, coord_key="nodes", dir_key="u_0", reorder=reorder, rank=rank, size=size)
+
+
+def test_device_cg_argument_checks_on_host():
+    """DeviceCG reaches fne_cg_create with the documented argument checks, which
+    run on the host before any device call: an entry outside the n x n block
+    is FNE_EBOUNDS, mismatched row / column arrays are rejected in Python."""
+    from fenics_nonlinear_energies_b200.newton import DeviceCG
+
+    with pytest.raises(_lib.FneError) as ei:
+        DeviceCG(3, np.array([0, 1, 3]), np.array([0, 1, 2]), device="cpu")
+    assert ei.value.code == _lib.FNE_EBOUNDS
+    with pytest.raises(_lib.FneError) as ei:
+        DeviceCG(3, np.array([0, 1, 2]), np.array([0, -1, 2]), device="cpu")
+    assert ei.value.code == _lib.FNE_EBOUNDS
+    with pytest.raises(ValueError):
+        DeviceCG(3, np.array([0, 1]), np.array([0, 1, 2]), device="cpu")
+    with pytest.raises(_lib.FneError) as ei:
+        DeviceCG(3, np.array([0, 1, 2]), np.array([0, 1, 2]), device="cpu", chunk=0)
+    assert ei.value.code == _lib.FNE_EINVAL
