@@ -526,8 +526,10 @@ def slope3d_problem(nx=8, ny=2, nz=4, *, degree=2, length=40.0, width=10.0, h_le
     tetrahedra (positively oriented), P1 or P2 nodes in the tetrahedral
     Lagrange order of ``tet_lagrange_counts``.  Fixed: all components at
     z = 0, u_x at x = 0 and x = length, u_y at y = 0 and y = width.  Davis-B
-    reduced strength at ``lam``; gravity ``gamma`` along -z.  Returns the
-    element data the 3-D density needs per element and quadrature point."""
+    reduced strength at ``lam``; gravity ``gamma`` along -z.  Quadrature:
+    the reference's rule for the degree (``tet_quadrature_reference``) unless
+    ``quad_n`` asks for a Gauss-Jacobi rule.  Returns the element data the
+    3-D density needs per element and quadrature point."""
     if degree not in (1, 2):
         raise ValueError("degree must be 1 or 2")
     xs = np.linspace(0.0, length, nx + 1)
@@ -569,7 +571,9 @@ def slope3d_problem(nx=8, ny=2, nz=4, *, degree=2, length=40.0, width=10.0, h_le
     fixed[(np.abs(nodes[:, 0]) < tol) | (np.abs(nodes[:, 0] - length) < tol), 0] = True
     fixed[(np.abs(nodes[:, 1]) < tol) | (np.abs(nodes[:, 1] - width) < tol), 1] = True
     freedofs = np.flatnonzero(~fixed.ravel()).astype(np.int64)
-    xi, wq = gauss_jacobi_tet(quad_n or (degree + 1))
+    # the reference's rule for the element degree (bit-compatible inputs), or
+    # a collapsed Gauss-Jacobi rule with quad_n points per direction
+    xi, wq = tet_quadrature_reference(degree) if quad_n is None else gauss_jacobi_tet(quad_n)
     _, d1, d2, d3 = tet_lagrange_tabulate(degree, xi)           # (n_p, nq)
     X = nodes[tets[:, :4]]                                     # (E, 4, 3)
     Jm = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)  # dx / dxi (E, 3, 3)
@@ -593,3 +597,26 @@ def slope3d_problem(nx=8, ny=2, nz=4, *, degree=2, length=40.0, width=10.0, h_le
         "c_bar": full(2.0 * c_bar * math.cos(math.radians(phi_red))), "sin_phi": full(math.sin(math.radians(phi_red))),
         "shear": full(shear), "bulk": full(bulk), "lame": full(lame), "force": load,
     }
+
+
+# The 3-D family's element rules for P1 / P2 tetrahedra, in the digits and
+# point order of src/problems/slope_stability_3d/support/mesh.py:935-1010 so
+# element inputs are bit-compatible: the centroid rule and Keast's 11-point
+# rule (one negative weight), weights already scaled to the volume 1/6.
+KEAST11_A, KEAST11_B = 0.0714285714285714, 0.785714285714286
+KEAST11_C, KEAST11_D = 0.399403576166799, 0.100596423833201
+KEAST11_W = (-0.013155555555555, 0.007622222222222, 0.024888888888888)
+
+
+def tet_quadrature_reference(degree):
+    """(xi (3, nq), w (nq,)) of the reference's tetrahedral rule for element degree 1 or 2."""
+    if degree == 1:
+        return np.full((3, 1), 0.25), np.array([1.0 / 6.0])
+    if degree != 2:
+        raise ValueError("the reference's tetrahedral rules here: degree 1 or 2")
+    a, b, c, d = KEAST11_A, KEAST11_B, KEAST11_C, KEAST11_D
+    pts = [(0.25, 0.25, 0.25)]
+    pts += [(a, a, a), (b, a, a), (a, b, a), (a, a, b)]                  # orbit (a, a, a, b)
+    pts += [(c, d, d), (d, c, d), (d, d, c), (c, c, d), (c, d, c), (d, c, c)]  # orbit (c, c, d, d)
+    w = [KEAST11_W[0]] + [KEAST11_W[1]] * 4 + [KEAST11_W[2]] * 6
+    return np.array(pts, dtype=np.float64).T, np.array(w, dtype=np.float64)

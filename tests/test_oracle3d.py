@@ -286,3 +286,26 @@ def test_device_point_function_on_host(mc3d_host, branch):
         sig_a, D_a, _, _ = E3.mc_stress_tangent(eps[i][None], c[i], sp[i], SHEAR, BULK, LAME)
         np.testing.assert_allclose(sig, sig_a[0], rtol=1e-9, atol=1e-11 * scale * np.abs(eps[i]).max())
         np.testing.assert_allclose(D, D_a[0], rtol=1e-7, atol=1e-9 * scale)
+
+
+def test_reference_tet_rules():
+    """The reference's P1 / P2 tet rules: volume 1/6, exactness (Keast's
+    11-point rule: degree 4, to the truncation of its digits), symmetric orbits."""
+    from math import factorial
+
+    from fenics_nonlinear_energies_b200 import meshes
+
+    for deg, exact_to in ((1, 1), (2, 4)):
+        xi, w = meshes.tet_quadrature_reference(deg)
+        assert abs(w.sum() - 1.0 / 6.0) < 1e-14
+        for a in range(exact_to + 1):
+            for b in range(exact_to + 1 - a):
+                for c in range(exact_to + 1 - a - b):
+                    exact = factorial(a) * factorial(b) * factorial(c) / factorial(a + b + c + 3)
+                    assert abs(np.sum(w * xi[0] ** a * xi[1] ** b * xi[2] ** c) - exact) < 2e-14
+    xi, w = meshes.tet_quadrature_reference(2)
+    bary = np.vstack([1.0 - xi.sum(0), xi])
+    for k in range(1, 11):  # every point's barycentric coordinates are one of the two orbits
+        s = np.sort(bary[:, k])
+        assert np.allclose(s, [meshes.KEAST11_A] * 3 + [meshes.KEAST11_B], atol=1e-14) or \
+            np.allclose(s, [meshes.KEAST11_D] * 2 + [meshes.KEAST11_C] * 2, atol=1e-14)
