@@ -213,5 +213,60 @@ FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K
   return br;
 }
 
+// One element with NP nodes (DOFs (x, y, z) per node) and nq points:
+// energy sum_q w_q psi_q, gradient g = sum_q w_q B_q^T sigma_q and Hessian
+// K = sum_q w_q B_q^T D_q B_q (dense 3NP x 3NP).  gx/gy/gz [nq][NP] are the
+// physical basis gradients, prm [nq][5] = (c_bar, sin_phi, shear, bulk, lame).
+template <int NP>
+FNE_HD double element(const double* u, const double* gx, const double* gy, const double* gz, const double* w,
+                      const double* prm, int nq, double tiny, double* g, double* K) {
+  constexpr int N = 3 * NP;
+  double e_tot = 0.0;
+  for (int i = 0; i < N; ++i) g[i] = 0.0;
+  for (int i = 0; i < N * N; ++i) K[i] = 0.0;
+  for (int q = 0; q < nq; ++q) {
+    const double* px = gx + q * NP;
+    const double* py = gy + q * NP;
+    const double* pz = gz + q * NP;
+    double e[6] = {0, 0, 0, 0, 0, 0};
+    for (int a = 0; a < NP; ++a) {
+      const double ux = u[3 * a], uy = u[3 * a + 1], uz = u[3 * a + 2];
+      e[0] += px[a] * ux;
+      e[1] += py[a] * uy;
+      e[2] += pz[a] * uz;
+      e[3] += py[a] * ux + px[a] * uy;
+      e[4] += pz[a] * uy + py[a] * uz;
+      e[5] += pz[a] * ux + px[a] * uz;
+    }
+    const double* m = prm + 5 * q;
+    double psi, sig[6], D[6][6];
+    point(e, m[0], m[1], m[2], m[3], m[4], tiny, psi, sig, D);
+    e_tot += w[q] * psi;
+    // B_q columns of DOF (a, c): the strain components it feeds
+    for (int a = 0; a < NP; ++a) {
+      const double b[3][6] = {{px[a], 0, 0, py[a], 0, pz[a]}, {0, py[a], 0, px[a], pz[a], 0}, {0, 0, pz[a], 0, py[a], px[a]}};
+      for (int c = 0; c < 3; ++c) {
+        double s = 0.0, Db[6];
+        for (int i = 0; i < 6; ++i) {
+          s += b[c][i] * sig[i];
+          Db[i] = 0.0;
+          for (int j = 0; j < 6; ++j) Db[i] += D[i][j] * b[c][j];
+        }
+        g[3 * a + c] += w[q] * s;
+        for (int a2 = 0; a2 < NP; ++a2) {
+          const double b2[3][6] = {{px[a2], 0, 0, py[a2], 0, pz[a2]}, {0, py[a2], 0, px[a2], pz[a2], 0},
+                                   {0, 0, pz[a2], 0, py[a2], px[a2]}};
+          for (int c2 = 0; c2 < 3; ++c2) {
+            double t = 0.0;
+            for (int i = 0; i < 6; ++i) t += b2[c2][i] * Db[i];
+            K[(3 * a2 + c2) * N + 3 * a + c] += w[q] * t;
+          }
+        }
+      }
+    }
+  }
+  return e_tot;
+}
+
 }  // namespace mc3d
 }  // namespace fne

@@ -243,6 +243,9 @@ def mc3d_host(tmp_path_factory):
     d = tmp_path_factory.mktemp("mc3d")
     src = d / "shim.cpp"
     src.write_text('#include "fne_mc3d_point.cuh"\n'
+                   'extern "C" double mc3d_element_p2_host(const double* u, const double* gx, const double* gy,\n'
+                   '    const double* gz, const double* w, const double* prm, int nq, double tiny, double* g,\n'
+                   '    double* K) { return fne::mc3d::element<10>(u, gx, gy, gz, w, prm, nq, tiny, g, K); }\n'
                    'extern "C" int mc3d_point_host(const double* e, double c, double sp, double mu, double K,\n'
                    '                               double lame, double tiny, double* psi, double* sig, double* D) {\n'
                    '  double Dm[6][6];\n'
@@ -258,6 +261,17 @@ def mc3d_host(tmp_path_factory):
     so.mc3d_point_host.restype = ctypes.c_int
     so.mc3d_point_host.argtypes = [dp] + [ctypes.c_double] * 6 + [dp, dp, dp]
 
+    so.mc3d_element_p2_host.restype = ctypes.c_double
+    so.mc3d_element_p2_host.argtypes = [dp] * 6 + [ctypes.c_int, ctypes.c_double, dp, dp]
+
+    def element(u, gx, gy, gz, w, prm, tiny=E3.TINY):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, gx, gy, gz, w, prm)]
+        g = np.zeros(30)
+        K = np.zeros(900)
+        e = so.mc3d_element_p2_host(*[a.ctypes.data_as(dp) for a in arrs], int(arrs[4].size), tiny,
+                                    g.ctypes.data_as(dp), K.ctypes.data_as(dp))
+        return e, g, K.reshape(30, 30)
+
     def call(e, c, sp, mu, K, lame, tiny=E3.TINY):
         e = np.ascontiguousarray(e, dtype=np.float64)
         psi = np.zeros(1)
@@ -267,6 +281,7 @@ def mc3d_host(tmp_path_factory):
                                 sig.ctypes.data_as(dp), D.ctypes.data_as(dp))
         return br, psi[0], sig, D.reshape(6, 6)
 
+    call.element = element
     return call
 
 
@@ -309,3 +324,21 @@ def test_reference_tet_rules():
         s = np.sort(bary[:, k])
         assert np.allclose(s, [meshes.KEAST11_A] * 3 + [meshes.KEAST11_B], atol=1e-14) or \
             np.allclose(s, [meshes.KEAST11_D] * 2 + [meshes.KEAST11_C] * 2, atol=1e-14)
+
+
+def test_device_element_function_on_host(mc3d_host):
+    """fne::mc3d::element<10> (P2 tet: energy, B^T sigma, B^T D B over the
+    reference's 11-point rule), host-compiled, against the oracle element."""
+    from fenics_nonlinear_energies_b200 import meshes
+
+    p = meshes.slope3d_problem(nx=2, ny=1, nz=1, degree=2, lam=1.5)
+    prm = np.stack([p[k] for k in ("c_bar", "sin_phi", "shear", "bulk", "lame")], axis=-1)  # (E, nq, 5)
+    rng = np.random.default_rng(21)
+    for el in (0, 5, 11):
+        u = 3e-3 * rng.standard_normal(30)
+        args = (p["dphix"][el], p["dphiy"][el], p["dphiz"][el], p["quad_weight"][el])
+        e_ref, g_ref, H_ref, br = E3.element_derivatives(u, *args, *[prm[el, :, k] for k in range(5)])
+        e, g, H = mc3d_host.element(u, *args, prm[el])
+        assert abs(e - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
+        np.testing.assert_allclose(g, g_ref, rtol=1e-9, atol=1e-10 * np.abs(g_ref).max())
+        np.testing.assert_allclose(H, H_ref, rtol=1e-7, atol=1e-9 * np.abs(H_ref).max())
