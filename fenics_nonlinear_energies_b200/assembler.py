@@ -464,23 +464,33 @@ class SlopeStabilityCudaAssembler(CudaElementAssemblerBase):
 class EnergyFunction(torch.autograd.Function):
     """``J(u)`` with ``dJ/du`` from the hand-written adjoint kernels.
 
+    ``u`` is the full reordered free vector (``layout.n_free`` entries).
     forward: one fused ENERGY|GRAD pass (the gradient is kept for backward);
-    backward: ``grad_out * gradient``.  The Hessian is not part of the autograd
-    graph: call ``assembler.assemble_hessian`` explicitly.
+    backward: ``grad_out * gradient`` as a tensor shaped like ``u``: the owned
+    rows ``[lo, hi)`` hold this rank's rows of dJ/du, the other rows are 0, so
+    summing the ranks' results gives dJ/du (one rank: dJ/du itself).  The
+    Hessian is not part of the autograd graph: call
+    ``assembler.assemble_hessian`` explicitly.
     """
 
     @staticmethod
     def forward(ctx, u, assembler):
+        if u.numel() != assembler.layout.n_free:
+            raise ValueError(f"u has {u.numel()} entries, expected layout.n_free = {assembler.layout.n_free}")
         e, g, _ = assembler.eval(u.detach().contiguous(), _lib.FNE_ENERGY | _lib.FNE_GRAD,
                                  energy=torch.empty(1, dtype=torch.float64, device=assembler.device),
-                                 grad=torch.empty(assembler.n_owned, dtype=torch.float64, device=assembler.device))
+                                 grad=torch.empty(max(1, assembler.n_owned), dtype=torch.float64,
+                                                  device=assembler.device))
         ctx.save_for_backward(g)
+        ctx.lo, ctx.hi, ctx.shape = int(assembler.layout.lo), int(assembler.layout.hi), u.shape
         return e[0]
 
     @staticmethod
     def backward(ctx, grad_out):
         (g,) = ctx.saved_tensors
-        return grad_out * g, None
+        full = torch.zeros(ctx.shape, dtype=g.dtype, device=g.device)
+        full.view(-1)[ctx.lo: ctx.hi] = g[: ctx.hi - ctx.lo]
+        return grad_out * full, None
 
 
 def energy(u, assembler):

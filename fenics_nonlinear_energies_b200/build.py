@@ -34,20 +34,32 @@ def needs_build() -> bool:
     return any(p.stat().st_mtime > t for p in deps if p.exists())
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    if not force and not needs_build():
-        return LIB
-    cmd = [
-        _nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-Xptxas=-warn-spills",
-        "-shared", "-o", str(LIB), *map(str, sources()),
-    ]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
+def _run(cmd):
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
+    return res.stdout + res.stderr
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    """Compile every translation unit to an object (in parallel), then link
+    the shared library.  Objects go to a temporary folder."""
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
+
+    if not force and not needs_build():
+        return LIB
+    flags = [_nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-Xptxas=-warn-spills"]
     if verbose:
-        sys.stdout.write(res.stdout + res.stderr)
+        flags.append("-Xptxas=-v")
+    with tempfile.TemporaryDirectory(prefix="fne_build_") as tmp:
+        objs = [Path(tmp) / (src.stem + ".o") for src in sources()]
+        cmds = [flags + ["-c", str(src), "-o", str(obj)] for src, obj in zip(sources(), objs)]
+        with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+            logs = list(ex.map(_run, cmds))
+        logs.append(_run([_nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs)]))
+    if verbose:
+        sys.stdout.write("".join(logs))
     return LIB
 
 

@@ -1255,26 +1255,28 @@ __global__ void __launch_bounds__(kElemThreads) k_energy_tet(const Chunk* __rest
 constexpr int kNoAllocMaxCtas = 1024;  // grid cap = number of partial sums
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxCtas + 1];  // + ticket slot
 
-__global__ void __launch_bounds__(256) k_energy_tri_soa(int fam, int n_el, const int* __restrict__ codes,
+__global__ void __launch_bounds__(256) k_energy_tri_soa(int fam, long long n_el, const int* __restrict__ codes,
                                                         const double* __restrict__ dvx,
                                                         const double* __restrict__ dvy,
                                                         const double* __restrict__ vol,
                                                         const double* __restrict__ weights,
                                                         const double* __restrict__ u,
                                                         const double* __restrict__ dir, Phys P,
-                                                        const double* __restrict__ rhs, int n_owned, long long lo,
-                                                        EnergyOut eo) {
+                                                        const double* __restrict__ rhs, long long n_owned,
+                                                        long long lo, EnergyOut eo) {
   double acc = 0.0;
-  const int stride = gridDim.x * blockDim.x;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += stride) {
+  // 64-bit element index: 3 * e exceeds INT32_MAX once n_el passes 715,827,882.
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n_el; e += stride) {
     const double w = weights ? weights[e] : 1.0;
     if (w == 0.0) continue;
     TriElem<double> t;
+    const long long b = 3LL * e;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      t.src[k] = codes[3 * e + k];
-      t.dvx[k] = dvx[3 * e + k];
-      t.dvy[k] = dvy[3 * e + k];
+      t.src[k] = codes[b + k];
+      t.dvx[k] = dvx[b + k];
+      t.dvy[k] = dvy[b + k];
     }
     t.vol = vol[e];
     t.wflag = 1;
@@ -1284,31 +1286,22 @@ __global__ void __launch_bounds__(256) k_energy_tri_soa(int fam, int n_el, const
     acc += w * (fam == FAM_PLAP ? tri_energy<double, FAM_PLAP>(P, vd, t) : tri_energy<double, FAM_GL>(P, vd, t));
   }
   if (rhs)
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_owned; i += stride) acc -= rhs[i] * u[lo + i];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_owned; i += stride)
+      acc -= rhs[i] * u[lo + i];
   energy_finalize(acc, eo);
 }
 
 namespace {
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device (looked up once
-// per device; the first call on a device performs the lookup).
+// Device address of g_noalloc_scratch on the current device.  It is looked up
+// on every call (cudaGetSymbolAddress allocates nothing and is cheap), so a
+// module reloaded after cudaDeviceReset or a primary-context re-creation is
+// picked up instead of a stale cached address.
 int noalloc_scratch(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(FNE_EBOUNDS, "device ordinal beyond 63");
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return set_error(FNE_ECUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = static_cast<double*>(p);
-  }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return set_error(FNE_ECUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+  *out = static_cast<double*>(p);
   return FNE_OK;
 }
 }  // namespace
@@ -1339,8 +1332,10 @@ extern "C" int fne_energy_p1tri_noalloc(int32_t family, int64_t n_elem, const in
   }
   P.p_is3 = family == FNE_PLAPLACE && params[0] == 3.0;
   int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t ae = cudaGetDevice(&dev);
+  if (ae == cudaSuccess) ae = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (ae != cudaSuccess)
+    return set_error(FNE_ECUDA, std::string("fne_energy_p1tri_noalloc device query: ") + cudaGetErrorString(ae));
   const int64_t work = std::max<int64_t>(n_elem, n_owned);
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)kNoAllocMaxCtas, (int64_t)sms * 8,
                                                                 (work + 255) / 256}));
@@ -1350,8 +1345,8 @@ extern "C" int fne_energy_p1tri_noalloc(int32_t family, int64_t n_elem, const in
   if (e != cudaSuccess)
     return set_error(FNE_ECUDA, std::string("fne_energy_p1tri_noalloc memset: ") + cudaGetErrorString(e));
   EnergyOut eo{scratch, ticket, energy, nullptr};
-  k_energy_tri_soa<<<grid, 256, 0, st>>>(family == FNE_PLAPLACE ? FAM_PLAP : FAM_GL, (int)n_elem, codes, dvx, dvy,
-                                         vol, weights, u, dirichlet, P, rhs, (int)n_owned, (long long)lo, eo);
+  k_energy_tri_soa<<<grid, 256, 0, st>>>(family == FNE_PLAPLACE ? FAM_PLAP : FAM_GL, (long long)n_elem, codes, dvx, dvy,
+                                         vol, weights, u, dirichlet, P, rhs, (long long)n_owned, (long long)lo, eo);
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_error(FNE_ECUDA, std::string("fne_energy_p1tri_noalloc launch: ") + cudaGetErrorString(e));

@@ -9,17 +9,18 @@
 // Q = eps_xx^2 + eps_yy^2 + eps_zz^2 + (xy^2 + yz^2 + xz^2) / 2, every
 // branch potential is a quadratic form in z = (lambda_1, lambda_2,
 // lambda_3, I1) plus mu Q (elastic and smooth branches), built from terms
-// -n^2 / (2 d) with n = a.z - c linear:
+// -d/2 (n / ds)^2 with n = a.z - c linear, d a constant denominator and ds
+// = d through the reference's signed tiny guard:
 //   elastic  lame/2 I1^2 + mu Q
-//   smooth   lame/2 I1^2 + mu Q - f^2 / (2 d_s),     f = 2mu((1+s)l1 - (1-s)l3) + 2 lame s I1 - c
-//   left     lame/2 I1^2 + mu(l3^2 + (l1+l2)^2/2) - n_l^2 / (2 d_l)
-//   right    lame/2 I1^2 + mu(l1^2 + (l2+l3)^2/2) - n_r^2 / (2 d_r)
-//   apex     K/2 I1^2 - n_a^2 / (2 d_a)
-// (each d through the reference's signed tiny guard).  The branch is picked
-// from the primal values in the reference's order.  Stress and tangent
+//   smooth   lame/2 I1^2 + mu Q - d_s/2 (f / ds_s)^2,  f = 2mu((1+s)l1 - (1-s)l3) + 2 lame s I1 - c
+//   left     lame/2 I1^2 + mu(l3^2 + (l1+l2)^2/2) - d_l/2 (n_l / ds_l)^2
+//   right    lame/2 I1^2 + mu(l1^2 + (l2+l3)^2/2) - d_r/2 (n_r / ds_r)^2
+//   apex     K/2 I1^2 - d_a/2 (n_a / ds_a)^2
+// The branch is picked from the primal values in the reference's order.  Stress and tangent
 // follow by the chain rule with the eigenvalue derivatives
 //   d lambda_k / dA = v_k v_k^T,
-//   d2 lambda_k / dA dA[X, Y] = 2 sum_{j != k} (v_k^T X v_j)(v_j^T Y v_k) / (lambda_k - lambda_j),
+//   d2 lambda_k / dA dA[X, Y] = 2 sum_{j != k} (v_k^T X v_j)(v_j^T Y v_k) / (lambda_k - lambda_j)
+// (summed per eigenvalue pair),
 // eigenvectors from a fixed six-sweep cyclic Jacobi solve.
 #pragma once
 
@@ -110,10 +111,14 @@ FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K
   const double f_tr = 2.0 * mu * ((1.0 + sp) * l1 - (1.0 - sp) * l3) + 2.0 * lame * sp * I1 - c_bar;
   const double g_sl = (l1 - l2) / fmax(tiny, 1.0 + sp), g_sr = (l2 - l3) / fmax(tiny, 1.0 - sp);
   const double g_la = (l1 + l2 - 2.0 * l3) / fmax(tiny, 3.0 - sp), g_ra = (2.0 * l1 - l2 - l3) / fmax(tiny, 3.0 + sp);
-  const double d_s = safe_denom(4.0 * lame * sp * sp + 4.0 * mu * (1.0 + sp * sp), tiny);
-  const double d_l = safe_denom(4.0 * lame * sp * sp + mu * (1.0 + sp) * (1.0 + sp) + 2.0 * mu * (1.0 - sp) * (1.0 - sp), tiny);
-  const double d_r = safe_denom(4.0 * lame * sp * sp + 2.0 * mu * (1.0 + sp) * (1.0 + sp) + mu * (1.0 - sp) * (1.0 - sp), tiny);
-  const double d_a = safe_denom(4.0 * K * sp * sp, tiny);
+  // raw denominators (they weight the return terms) and their signed-tiny
+  // guarded copies (they divide)
+  const double r_s = 4.0 * lame * sp * sp + 4.0 * mu * (1.0 + sp * sp);
+  const double r_l = 4.0 * lame * sp * sp + mu * (1.0 + sp) * (1.0 + sp) + 2.0 * mu * (1.0 - sp) * (1.0 - sp);
+  const double r_r = 4.0 * lame * sp * sp + 2.0 * mu * (1.0 + sp) * (1.0 + sp) + mu * (1.0 - sp) * (1.0 - sp);
+  const double r_a = 4.0 * K * sp * sp;
+  const double d_s = safe_denom(r_s, tiny), d_l = safe_denom(r_l, tiny), d_r = safe_denom(r_r, tiny),
+               d_a = safe_denom(r_a, tiny);
   // linear forms n = a.z - c over z = (l1, l2, l3, I1)
   const double as[4] = {2.0 * mu * (1.0 + sp), 0.0, -2.0 * mu * (1.0 - sp), 2.0 * lame * sp};
   const double al[4] = {mu * (1.0 + sp), mu * (1.0 + sp), -2.0 * mu * (1.0 - sp), 2.0 * lame * sp};
@@ -136,19 +141,22 @@ FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K
     if (i != j) Fzz[j][i] += coef;
   };
   const double z[4] = {l1, l2, l3, I1};
-  auto add_neg_sq = [&](const double a[4], double d) {  // - n^2 / (2 d), n = a.z - c
-    const double n = lin(a);
-    psi -= 0.5 * n * n / d;
+  // - d/2 (n / ds)^2 with n = a.z - c, d the raw denominator and ds its
+  // guarded copy (the reference's form: where |d| < tiny the term is
+  // d/2 (n/tiny)^2, vanishing with d, not n^2 / (2 tiny))
+  auto add_neg_sq = [&](const double a[4], double d, double ds) {
+    const double n = lin(a), r = d / (ds * ds);
+    psi -= 0.5 * r * n * n;
     for (int i = 0; i < 4; ++i) {
-      Fz[i] -= n / d * a[i];
-      for (int j = 0; j < 4; ++j) Fzz[i][j] -= a[i] * a[j] / d;
+      Fz[i] -= r * n * a[i];
+      for (int j = 0; j < 4; ++j) Fzz[i][j] -= r * a[i] * a[j];
     }
   };
   if (br == 4) {
     psi = 0.5 * K * I1 * I1;
     Fz[3] += K * I1;
     add_quad(3, 3, K);
-    add_neg_sq(aa, d_a);
+    add_neg_sq(aa, r_a, d_a);
   } else {
     psi = 0.5 * lame * I1 * I1;
     Fz[3] += lame * I1;
@@ -156,7 +164,7 @@ FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K
     if (br <= 1) {
       psi += mu * Qv;
       wQ = mu;
-      if (br == 1) add_neg_sq(as, d_s);
+      if (br == 1) add_neg_sq(as, r_s, d_s);
     } else if (br == 2) {  // mu (l3^2 + (l1 + l2)^2 / 2)
       psi += mu * (l3 * l3 + 0.5 * (l1 + l2) * (l1 + l2));
       Fz[2] += 2.0 * mu * l3;
@@ -166,7 +174,7 @@ FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K
       add_quad(0, 0, mu);
       add_quad(1, 1, mu);
       add_quad(0, 1, mu);
-      add_neg_sq(al, d_l);
+      add_neg_sq(al, r_l, d_l);
     } else {  // mu (l1^2 + (l2 + l3)^2 / 2)
       psi += mu * (l1 * l1 + 0.5 * (l2 + l3) * (l2 + l3));
       Fz[0] += 2.0 * mu * l1;
@@ -176,7 +184,7 @@ FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K
       add_quad(1, 1, mu);
       add_quad(2, 2, mu);
       add_quad(1, 2, mu);
-      add_neg_sq(ar, d_r);
+      add_neg_sq(ar, r_r, d_r);
     }
   }
   (void)z;
@@ -205,9 +213,16 @@ FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K
       double s = (m == n) ? wQ * (m < 3 ? 2.0 : 1.0) : 0.0;
       for (int a = 0; a < 4; ++a)
         for (int b = 0; b < 4; ++b) s += Fzz[a][b] * dz[a][m] * dz[b][n];
-      for (int k = 0; k < 3; ++k)
-        for (int j = 0; j < 3; ++j)
-          if (j != k) s += Fz[k] * 2.0 * X[k][j][m] * X[j][k][n] / (lam[k] - lam[j]);
+      // eigenvalue curvature, one term per pair k < j (X[k][j] = X[j][k]):
+      // 2 (Fz_k - Fz_j) / (lambda_k - lambda_j) X_kj[m] X_kj[n].  Summing the
+      // pair once avoids the cancellation of two ~1/(lambda_k - lambda_j)
+      // terms; a pair with Fz_k == Fz_j, or with coincident eigenvalues
+      // (tie-break absorbed), contributes 0 instead of 0/0.
+      for (int k = 0; k < 2; ++k)
+        for (int j = k + 1; j < 3; ++j) {
+          const double dF = Fz[k] - Fz[j], dl = lam[k] - lam[j];
+          if (dF != 0.0 && dl != 0.0) s += 2.0 * dF / dl * X[k][j][m] * X[k][j][n];
+        }
       D[m][n] = s;
     }
   return br;

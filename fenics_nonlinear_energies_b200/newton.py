@@ -34,40 +34,46 @@ from fenics_nonlinear_energies_b200 import _lib
 
 
 def golden_section_search(f, a, b, tol):
-    """Minimise ``f`` on ``[a, b]``; returns ``(alpha, n_evals)``."""
-    gamma = 0.5 + math.sqrt(5.0) / 2.0
-    an, bn = float(a), float(b)
-    fan, fbn = f(an), f(bn)
-    dn = (bn - an) / gamma + an
-    cn = an + bn - dn
-    fcn, fdn = f(cn), f(dn)
+    """Minimise ``f`` on ``[a, b]``; returns ``(alpha, n_evals)``.
+
+    Golden-section bracketing in the reference's evaluation order
+    (``core/petsc/minimizers.py:14-61``): both ends and both interior points
+    are evaluated first; each step keeps the sub-bracket around the smaller
+    interior value and evaluates one new interior point; the smallest value
+    seen anywhere is tracked; the bracket's midpoint is evaluated last.
+    """
+    ratio = 0.5 + math.sqrt(5.0) / 2.0
+    lo, hi = float(a), float(b)
+    f_lo, f_hi = f(lo), f(hi)
+    right = (hi - lo) / ratio + lo
+    left = lo + hi - right
+    f_left, f_right = f(left), f(right)
     n_evals = 4
-    best_alpha, best_value = an, fan
-    for alpha, value in ((bn, fbn), (cn, fcn), (dn, fdn)):
-        if value < best_value:
-            best_alpha, best_value = alpha, value
-    while bn - an > tol:
-        if fcn < fdn:
-            bn = dn
-            dn, cn = cn, an + bn - cn
-            fdn, fcn = fcn, f(cn)
-            for alpha, value in ((dn, fdn), (cn, fcn)):
-                if value < best_value:
-                    best_alpha, best_value = alpha, value
-        else:
-            an = cn
-            cn, dn = dn, an + bn - dn
-            fcn, fdn = fdn, f(dn)
-            for alpha, value in ((cn, fcn), (dn, fdn)):
-                if value < best_value:
-                    best_alpha, best_value = alpha, value
+    arg_min, f_min = lo, f_lo
+    for t, ft in ((hi, f_hi), (left, f_left), (right, f_right)):
+        if ft < f_min:
+            arg_min, f_min = t, ft
+    while hi - lo > tol:
+        if f_left < f_right:  # minimum in [lo, right]: old left becomes the right point
+            hi = right
+            right, left = left, lo + hi - left
+            f_right, f_left = f_left, f(left)
+            fresh = ((right, f_right), (left, f_left))
+        else:  # minimum in [left, hi]: old right becomes the left point
+            lo = left
+            left, right = right, lo + hi - right
+            f_left, f_right = f_right, f(right)
+            fresh = ((left, f_left), (right, f_right))
+        for t, ft in fresh:
+            if ft < f_min:
+                arg_min, f_min = t, ft
         n_evals += 1
-    mid = 0.5 * (an + bn)
-    fmid = f(mid)
+    mid = 0.5 * (lo + hi)
+    f_mid = f(mid)
     n_evals += 1
-    if fmid < best_value:
-        best_alpha = mid
-    return float(best_alpha), n_evals
+    if f_mid < f_min:
+        arg_min = mid
+    return float(arg_min), n_evals
 
 
 def repair_linesearch_interval(f, a, b, center=0.0, center_value=None, tol=1e-6, max_bisect=60):

@@ -254,9 +254,12 @@ int fne_destroy(fne_handle* h);
  * Scratch: a fixed device array inside libfne_asm.so (1024 FP64 partial sums
  * and a ticket, ~8 KB per GPU, held until the process exits); the grid is
  * capped at 1024 CTAs, so any n_elem up to 2^31-1 fits and larger sizes are
- * rejected with FNE_EBOUNDS.  The first call on a device looks the array's
- * address up (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other
+ * rejected with FNE_EBOUNDS.  Every call looks the array's device address up
+ * with cudaGetSymbolAddress on the current device (so an address made stale
+ * by cudaDeviceReset is never reused); the first call on a device may load
+ * the library's device code, so make that first call before any stream
+ * capture.  All calls share the array and it keeps the last call's contents
+ * (the ticket is cleared by each call): calls that overlap on the GPU (other
  * streams, other threads) race and must be serialised by the caller.  No
  * cudaMalloc, cudaFree or allocating library routine is called.
  */

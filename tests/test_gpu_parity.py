@@ -168,6 +168,25 @@ def test_autograd_energy_function():
     np.testing.assert_allclose(u.grad.cpu().numpy(), ref.gradient_fn(u0), rtol=0, atol=1e-12 * np.abs(ref.gradient_fn(u0)).max())
 
 
+def test_autograd_energy_function_rank_split():
+    """Two ranks' EnergyFunction gradients are shaped like u and sum to dJ/du."""
+    from types import SimpleNamespace
+
+    from fenics_nonlinear_energies_b200.assembler import GLCudaAssembler, energy
+
+    params, u0 = meshes.gl_problem(n=24, seed=3)
+    ref = OracleAssembler("gl", params)
+    total = np.zeros_like(u0)
+    for r in range(2):
+        gpu = GLCudaAssembler(params, SimpleNamespace(rank=r, size=2))
+        u = torch.as_tensor(u0, device="cuda").requires_grad_(True)
+        energy(u, gpu).backward()
+        assert u.grad.shape == u.shape
+        total += u.grad.cpu().numpy()
+    g_ref = ref.gradient_fn(u0)
+    np.testing.assert_allclose(total, g_ref, rtol=0, atol=1e-12 * np.abs(g_ref).max())
+
+
 def test_empty_and_tiny_meshes():
     # 1x1 grid: no free DOF at all; 2x2 grid: a single free node
     for n in (1, 2):

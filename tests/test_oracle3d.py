@@ -342,3 +342,63 @@ def test_device_element_function_on_host(mc3d_host):
         assert abs(e - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
         np.testing.assert_allclose(g, g_ref, rtol=1e-9, atol=1e-10 * np.abs(g_ref).max())
         np.testing.assert_allclose(H, H_ref, rtol=1e-7, atol=1e-9 * np.abs(H_ref).max())
+
+
+def test_device_point_zero_friction(mc3d_host):
+    """sin_phi = 0 (Tresca limit): the apex denominator 4 K sin^2(phi) is 0
+    and every return term is written as the reference writes it,
+    -d/2 (n / guarded d)^2, so a zero denominator weights its term by 0.
+    At sin_phi = 0 the branch tests never select the apex (the edge returns
+    always hold); every branch that is reached matches the oracle."""
+    rng = np.random.default_rng(11)
+    n = 3000
+    eps = rng.standard_normal((n, 6)) * 10 ** rng.uniform(-5, -2, size=(n, 1))
+    eps[:, :3] += rng.uniform(-5, 5, size=(n, 1)) * 10 ** rng.uniform(-5, -2, size=(n, 1))
+    c = 10 ** rng.uniform(-3, 1.5, size=n)
+    psi_ref, br = E3.mc_density(eps, c, np.zeros(n), SHEAR, BULK, LAME)
+    assert set(np.unique(br)) == {0, 1, 2, 3}
+    scale = LAME + 2.0 * SHEAR
+    for branch in (0, 1, 2, 3):
+        for i in np.flatnonzero(br == branch)[:4]:
+            b, psi, sig, D = mc3d_host(eps[i], c[i], 0.0, SHEAR, BULK, LAME)
+            assert b == branch
+            assert abs(psi - psi_ref[i]) <= 1e-12 * max(1.0, abs(psi_ref[i]))
+            sig_a, D_a, _, _ = E3.mc_stress_tangent(eps[i][None], c[i], 0.0, SHEAR, BULK, LAME)
+            np.testing.assert_allclose(sig, sig_a[0], rtol=1e-9, atol=1e-11 * scale * np.abs(eps[i]).max())
+            np.testing.assert_allclose(D, D_a[0], rtol=1e-7, atol=1e-9 * scale)
+
+
+@pytest.mark.parametrize("branch", [2, 3])
+def test_device_point_near_degenerate_edges(mc3d_host, branch):
+    """Edge returns with the two eigenvalues of the edge equal up to the
+    reference's 1e-15 tie-break: the pair-summed eigenvalue curvature keeps
+    D finite and symmetric, and D matches central differences of the
+    oracle's stress."""
+    rng = np.random.default_rng(12 + branch)
+    found = 0
+    for _ in range(20000):
+        a, b = sorted(rng.uniform(-2e-3, 4e-3, size=2))[::-1]
+        eps = np.array([a, a, b, 0.0, 0.0, 0.0]) if branch == 2 else np.array([a, b, b, 0.0, 0.0, 0.0])
+        c = rng.uniform(0.1, 20.0)
+        sp = rng.uniform(0.2, 0.7)
+        _, br = E3.mc_density(eps[None], c, sp, SHEAR, BULK, LAME)
+        if br[0] != branch:
+            continue
+        bb, psi, sig, D = mc3d_host(eps, c, sp, SHEAR, BULK, LAME)
+        assert bb == branch
+        assert np.isfinite(D).all()
+        np.testing.assert_allclose(D, D.T, rtol=0, atol=1e-9 * np.abs(D).max())
+        h = 1e-8 * max(1e-3, np.abs(eps).max())
+        Dfd = np.zeros((6, 6))
+        for m in range(6):
+            ep, em = eps.copy(), eps.copy()
+            ep[m] += h
+            em[m] -= h
+            sp_, _, _, _ = E3.mc_stress_tangent(ep[None], c, sp, SHEAR, BULK, LAME)
+            sm_, _, _, _ = E3.mc_stress_tangent(em[None], c, sp, SHEAR, BULK, LAME)
+            Dfd[:, m] = (sp_[0] - sm_[0]) / (2 * h)
+        np.testing.assert_allclose(D, Dfd, rtol=1e-4, atol=1e-5 * np.abs(Dfd).max())
+        found += 1
+        if found == 3:
+            break
+    assert found == 3

@@ -42,8 +42,9 @@ def _soa_inputs(asm, params):
     }
 
 
-def _noalloc_energy(family, n_elem, d, u, scalars, rhs=None, n_owned=0):
-    out = torch.full((1,), float("nan"), dtype=torch.float64, device=u.device)
+def _noalloc_energy(family, n_elem, d, u, scalars, rhs=None, n_owned=0, out=None):
+    if out is None:
+        out = torch.full((1,), float("nan"), dtype=torch.float64, device=u.device)
     sc = (C.c_double * 16)(*scalars)
     stream = torch.cuda.current_stream(u.device).cuda_stream
     _lib.check(_lib.lib.fne_energy_p1tri_noalloc(
@@ -75,9 +76,24 @@ def test_noalloc_energy_matches_fne_eval_twice(family):
     if family == "gl":  # fne_eval adds the Dirichlet-only element energy; the SoA call covers all elements
         all_w = torch.ones_like(d["weights"])
         d = dict(d, weights=all_w)
-    first = _noalloc_energy(fam, len(params["elems"]), d, u, scalars, rhs, n_owned)
-    second = _noalloc_energy(fam, len(params["elems"]), d, u, scalars, rhs, n_owned)
+    n_elem = len(params["elems"])
+    # Warm-up call: the first call on a device may load the library's device code.
+    _noalloc_energy(fam, n_elem, d, u, scalars, rhs, n_owned)
+    first = torch.full((1,), float("nan"), dtype=torch.float64, device=u.device)
+    second = torch.full((1,), float("nan"), dtype=torch.float64, device=u.device)
     torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info(u.device)
+    stats_before = torch.cuda.memory_stats(u.device)
+    _noalloc_energy(fam, n_elem, d, u, scalars, rhs, n_owned, out=first)
+    _noalloc_energy(fam, n_elem, d, u, scalars, rhs, n_owned, out=second)
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info(u.device)
+    stats_after = torch.cuda.memory_stats(u.device)
+    # The defining property: the two calls allocated no device memory, neither
+    # through the driver (free memory unchanged) nor through torch's allocator.
+    assert free_after == free_before, (free_before, free_after)
+    for key in ("allocation.all.allocated", "segment.all.allocated"):
+        assert stats_after.get(key, 0) == stats_before.get(key, 0), key
     scale = max(1.0, abs(ref))
     assert abs(float(first.item()) - ref) <= FP64_TOL * scale, (float(first.item()), ref)
     assert abs(float(second.item()) - ref) <= FP64_TOL * scale, (float(second.item()), ref)
