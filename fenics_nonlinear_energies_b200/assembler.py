@@ -372,11 +372,16 @@ class SlopeStabilityCudaAssembler(CudaElementAssemblerBase):
     (slope_stability/jax_petsc/reordered_element_assembler.py:75-243), plane-strain
     Mohr-Coulomb (``constitutive_mode="mc"``) or linear elastic (``"elastic"``).
 
-    The element operators are passed in affine form (inverse Jacobian,
+    The element operators are passed as the element map (inverse Jacobian,
     ``|det J|`` and the reference-element basis gradients at the quadrature
-    points) instead of the reference's stored ``elem_B``; for straight-sided
-    triangles both give the same strains.  The load vector is the gravity
-    ``force`` restricted to the owned DOFs.
+    points) instead of the reference's stored ``elem_B``: one map per element
+    (``inv_jac (E, 4)``, ``det_j (E,)``; P4, affine), or one per quadrature
+    point (``(E, nq, 4)``, ``(E, nq)``; the isoparametric P2 map).  Without
+    ``inv_jac`` the per-point map is recovered from the reference's
+    ``elem_B`` / ``quad_weight`` (``meshes.geometry_from_elem_B``), so the
+    reference's own problem data can be passed as is (it must then also
+    carry ``dhat1``, ``dhat2`` and ``quad_w``).  The load vector is the
+    gravity ``force`` restricted to the owned DOFs.
     """
 
     family = _lib.FNE_MOHR_COULOMB
@@ -390,19 +395,31 @@ class SlopeStabilityCudaAssembler(CudaElementAssemblerBase):
         self.npe = int(np.asarray(params["elems_scalar"]).shape[1])
         super().__init__(params, comm, adjacency, **kw)
 
+    def _geometry(self):
+        p = self.params
+        if "inv_jac" in p:
+            return np.asarray(p["inv_jac"], dtype=np.float64), np.asarray(p["det_j"], dtype=np.float64)
+        from fenics_nonlinear_energies_b200.meshes import geometry_from_elem_B
+
+        return geometry_from_elem_B(np.asarray(p["elem_B"], dtype=np.float64),
+                                    np.asarray(p["quad_weight"], dtype=np.float64),
+                                    np.asarray(p["dhat1"]), np.asarray(p["dhat2"]), np.asarray(p["quad_w"]))
+
     def _element_arrays(self):
         p = self.params
         epsp = np.asarray(p["eps_p_old"], dtype=np.float64)
         tables = np.concatenate((np.ravel(p["dhat1"]), np.ravel(p["dhat2"]), np.ravel(p["quad_w"])))
-        return [np.asarray(p["inv_jac"]), np.asarray(p["det_j"]), epsp if np.any(epsp) else None, tables]
+        inv, det = self._geometry()
+        return [inv, det, epsp if np.any(epsp) else None, tables]
 
     def _nq(self):
         return int(np.asarray(self.params["quad_w"]).size)
 
     def _scalars(self):
         p = self.params
+        per_point = 1.0 if self._geometry()[1].ndim == 2 else 0.0
         return [float(p["E"]), float(p["nu"]), float(p["phi_deg"]), float(p["cohesion"]),
-                float(p.get("reg", 1.0e-12)), 1.0 if self.constitutive_mode == "elastic" else 0.0]
+                float(p.get("reg", 1.0e-12)), 1.0 if self.constitutive_mode == "elastic" else 0.0, per_point]
 
     # ---- matrix-free Hessian products -----------------------------------------
     # prepare_matrix_free_operator / matrix_free_mult / matrix_free_get_diagonal

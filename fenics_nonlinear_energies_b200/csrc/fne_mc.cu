@@ -8,8 +8,10 @@
 // with sigma = dpsi/deps (the returned stress) and C = dsigma/deps (the
 // consistent tangent of the line / apex return), written by hand instead of
 // JAX's autodiff through lax.cond.  B_q is rebuilt on the fly from the
-// affine element map: B_q = (reference basis gradients at q) x J^-1, so the
-// element data is 5 numbers instead of the reference's nq x 3 x 2n elem_B.
+// element map: B_q = (reference basis gradients at q) x J^-1, so the element
+// data is 5 numbers (affine map: J^-1 and |det J|) -- or 5 per quadrature
+// point for the isoparametric P2 map (GQ kernels) -- instead of the
+// reference's nq x 3 x 2n elem_B.
 //
 // Three kernels: k_mc_elem (one warp per element: nodal values and basis
 // gradients staged in shared memory, one lane per quadrature point for the
@@ -169,7 +171,7 @@ constexpr int kMcWarps = 4;  // elements per CTA (one warp each)
 struct McArgs {
   int n_el;
   const int* __restrict__ codes;     // [n_el * n] per-DOF gather codes
-  const double* __restrict__ geom;   // [n_el * 5] J^-1 (4), |det J|
+  const double* __restrict__ geom;   // [n_el * 5] J^-1 (4), |det J|; GQ kernels [n_el * nq * 5]
   const double* __restrict__ epsp;   // [n_el * nq * 3] or null
   const unsigned char* __restrict__ wflag;  // [n_el]
   const double* __restrict__ dhat1;  // [nq * np]
@@ -182,7 +184,11 @@ struct McArgs {
   long long lo;
 };
 
-template <typename Real, int NP, int NQ, int WANT>
+// Geometry values per element: 5 (affine map) or 5 per quadrature point (GQ).
+template <int NQ, bool GQ>
+__host__ __device__ constexpr int geo_stride() { return GQ ? 5 * NQ : 5; }
+
+template <typename Real, int NP, int NQ, int WANT, bool GQ>
 __global__ void __launch_bounds__(32 * kMcWarps) k_mc_elem(McArgs A, McConstR<Real> M, Real* __restrict__ Kbuf,
                                                            Real* __restrict__ gbuf, double* __restrict__ partials,
                                                            unsigned* __restrict__ counter, double* __restrict__ eout) {
@@ -210,16 +216,15 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_elem(McArgs A, McConstR<Re
   double eacc = 0.0;
   const int gwarps = gridDim.x * kMcWarps;
   for (int e = blockIdx.x * kMcWarps + wid; e < A.n_el; e += gwarps) {
-    const double* gm = A.geom + 5LL * e;
-    const Real i00 = (Real)gm[0], i01 = (Real)gm[1], i10 = (Real)gm[2], i11 = (Real)gm[3];
-    const Real dj = (Real)gm[4];
+    const double* gm = A.geom + (long long)geo_stride<NQ, GQ>() * e;
     for (int i = lane; i < N; i += 32) {
       const int code = A.codes[(long long)e * N + i];
       ue[i] = (Real)(code >= 0 ? A.u[code] : A.dir[-1 - code]);
     }
     for (int i = lane; i < NQ * NP; i += 32) {
-      gx[i] = i00 * s_dh1[i] + i01 * s_dh2[i];
-      gy[i] = i10 * s_dh1[i] + i11 * s_dh2[i];
+      const double* g = GQ ? gm + 5 * (i / NP) : gm;
+      gx[i] = (Real)g[0] * s_dh1[i] + (Real)g[1] * s_dh2[i];
+      gy[i] = (Real)g[2] * s_dh1[i] + (Real)g[3] * s_dh2[i];
     }
     __syncwarp();
     if (lane < NQ) {  // constitutive update, one lane per quadrature point
@@ -240,7 +245,7 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_elem(McArgs A, McConstR<Re
       }
       Real sig[3], Ct[6], psi;
       mc_point(M, eps, sig, Ct, psi);
-      const Real w = dj * s_w[q];
+      const Real w = (Real)gm[GQ ? 5 * q + 4 : 4] * s_w[q];
 #pragma unroll
       for (int k = 0; k < 3; ++k) ws[q * 3 + k] = w * sig[k];
 #pragma unroll
@@ -335,7 +340,7 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_elem(McArgs A, McConstR<Re
 // K_e; the element vectors are summed per owned row by k_rowgrad.  One warp
 // per element, one lane per quadrature point, then one lane per element DOF.
 // ---------------------------------------------------------------------------
-template <typename Real, int NP, int NQ>
+template <typename Real, int NP, int NQ, bool GQ>
 __global__ void __launch_bounds__(32 * kMcWarps) k_mc_lin(McArgs A, McConstR<Real> M, Real* __restrict__ wct) {
   constexpr int N = 2 * NP;
   __shared__ Real s_dh1[NQ * NP], s_dh2[NQ * NP], s_w[NQ];
@@ -349,8 +354,6 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_lin(McArgs A, McConstR<Rea
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   Real* ue = s_u[wid];
   for (int e = blockIdx.x * kMcWarps + wid; e < A.n_el; e += gridDim.x * kMcWarps) {
-    const double* gm = A.geom + 5LL * e;
-    const Real i00 = (Real)gm[0], i01 = (Real)gm[1], i10 = (Real)gm[2], i11 = (Real)gm[3], dj = (Real)gm[4];
     for (int i = lane; i < N; i += 32) {
       const int code = A.codes[(long long)e * N + i];
       ue[i] = (Real)(code >= 0 ? A.u[code] : A.dir[-1 - code]);
@@ -358,6 +361,8 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_lin(McArgs A, McConstR<Rea
     __syncwarp();
     if (lane < NQ) {
       const int q = lane;
+      const double* gm = A.geom + (long long)geo_stride<NQ, GQ>() * e + (GQ ? 5 * q : 0);
+      const Real i00 = (Real)gm[0], i01 = (Real)gm[1], i10 = (Real)gm[2], i11 = (Real)gm[3], dj = (Real)gm[4];
       Real ex = Real(0), ey = Real(0), exy = Real(0);
       for (int a = 0; a < NP; ++a) {
         const Real r1 = s_dh1[q * NP + a], r2 = s_dh2[q * NP + a];
@@ -384,7 +389,7 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_lin(McArgs A, McConstR<Rea
   }
 }
 
-template <typename Real, int NP, int NQ, bool DIAG>
+template <typename Real, int NP, int NQ, bool DIAG, bool GQ>
 __global__ void __launch_bounds__(32 * kMcWarps) k_mc_hvp(McArgs A, const Real* __restrict__ wct,
                                                           Real* __restrict__ ebuf) {
   constexpr int N = 2 * NP;
@@ -400,8 +405,7 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_hvp(McArgs A, const Real* 
   Real* xe = s_x[wid];
   Real* ss = s_s[wid];
   for (int e = blockIdx.x * kMcWarps + wid; e < A.n_el; e += gridDim.x * kMcWarps) {
-    const double* gm = A.geom + 5LL * e;
-    const Real i00 = (Real)gm[0], i01 = (Real)gm[1], i10 = (Real)gm[2], i11 = (Real)gm[3];
+    const double* gm = A.geom + (long long)geo_stride<NQ, GQ>() * e;
     const Real* wc = wct + (long long)e * NQ * 6;
     if (!DIAG) {
       // tangent direction: free DOFs from x, Dirichlet DOFs zero
@@ -415,6 +419,8 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_hvp(McArgs A, const Real* 
         // B_q x_e = J^-T-weighted z; s = (w C_q) strain; pulled back
         // t[c][l] = sum_i J^-1_il s[v(c,i)], so that y_(a,c) = sum_q sum_l R_qal t[c][l]
         const int q = lane;
+        const double* gq = gm + (GQ ? 5 * q : 0);
+        const Real i00 = (Real)gq[0], i01 = (Real)gq[1], i10 = (Real)gq[2], i11 = (Real)gq[3];
         Real z01 = Real(0), z02 = Real(0), z11 = Real(0), z12 = Real(0);
         for (int a = 0; a < NP; ++a) {
           const Real r1 = s_dh1[q * NP + a], r2 = s_dh2[q * NP + a];
@@ -444,7 +450,8 @@ __global__ void __launch_bounds__(32 * kMcWarps) k_mc_hvp(McArgs A, const Real* 
         const Real r1 = s_dh1[q * NP + a], r2 = s_dh2[q * NP + a];
         if (DIAG) {
           // B column (a, c): c = 0 -> (px, 0, py); c = 1 -> (0, py, px)
-          const Real px = i00 * r1 + i01 * r2, py = i10 * r1 + i11 * r2;
+          const double* gq = gm + (GQ ? 5 * q : 0);
+          const Real px = (Real)gq[0] * r1 + (Real)gq[1] * r2, py = (Real)gq[2] * r1 + (Real)gq[3] * r2;
           const Real* C = wc + q * 6;
           acc += c == 0 ? px * (C[0] * px + C[2] * py) + py * (C[2] * px + C[5] * py)
                         : py * (C[3] * py + C[4] * px) + px * (C[4] * py + C[5] * px);
@@ -553,8 +560,9 @@ __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__flo
 }  // namespace tc
 
 // Tile geometry of the tensor-core kernel for (NP, NQ).
-template <int NP, int NQ>
+template <int NP, int NQ, bool GQ = false>
 struct McTile {
+  static constexpr int GS = geo_stride<NQ, GQ>();   // geometry values per element
   static constexpr int NPAIR = NP * (NP + 1) / 2;
   static constexpr int KK = 4 * NQ;                 // (q, k, l)
   static constexpr int KP = (KK + 7) / 8 * 8;       // padded to the MMA K step (8 tf32)
@@ -571,8 +579,8 @@ struct McTile {
   static constexpr int OFF_S = 2 * A_BYTES + 2 * B_BYTES;          // [NQ][TE][4] gradient helper
   static constexpr int OFF_R = OFF_S + TE * NQ * 16;                // dh1, dh2 [NQ * NP], qw [NQ]
   static constexpr int OFF_U = OFF_R + ((2 * NQ * NP + NQ) * 4 + 15) / 16 * 16;  // [TE][2 NP]
-  static constexpr int OFF_G = OFF_U + (TE * 2 * NP * 4 + 15) / 16 * 16;          // [TE][5]
-  static constexpr int OFF_PLAN = OFF_G + (TE * 5 * 4 + 15) / 16 * 16;            // [TE][NP * NP] uint16 codes
+  static constexpr int OFF_G = OFF_U + (TE * 2 * NP * 4 + 15) / 16 * 16;          // [TE][GS]
+  static constexpr int OFF_PLAN = OFF_G + (TE * GS * 4 + 15) / 16 * 16;           // [TE][NP * NP] uint16 codes
   static constexpr int PLAN_WORDS = (TE * NP * NP + 1) / 2;                       // as uint32 words
   static constexpr int OFF_ROW = OFF_PLAN + (PLAN_WORDS * 4 + 15) / 16 * 16;      // [TE][NP][2] row starts
   static constexpr int OFF_SB = OFF_ROW + (TE * NP * 2 * 4 + 15) / 16 * 16;       // [TE] shared-slot bases
@@ -598,14 +606,15 @@ struct McTcArgs {
   float* sbuf;
 };
 
-template <int NP, int NQ, int WANT, typename HOut>
-__global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_BLOCKS)
+template <int NP, int NQ, int WANT, typename HOut, bool GQ>
+__global__ void __launch_bounds__(McTile<NP, NQ, GQ>::THREADS, McTile<NP, NQ, GQ>::MIN_BLOCKS)
     k_mc_tc(McArgs A, McConstR<float> C, McTcArgs T, HOut* __restrict__ hout, float* __restrict__ gbuf,
             double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ eout) {
-  using G = McTile<NP, NQ>;
+  using G = McTile<NP, NQ, GQ>;
   constexpr int N2 = 2 * NP, TE = G::TE, N = G::N, M = G::M, KP = G::KP, NPAIR = G::NPAIR, NT = G::THREADS;
+  constexpr int GS = G::GS;
   constexpr int UPT = (TE * N2 + NT - 1) / NT;  // nodal values per thread (prefetch)
-  constexpr int GPT = (TE * 5 + NT - 1) / NT;   // geometry values per thread (prefetch)
+  constexpr int GPT = (TE * GS + NT - 1) / NT;  // geometry values per thread (prefetch)
   extern __shared__ __align__(1024) unsigned char smem[];
   float* sAhi = reinterpret_cast<float*>(smem + G::OFF_AHI);
   float* sAlo = reinterpret_cast<float*>(smem + G::OFF_ALO);
@@ -678,10 +687,10 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
     }
 #pragma unroll
     for (int k = 0; k < GPT; ++k) {
-      const int i = tid + k * NT, el = i / 5;
+      const int i = tid + k * NT, el = i / GS;
       const int e = tile * TE + el;
-      gv[k] = (tile < n_tiles && i < TE * 5 && e < A.n_el) ? (float)__ldg(A.geom + (long long)tile * TE * 5 + i)
-                                                           : 0.f;
+      gv[k] = (tile < n_tiles && i < TE * GS && e < A.n_el) ? (float)__ldg(A.geom + (long long)tile * TE * GS + i)
+                                                            : 0.f;
     }
     if (WANT & MW_H) {
       const int ne_t = tile < n_tiles ? min(TE, A.n_el - tile * TE) : 0;
@@ -721,7 +730,7 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
       if (tid + k * NT < TE * N2) sU[tid + k * NT] = uv[k];
 #pragma unroll
     for (int k = 0; k < GPT; ++k)
-      if (tid + k * NT < TE * 5) sGm[tid + k * NT] = gv[k];
+      if (tid + k * NT < TE * GS) sGm[tid + k * NT] = gv[k];
     if (WANT & MW_H) {
 #pragma unroll
       for (int k = 0; k < WPT; ++k)
@@ -752,7 +761,7 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
       float4 at[4];  // (c, d) blocks j = c * 2 + d: [k * 2 + l]
       float4 sg = make_float4(0.f, 0.f, 0.f, 0.f);
       if (el < ne) {
-        const float* gm = sGm + el * 5;
+        const float* gm = sGm + el * GS + (GQ ? 5 * q : 0);
         const float i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
         const float* ue = sU + el * N2;
         float gx1 = 0.f, gx2 = 0.f, gy1 = 0.f, gy2 = 0.f;  // reference-gradient contractions
@@ -957,7 +966,7 @@ __global__ void __launch_bounds__(McTile<NP, NQ>::THREADS, McTile<NP, NQ>::MIN_B
 // ---------------------------------------------------------------------------
 constexpr int kEgTile = 32, kEgThreads = 256;
 
-template <typename Real, int NP, int NQ, int WANT>
+template <typename Real, int NP, int NQ, int WANT, bool GQ>
 __global__ void __launch_bounds__(kEgThreads) k_mc_eg(McArgs A, McConstR<Real> M, Real* __restrict__ gbuf,
                                                       double* __restrict__ partials, unsigned* __restrict__ counter,
                                                       double* __restrict__ eout) {
@@ -965,7 +974,8 @@ __global__ void __launch_bounds__(kEgThreads) k_mc_eg(McArgs A, McConstR<Real> M
   constexpr int US = N2 + 1;  // odd row stride of the staged nodal values: no bank conflicts
   __shared__ Real sD1[NQ * NP], sD2[NQ * NP], sW[NQ];
   __shared__ Real sU[TE * US];
-  __shared__ Real sGm[TE * 5];
+  constexpr int GS = geo_stride<NQ, GQ>();
+  __shared__ Real sGm[TE * GS];
   __shared__ Real sS[(WANT & MW_G) ? NQ * TE * 4 : 1];
   const int tid = threadIdx.x;
   for (int i = tid; i < NQ * NP; i += NT) {
@@ -983,12 +993,12 @@ __global__ void __launch_bounds__(kEgThreads) k_mc_eg(McArgs A, McConstR<Real> M
       const int code = __ldg(A.codes + (long long)e0 * N2 + i);
       sU[(i / N2) * US + i % N2] = (Real)(code >= 0 ? __ldg(A.u + code) : __ldg(A.dir + (-1 - code)));
     }
-    for (int i = tid; i < ne * 5; i += NT) sGm[i] = (Real)__ldg(A.geom + (long long)e0 * 5 + i);
+    for (int i = tid; i < ne * GS; i += NT) sGm[i] = (Real)__ldg(A.geom + (long long)e0 * GS + i);
     __syncthreads();
     for (int p = tid; p < TE * NQ; p += NT) {
       const int q = p / TE, el = p - q * TE;
       if (el >= ne) continue;
-      const Real* gm = sGm + el * 5;
+      const Real* gm = sGm + el * GS + (GQ ? 5 * q : 0);
       const Real i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
       const Real* ue = sU + el * US;
       // reference-gradient contractions first (4 multiply-adds per node),
@@ -1059,8 +1069,9 @@ __global__ void __launch_bounds__(kEgThreads) k_mc_eg(McArgs A, McConstR<Real> M
 // and writes its blocks; the element gradient follows on the CUDA cores.
 // Two CTAs per SM, so one CTA's return map overlaps the other's MMAs.
 // ---------------------------------------------------------------------------
-template <int NP, int NQ>
+template <int NP, int NQ, bool GQ = false>
 struct McTileD {
+  static constexpr int GS = geo_stride<NQ, GQ>();        // geometry values per element
   static constexpr int NPAIR = NP * (NP + 1) / 2;
   static constexpr int MT = (NPAIR + 15) / 16;          // m16 tiles of node pairs
   static constexpr int KK = 4 * NQ;                      // (q, k, l)
@@ -1076,8 +1087,8 @@ struct McTileD {
   static constexpr int OFF_S = OFF_B + R16(KK * NS * 8);             // [NQ][TE] 4 doubles
   static constexpr int OFF_R = OFF_S + NQ * TE * 32;                 // dh1, dh2 [NQ * NP], qw [NQ]
   static constexpr int OFF_U = OFF_R + R16((2 * NQ * NP + NQ) * 8);  // [TE][2 NP]
-  static constexpr int OFF_G = OFF_U + R16(TE * 2 * NP * 8);         // [TE][5]
-  static constexpr int OFF_PLAN = OFF_G + R16(TE * 5 * 8);           // [TE][NP * NP] uint16 codes
+  static constexpr int OFF_G = OFF_U + R16(TE * 2 * NP * 8);         // [TE][GS]
+  static constexpr int OFF_PLAN = OFF_G + R16(TE * GS * 8);          // [TE][NP * NP] uint16 codes
   static constexpr int PLAN_WORDS = (TE * NP * NP + 1) / 2;
   static constexpr int OFF_ROW = OFF_PLAN + R16(PLAN_WORDS * 4);     // [TE][NP][2] row starts
   static constexpr int OFF_SB = OFF_ROW + R16(TE * NP * 2 * 4);      // [TE] shared-slot bases
@@ -1098,15 +1109,15 @@ __device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1
                : "d"(a0), "d"(a1), "d"(b0));
 }
 
-template <int NP, int NQ, int WANT>
-__global__ void __launch_bounds__(McTileD<NP, NQ>::THREADS, McTileD<NP, NQ>::MIN_BLOCKS)
+template <int NP, int NQ, int WANT, bool GQ>
+__global__ void __launch_bounds__(McTileD<NP, NQ, GQ>::THREADS, McTileD<NP, NQ, GQ>::MIN_BLOCKS)
     k_mc_dmma(McArgs A, McConstR<double> C, McDmArgs T, double* __restrict__ hout, double* __restrict__ gbuf,
               double* __restrict__ partials, unsigned* __restrict__ counter, double* __restrict__ eout) {
-  using G = McTileD<NP, NQ>;
+  using G = McTileD<NP, NQ, GQ>;
   constexpr int N2 = 2 * NP, TE = G::TE, NS = G::NS, NPAIR = G::NPAIR, NT = G::THREADS;
-  constexpr int NN = NP * NP;
+  constexpr int NN = NP * NP, GS = G::GS;
   constexpr int UPT = (TE * N2 + NT - 1) / NT;
-  constexpr int GPT = (TE * 5 + NT - 1) / NT;
+  constexpr int GPT = (TE * GS + NT - 1) / NT;
   constexpr int RPT = (TE * NP + NT - 1) / NT;
   constexpr int WPT = (G::PLAN_WORDS + NT - 1) / NT;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1144,9 +1155,9 @@ __global__ void __launch_bounds__(McTileD<NP, NQ>::THREADS, McTileD<NP, NQ>::MIN
     }
 #pragma unroll
     for (int k = 0; k < GPT; ++k) {
-      const int i = tid + k * NT, el = i / 5;
+      const int i = tid + k * NT, el = i / GS;
       const int e = tile * TE + el;
-      gv[k] = (tile < n_tiles && i < TE * 5 && e < A.n_el) ? __ldg(A.geom + (long long)tile * TE * 5 + i) : 0.0;
+      gv[k] = (tile < n_tiles && i < TE * GS && e < A.n_el) ? __ldg(A.geom + (long long)tile * TE * GS + i) : 0.0;
     }
     const int ne_t = tile < n_tiles ? min(TE, A.n_el - tile * TE) : 0;
     const int nw = (ne_t * NN + 1) / 2;
@@ -1182,7 +1193,7 @@ __global__ void __launch_bounds__(McTileD<NP, NQ>::THREADS, McTileD<NP, NQ>::MIN
       if (tid + k * NT < TE * N2) sU[tid + k * NT] = uv[k];
 #pragma unroll
     for (int k = 0; k < GPT; ++k)
-      if (tid + k * NT < TE * 5) sGm[tid + k * NT] = gv[k];
+      if (tid + k * NT < TE * GS) sGm[tid + k * NT] = gv[k];
 #pragma unroll
     for (int k = 0; k < WPT; ++k)
       if (tid + k * NT < G::PLAN_WORDS) sPlanW[tid + k * NT] = pw[k];
@@ -1234,7 +1245,7 @@ __global__ void __launch_bounds__(McTileD<NP, NQ>::THREADS, McTileD<NP, NQ>::MIN
       double at[4][4];
       double2 s01 = make_double2(0.0, 0.0), s23 = make_double2(0.0, 0.0);
       if (el < ne) {
-        const double* gm = sGm + el * 5;
+        const double* gm = sGm + el * GS + (GQ ? 5 * q : 0);
         const double i00 = gm[0], i01 = gm[1], i10 = gm[2], i11 = gm[3];
         const double* ue = sU + el * N2;
         double gx1 = 0.0, gx2 = 0.0, gy1 = 0.0, gy2 = 0.0;  // reference-gradient contractions
@@ -1418,6 +1429,7 @@ struct McHandle {
       *bp_rn_inc = nullptr, *bp_con = nullptr, *bp_inc = nullptr;
   unsigned* bp_blk = nullptr;
   // tensor-core path (FP32, P2 / P4): constant operand halves, status word
+  int gq = 0;  // 1: geometry per quadrature point (isoparametric P2), 5 * nq values per element
   int tc = 0, grid_tc = 1;
   float *Phi = nullptr, *Plo = nullptr;
   int* err = nullptr;
@@ -1495,7 +1507,7 @@ cudaError_t mc_gathers(McHandle* h, int flags, const Real* K, const Real* g, dou
   return cudaGetLastError();
 }
 
-template <typename Real, typename HOut, int NP, int NQ>
+template <typename Real, typename HOut, int NP, int NQ, bool GQ>
 cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, double* grad, void* hess,
                       cudaStream_t st) {
   McArgs A;
@@ -1519,33 +1531,33 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
   const int T = 32 * kMcWarps;
   if constexpr (sizeof(Real) == 4 && NP > 3) {
     if (h->tc && (flags & MW_H)) {
-      using G = McTile<NP, NQ>;
+      using G = McTile<NP, NQ, GQ>;
       McTcArgs T{h->Phi, h->Plo, h->err, h->dp_code, h->dp_sbase, h->dp_elem_rn, h->bp_rn_row,
                  static_cast<float*>(h->dp_sbuf)};
       float* g = static_cast<float*>(h->gbuf);
       HOut* H = static_cast<HOut*>(hess);
       const McConstR<float> Mf = cast_const<float>(h->mc);
       switch (flags) {
-        case 4: k_mc_tc<NP, NQ, 4, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
-        case 5: k_mc_tc<NP, NQ, 5, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
-        case 6: k_mc_tc<NP, NQ, 6, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
-        default: k_mc_tc<NP, NQ, 7, HOut><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
+        case 4: k_mc_tc<NP, NQ, 4, HOut, GQ><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
+        case 5: k_mc_tc<NP, NQ, 5, HOut, GQ><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
+        case 6: k_mc_tc<NP, NQ, 6, HOut, GQ><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
+        default: k_mc_tc<NP, NQ, 7, HOut, GQ><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
       }
       return mc_gathers<float, HOut, NP>(h, flags, static_cast<const float*>(nullptr), g, grad, hess, st);
     }
   }
   if constexpr (sizeof(Real) == 8 && NP > 3) {
     if (h->dm && (flags & MW_H)) {
-      using G = McTileD<NP, NQ>;
+      using G = McTileD<NP, NQ, GQ>;
       McDmArgs T{h->dp_code, h->dp_sbase, h->dp_elem_rn, h->bp_rn_row, static_cast<double*>(h->dp_sbuf)};
       double* g = static_cast<double*>(h->gbuf);
       double* H = static_cast<double*>(hess);
       const McConstR<double> Md = cast_const<double>(h->mc);
       switch (flags) {
-        case 4: k_mc_dmma<NP, NQ, 4><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
-        case 5: k_mc_dmma<NP, NQ, 5><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
-        case 6: k_mc_dmma<NP, NQ, 6><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
-        default: k_mc_dmma<NP, NQ, 7><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
+        case 4: k_mc_dmma<NP, NQ, 4, GQ><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
+        case 5: k_mc_dmma<NP, NQ, 5, GQ><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
+        case 6: k_mc_dmma<NP, NQ, 6, GQ><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
+        default: k_mc_dmma<NP, NQ, 7, GQ><<<h->grid_dm, G::THREADS, G::SMEM, st>>>(A, Md, T, H, g, h->partials, h->counter, energy); break;
       }
       return mc_gathers<double, double, NP>(h, flags, static_cast<const double*>(nullptr), g, grad, hess, st);
     }
@@ -1553,21 +1565,21 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
   if (!(flags & MW_H) && h->use_eg) {  // energy / gradient callbacks
     const int ge = h->grid_eg;
     switch (flags) {
-      case 1: k_mc_eg<Real, NP, NQ, 1><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
-      case 2: k_mc_eg<Real, NP, NQ, 2><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
-      case 3: k_mc_eg<Real, NP, NQ, 3><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
+      case 1: k_mc_eg<Real, NP, NQ, 1, GQ><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
+      case 2: k_mc_eg<Real, NP, NQ, 2, GQ><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
+      case 3: k_mc_eg<Real, NP, NQ, 3, GQ><<<ge, kEgThreads, 0, st>>>(A, M, g, h->partials, h->counter, energy); break;
       default: return cudaErrorInvalidValue;
     }
     return mc_gathers<Real, HOut, NP>(h, flags, K, g, grad, hess, st);
   }
   switch (flags) {
-    case 1: k_mc_elem<Real, NP, NQ, 1><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
-    case 2: k_mc_elem<Real, NP, NQ, 2><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
-    case 3: k_mc_elem<Real, NP, NQ, 3><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
-    case 4: k_mc_elem<Real, NP, NQ, 4><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
-    case 5: k_mc_elem<Real, NP, NQ, 5><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
-    case 6: k_mc_elem<Real, NP, NQ, 6><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
-    case 7: k_mc_elem<Real, NP, NQ, 7><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
+    case 1: k_mc_elem<Real, NP, NQ, 1, GQ><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
+    case 2: k_mc_elem<Real, NP, NQ, 2, GQ><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
+    case 3: k_mc_elem<Real, NP, NQ, 3, GQ><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
+    case 4: k_mc_elem<Real, NP, NQ, 4, GQ><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
+    case 5: k_mc_elem<Real, NP, NQ, 5, GQ><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
+    case 6: k_mc_elem<Real, NP, NQ, 6, GQ><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
+    case 7: k_mc_elem<Real, NP, NQ, 7, GQ><<<grid, T, 0, st>>>(A, M, K, g, h->partials, h->counter, energy); break;
     default: return cudaErrorInvalidValue;
   }
   return mc_gathers<Real, HOut, NP>(h, flags, K, g, grad, hess, st);
@@ -1576,9 +1588,11 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
 template <typename Real, typename HOut>
 cudaError_t mc_dispatch(McHandle* h, int flags, const double* u, double* energy, double* grad, void* hess,
                         cudaStream_t st) {
-  if (h->np == 3 && h->nq == 1) return mc_launch<Real, HOut, 3, 1>(h, flags, u, energy, grad, hess, st);
-  if (h->np == 6 && h->nq == 7) return mc_launch<Real, HOut, 6, 7>(h, flags, u, energy, grad, hess, st);
-  if (h->np == 15 && h->nq == 25) return mc_launch<Real, HOut, 15, 25>(h, flags, u, energy, grad, hess, st);
+  if (h->np == 3 && h->nq == 1) return mc_launch<Real, HOut, 3, 1, false>(h, flags, u, energy, grad, hess, st);
+  if (h->np == 6 && h->nq == 7)
+    return h->gq ? mc_launch<Real, HOut, 6, 7, true>(h, flags, u, energy, grad, hess, st)
+                 : mc_launch<Real, HOut, 6, 7, false>(h, flags, u, energy, grad, hess, st);
+  if (h->np == 15 && h->nq == 25) return mc_launch<Real, HOut, 15, 25, false>(h, flags, u, energy, grad, hess, st);
   return cudaErrorInvalidValue;
 }
 
@@ -1586,9 +1600,9 @@ cudaError_t mc_dispatch(McHandle* h, int flags, const double* u, double* energy,
 // kernel, split into TF32 hi / lo parts and laid out as the kernel's shared
 // memory image ([K / 4][M][4] floats, zero padding); also sizes the grid and
 // opts the kernel into its shared memory.
-template <int NP, int NQ>
+template <int NP, int NQ, bool GQ>
 int mc_tc_prepare(McHandle* h, const double* tables, std::vector<float>& phi, std::vector<float>& plo) {
-  using G = McTile<NP, NQ>;
+  using G = McTile<NP, NQ, GQ>;
   const double* d1 = tables;
   const double* d2 = tables + NQ * NP;
   phi.assign((size_t)G::M * G::KP, 0.f);
@@ -1616,14 +1630,14 @@ int mc_tc_prepare(McHandle* h, const double* tables, std::vector<float>& phi, st
   auto opt_in = [&](const void* f) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
   };
-  opt_in((const void*)k_mc_tc<NP, NQ, 4, float>);
-  opt_in((const void*)k_mc_tc<NP, NQ, 5, float>);
-  opt_in((const void*)k_mc_tc<NP, NQ, 6, float>);
-  opt_in((const void*)k_mc_tc<NP, NQ, 7, float>);
-  opt_in((const void*)k_mc_tc<NP, NQ, 4, double>);
-  opt_in((const void*)k_mc_tc<NP, NQ, 5, double>);
-  opt_in((const void*)k_mc_tc<NP, NQ, 6, double>);
-  opt_in((const void*)k_mc_tc<NP, NQ, 7, double>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 4, float, GQ>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 5, float, GQ>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 6, float, GQ>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 7, float, GQ>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 4, double, GQ>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 5, double, GQ>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 6, double, GQ>);
+  opt_in((const void*)k_mc_tc<NP, NQ, 7, double, GQ>);
   if (e != cudaSuccess)
     return set_error(FNE_ECUDA, std::string("Mohr-Coulomb: tensor-core kernel shared memory: ") +
                                     cudaGetErrorString(e));
@@ -1633,17 +1647,17 @@ int mc_tc_prepare(McHandle* h, const double* tables, std::vector<float>& phi, st
 }
 
 // FP64 DMMA kernel: grid (two CTAs per SM) and the shared-memory opt-in.
-template <int NP, int NQ>
+template <int NP, int NQ, bool GQ>
 int mc_dm_prepare(McHandle* h) {
-  using G = McTileD<NP, NQ>;
+  using G = McTileD<NP, NQ, GQ>;
   cudaError_t e = cudaSuccess;
   auto opt_in = [&](const void* f) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
   };
-  opt_in((const void*)k_mc_dmma<NP, NQ, 4>);
-  opt_in((const void*)k_mc_dmma<NP, NQ, 5>);
-  opt_in((const void*)k_mc_dmma<NP, NQ, 6>);
-  opt_in((const void*)k_mc_dmma<NP, NQ, 7>);
+  opt_in((const void*)k_mc_dmma<NP, NQ, 4, GQ>);
+  opt_in((const void*)k_mc_dmma<NP, NQ, 5, GQ>);
+  opt_in((const void*)k_mc_dmma<NP, NQ, 6, GQ>);
+  opt_in((const void*)k_mc_dmma<NP, NQ, 7, GQ>);
   if (e != cudaSuccess)
     return set_error(FNE_ECUDA, std::string("Mohr-Coulomb: FP64 DMMA kernel shared memory: ") + cudaGetErrorString(e));
   const int n_tiles = (h->n_local + G::TE - 1) / G::TE;
@@ -1677,6 +1691,10 @@ int mc_create(const fne_desc* d, McHandle** out) {
   const int64_t* t2f = d->total_to_free_reord;
   if (E * (int64_t)n * n >= (int64_t)INT32_MAX || d->nnz >= (int64_t)INT32_MAX)
     return set_error(FNE_EBOUNDS, "Mohr-Coulomb: element matrices exceed 32-bit indexing");
+  // s[6] = 1: e0 / e1 hold J^-1 / |det J| per quadrature point (isoparametric map)
+  const bool per_point = d->s[6] != 0.0 && nq > 1;
+  if (per_point && np != 6)
+    return set_error(FNE_EINVAL, "Mohr-Coulomb: per-quadrature-point geometry is supported for P2 (6 nodes) only");
   // per-DOF gather codes and local elements
   std::vector<int32_t> codes;
   std::vector<double> geom, epsp;
@@ -1696,8 +1714,15 @@ int mc_create(const fne_desc* d, McHandle** out) {
       const int64_t dof = d->elems[e * n + i];
       codes.push_back(t2f[dof] >= 0 ? (int32_t)t2f[dof] : (int32_t)(-1 - dof));
     }
-    for (int k = 0; k < 4; ++k) geom.push_back(d->e0[e * 4 + k]);
-    geom.push_back(d->e1[e]);
+    if (per_point) {  // J_q^-1 (4) and |det J_q| per quadrature point
+      for (int q = 0; q < nq; ++q) {
+        for (int k = 0; k < 4; ++k) geom.push_back(d->e0[(e * nq + q) * 4 + k]);
+        geom.push_back(d->e1[e * nq + q]);
+      }
+    } else {
+      for (int k = 0; k < 4; ++k) geom.push_back(d->e0[e * 4 + k]);
+      geom.push_back(d->e1[e]);
+    }
     if (d->e2)
       for (int k = 0; k < nq * 3; ++k) epsp.push_back(d->e2[e * nq * 3 + k]);
     const double w = d->energy_weights ? d->energy_weights[e] : 1.0;
@@ -1800,6 +1825,7 @@ int mc_create(const fne_desc* d, McHandle** out) {
   h->hess_fp32 = d->precision == FNE_FP32 && d->hess_fp32;
   h->np = np;
   h->nq = nq;
+  h->gq = per_point ? 1 : 0;
   h->n = n;
   h->n_local = (int)nl;
   h->n_rows = use_blk ? (int32_t)n_owned : n_rows;
@@ -1905,7 +1931,8 @@ int mc_create(const fne_desc* d, McHandle** out) {
     MC_TRY(mc_upload(h, &h->fx_desc, dp.fdesc.data(), dp.fdesc.size()));
   }
   if (h->dm) {
-    const int rc_dm = np == 15 ? mc_dm_prepare<15, 25>(h) : mc_dm_prepare<6, 7>(h);
+    const int rc_dm = np == 15 ? mc_dm_prepare<15, 25, false>(h)
+                               : (h->gq ? mc_dm_prepare<6, 7, true>(h) : mc_dm_prepare<6, 7, false>(h));
     if (rc_dm) {
       mc_destroy(h);
       return rc_dm;
@@ -1913,7 +1940,9 @@ int mc_create(const fne_desc* d, McHandle** out) {
   }
   if (h->tc) {
     std::vector<float> phi, plo;
-    int rc_tc = np == 15 ? mc_tc_prepare<15, 25>(h, d->e3, phi, plo) : mc_tc_prepare<6, 7>(h, d->e3, phi, plo);
+    int rc_tc = np == 15 ? mc_tc_prepare<15, 25, false>(h, d->e3, phi, plo)
+                         : (h->gq ? mc_tc_prepare<6, 7, true>(h, d->e3, phi, plo)
+                                  : mc_tc_prepare<6, 7, false>(h, d->e3, phi, plo));
     if (rc_tc) {
       mc_destroy(h);
       return rc_tc;
@@ -1953,8 +1982,8 @@ int mc_set_dirichlet(McHandle* h, const double* dirichlet) {
 
 namespace {
 
-template <typename Real, int NP, int NQ>
-cudaError_t mc_lin_launch(McHandle* h, int op, const double* v, double* out, cudaStream_t st) {
+template <typename Real, int NP, int NQ, bool GQ>
+cudaError_t mc_lin_launch_g(McHandle* h, int op, const double* v, double* out, cudaStream_t st) {
   McArgs A{};
   A.n_el = h->n_local;
   A.codes = h->codes;
@@ -1973,13 +2002,13 @@ cudaError_t mc_lin_launch(McHandle* h, int op, const double* v, double* out, cud
   Real* eb = static_cast<Real*>(h->lin_ebuf);
   const int grid = h->grid_elem, T = 32 * kMcWarps;
   if (op == 0) {
-    k_mc_lin<Real, NP, NQ><<<grid, T, 0, st>>>(A, cast_const<Real>(h->mc), wct);
+    k_mc_lin<Real, NP, NQ, GQ><<<grid, T, 0, st>>>(A, cast_const<Real>(h->mc), wct);
     return cudaGetLastError();
   }
   if (op == 1)
-    k_mc_hvp<Real, NP, NQ, false><<<grid, T, 0, st>>>(A, wct, eb);
+    k_mc_hvp<Real, NP, NQ, false, GQ><<<grid, T, 0, st>>>(A, wct, eb);
   else
-    k_mc_hvp<Real, NP, NQ, true><<<grid, T, 0, st>>>(A, wct, eb);
+    k_mc_hvp<Real, NP, NQ, true, GQ><<<grid, T, 0, st>>>(A, wct, eb);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (h->use_blk) {
@@ -1991,6 +2020,13 @@ cudaError_t mc_lin_launch(McHandle* h, int op, const double* v, double* out, cud
     k_mc_grad_gather<Real><<<gg, 256, 0, st>>>(h->n_rows, h->gptr, h->gidx, eb, h->row_gpos, nullptr, out);
   }
   return cudaGetLastError();
+}
+
+template <typename Real, int NP, int NQ>
+cudaError_t mc_lin_launch(McHandle* h, int op, const double* v, double* out, cudaStream_t st) {
+  if constexpr (NP == 6)
+    if (h->gq) return mc_lin_launch_g<Real, NP, NQ, true>(h, op, v, out, st);
+  return mc_lin_launch_g<Real, NP, NQ, false>(h, op, v, out, st);
 }
 
 template <typename Real>

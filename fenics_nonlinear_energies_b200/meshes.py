@@ -236,34 +236,60 @@ def slope_counts(h, x1=15.0, x2=10.0, x3=15.0, y1=10.0, y2=10.0):
     return nx12, nx3, ny1, ny2
 
 
-def slope_macro_mesh(h, x1=15.0, x2=10.0, x3=15.0, y1=10.0, y2=10.0):
-    """Vertices and P1 triangles of the 2-D slope: a full block ``[0, x1+x2+x3] x [0, y1]``
-    under a trapezoid whose right edge runs from ``(x1+x2, y1)`` to ``(x1, y1+y2)``.
-    Every cell is split into ``(ll, lr, ul)`` and ``(ur, ul, lr)``; lower block first."""
+def slope_p2_mesh(h, x1=15.0, x2=10.0, x3=15.0, y1=10.0, y2=10.0):
+    """P2 slope mesh with the node and element numbering of the reference's
+    generator (``slope_stability/support/mesh.py:334-521``).
+
+    Nodes live on the half-spacing grid: ``2 nx + 1`` columns for the rows of
+    the lower block ``[0, x1+x2+x3] x [0, y1]``, ``2 nx12 + 1`` columns for
+    the rows above it, whose right end follows the slope from ``(x1+x2, y1)``
+    to ``(x1, y1+y2)``; numbered row by row from the bottom, left to right.
+    Each cell (lower block first, then the upper part; rows outer, columns
+    inner) gives the triangles ``(ll, lr, ul)`` and ``(ur, ul, lr)``, each
+    with its vertices and then the midpoints of the edges opposite vertex
+    0, 1 and 2.  Returns ``nodes (N, 2)`` and ``elems (E, 6)``."""
     nx12, nx3, ny1, ny2 = slope_counts(h, x1, x2, x3, y1, y2)
     nx = nx12 + nx3
-    cx = np.concatenate((np.linspace(0.0, x1 + x2, nx12 + 1), np.linspace(x1 + x2, x1 + x2 + x3, nx3 + 1)[1:]))
-    cy = np.concatenate((np.linspace(0.0, y1, ny1 + 1), np.linspace(y1, y1 + y2, ny2 + 1)[1:]))
-    ids = {}
-    pts = []
-    for j in range(ny1 + 1):
-        for i in range(nx + 1):
-            ids[(i, j)] = len(pts)
-            pts.append((cx[i], cy[j]))
-    for j in range(ny1 + 1, ny1 + ny2 + 1):
-        xmax = x1 + x2 * (y1 + y2 - cy[j]) / y2
-        lx = np.linspace(0.0, xmax, nx12 + 1)
-        for i in range(nx12 + 1):
-            ids[(i, j)] = len(pts)
-            pts.append((lx[i], cy[j]))
+    gx = np.concatenate((np.linspace(0.0, x1 + x2, 2 * nx12 + 1), np.linspace(x1 + x2, x1 + x2 + x3, 2 * nx3 + 1)[1:]))
+    gy = np.concatenate((np.linspace(0.0, y1, 2 * ny1 + 1), np.linspace(y1, y1 + y2, 2 * ny2 + 1)[1:]))
+    rows = []
+    for j in range(2 * (ny1 + ny2) + 1):
+        if j <= 2 * ny1:
+            xs = gx
+        else:
+            xs = np.linspace(0.0, x1 + x2 * (y1 + y2 - gy[j]) / y2, 2 * nx12 + 1)
+        rows.append(np.column_stack((xs, np.full(xs.size, gy[j]))))
+    start = np.cumsum([0] + [r.shape[0] for r in rows])
+    nodes = np.vstack(rows)
+
+    def nid(i, j):
+        return start[j] + i
+
     tris = []
-    for (j0, j1, ni) in ((0, ny1, nx), (ny1, ny1 + ny2, nx12)):
+    for (j0, j1, ncols) in ((0, ny1, nx), (ny1, ny1 + ny2, nx12)):
         for j in range(j0, j1):
-            for i in range(ni):
-                ll, lr, ul, ur = ids[(i, j)], ids[(i + 1, j)], ids[(i, j + 1)], ids[(i + 1, j + 1)]
-                tris.append((ll, lr, ul))
-                tris.append((ur, ul, lr))
-    return np.asarray(pts, dtype=np.float64), np.asarray(tris, dtype=np.int64)
+            for i in range(ncols):
+                a, b = 2 * i, 2 * j
+                tris.append((nid(a, b), nid(a + 2, b), nid(a, b + 2),
+                             nid(a + 1, b + 1), nid(a, b + 1), nid(a + 1, b)))
+                tris.append((nid(a + 2, b + 2), nid(a, b + 2), nid(a + 2, b),
+                             nid(a + 1, b + 1), nid(a + 2, b + 1), nid(a + 1, b + 2)))
+    return nodes, np.asarray(tris, dtype=np.int64)
+
+
+def slope_macro_mesh(h, x1=15.0, x2=10.0, x3=15.0, y1=10.0, y2=10.0):
+    """Vertices and P1 triangles of the 2-D slope: the vertices of the P2 mesh
+    (``slope_p2_mesh``) renumbered in their P2 order, and its triangles'
+    vertex columns -- the macro mesh the reference's same-mesh Pk builder
+    starts from (``slope_stability/support/mesh.py:698-708``).  A full block
+    ``[0, x1+x2+x3] x [0, y1]`` under a trapezoid whose right edge runs from
+    ``(x1+x2, y1)`` to ``(x1, y1+y2)``; every cell split into ``(ll, lr, ul)``
+    and ``(ur, ul, lr)``; lower block first."""
+    p2_nodes, p2_elems = slope_p2_mesh(h, x1, x2, x3, y1, y2)
+    verts = np.unique(p2_elems[:, :3])
+    new_id = np.full(p2_nodes.shape[0], -1, dtype=np.int64)
+    new_id[verts] = np.arange(verts.size, dtype=np.int64)
+    return p2_nodes[verts].copy(), new_id[p2_elems[:, :3]]
 
 
 def lagrange_points(degree):
@@ -359,6 +385,42 @@ def affine_triangle_geometry(nodes, elems_scalar):
     return inv, np.abs(det)
 
 
+def isoparametric_triangle_geometry(nodes, elems_scalar, dhat1, dhat2):
+    """Inverse Jacobian and ``|det J|`` at every quadrature point of the
+    isoparametric map through all element nodes, ``(E, nq, 4)`` and
+    ``(E, nq)``: ``J_q = [[x.dh1_q, y.dh1_q], [x.dh2_q, y.dh2_q]]`` with
+    ``dhat1 / dhat2 (nq, n_p)`` the reference basis gradients -- the map of
+    the reference's P2 slope operators (``slope_stability/support/mesh.py:530-567``),
+    whose slope-side elements have their hypotenuse midpoint off the
+    straight edge."""
+    x = nodes[elems_scalar, 0]                      # (E, n_p)
+    y = nodes[elems_scalar, 1]
+    j11, j12 = x @ dhat1.T, y @ dhat1.T             # (E, nq)
+    j21, j22 = x @ dhat2.T, y @ dhat2.T
+    det = j11 * j22 - j12 * j21
+    inv = np.stack((j22 / det, -j12 / det, -j21 / det, j11 / det), axis=-1)
+    return inv, np.abs(det)
+
+
+def geometry_from_elem_B(elem_B, quad_weight, dhat1, dhat2, quad_w):
+    """Per-point ``J^-1 (E, nq, 4)`` and ``|det J| (E, nq)`` recovered from the
+    reference's stored operators: ``elem_B[e, q]`` holds the physical basis
+    gradients ``g = J_q^-1 [dh1; dh2]`` (rows xx: g_x at even columns, yy: g_y
+    at odd columns) and ``quad_weight = |det J_q| w_q``.  ``J_q^-1`` is the
+    least-squares solution over the element's nodes (exact for data that
+    came from a Jacobian)."""
+    gx = elem_B[:, :, 0, 0::2]                      # (E, nq, n_p)
+    gy = elem_B[:, :, 1, 1::2]
+    R = np.stack((dhat1, dhat2), axis=1)            # (nq, 2, n_p)
+    # g = X R  with X (2x2) per (e, q):  X = g R^T (R R^T)^-1
+    RRt_inv = np.linalg.inv(np.einsum("qkn,qln->qkl", R, R))
+    Rp = np.einsum("qkn,qkl->qnl", R, RRt_inv)      # (nq, n_p, 2)
+    ix = np.einsum("eqn,qnl->eql", gx, Rp)          # row 0 of J^-1
+    iy = np.einsum("eqn,qnl->eql", gy, Rp)          # row 1
+    inv = np.concatenate((ix, iy), axis=-1)
+    return inv, quad_weight / quad_w[None, :]
+
+
 def davis_b_reduction(c0, phi_deg, psi_deg, lam):
     """Davis-B strength reduction: reduced cohesion and friction angle (degrees)."""
     if lam <= 0.0:
@@ -376,18 +438,24 @@ def slope_problem(*, level=None, h=None, degree=4, E=2.0e4, nu=0.49, c0=6.0, phi
     """Homogeneous slope, plane strain, Pk same-mesh elements, Davis-B reduced strength."""
     if h is None:
         h = SLOPE_LEVEL_TO_H[int(level)]
-    macro_nodes, macro_elems = slope_macro_mesh(h)
-    nodes, es = same_mesh_lagrange(macro_nodes, macro_elems, degree)
+    if int(degree) == 2:  # the reference builds P2 with its own grid generator
+        nodes, es = slope_p2_mesh(h)
+    else:
+        macro_nodes, macro_elems = slope_macro_mesh(h)
+        nodes, es = same_mesh_lagrange(macro_nodes, macro_elems, degree)
     xi, wq = slope_quadrature(degree)
     hatp, dh1, dh2 = lagrange_tabulate(degree, xi)      # (n_p, nq)
-    inv, det = affine_triangle_geometry(nodes, es)
+    if int(degree) == 2:  # per-point map through all six nodes, as the reference's P2 operators
+        inv, det = isoparametric_triangle_geometry(nodes, es, dh1.T, dh2.T)
+    else:                 # vertex (affine) map, as the reference's Pk same-mesh operators
+        inv, det = affine_triangle_geometry(nodes, es)
     n_nodes = nodes.shape[0]
     xmax = float(np.max(nodes[:, 0])) - 1.0e-9
     q_mask = np.zeros((n_nodes, 2), dtype=bool)
     q_mask[:, 0] = (nodes[:, 0] > 0.0) & (nodes[:, 1] > 0.0) & (nodes[:, 0] < xmax)
     q_mask[:, 1] = nodes[:, 1] > 0.0
     freedofs = np.arange(2 * n_nodes, dtype=np.int64).reshape(n_nodes, 2)[q_mask]
-    qw = det[:, None] * wq[None, :]                       # (E, nq)
+    qw = (det if det.ndim == 2 else det[:, None]) * wq[None, :]   # (E, nq)
     # gravity load f_a = sum_q w_q phi_a(q) (0, -gamma)
     force = np.zeros(2 * n_nodes)
     np.add.at(force, 2 * es + 1, -gamma * (qw @ hatp.T))
@@ -412,8 +480,10 @@ def slope_elem_B(params):
     rows (eps_xx, eps_yy, gamma_xy), interleaved (u_x, u_y) per node."""
     inv = params["inv_jac"]
     d1, d2 = params["dhat1"], params["dhat2"]            # (nq, n_p)
-    gx = inv[:, 0, None, None] * d1[None] + inv[:, 1, None, None] * d2[None]
-    gy = inv[:, 2, None, None] * d1[None] + inv[:, 3, None, None] * d2[None]
+    if inv.ndim == 2:  # affine: one J^-1 per element
+        inv = np.broadcast_to(inv[:, None, :], (inv.shape[0], d1.shape[0], 4))
+    gx = inv[:, :, 0, None] * d1[None] + inv[:, :, 1, None] * d2[None]
+    gy = inv[:, :, 2, None] * d1[None] + inv[:, :, 3, None] * d2[None]
     E, nq, n_p = gx.shape
     B = np.zeros((E, nq, 3, 2 * n_p))
     B[:, :, 0, 0::2] = gx

@@ -140,6 +140,10 @@ typedef struct {
    *                    gradients J_e^-T grad(phi_a)(xi_q); quad_weight[e,q]
    *                    = |det J_e| w_q):
    *                    e0 = J_e^-1 row-major [E*4], e1 = |det J_e| [E],
+   *                    or, with s[6] = 1 (P2 only), the isoparametric map's
+   *                    e0 = J_eq^-1 [E*nq*4], e1 = |det J_eq| [E*nq] per
+   *                    quadrature point (the reference's P2 operators,
+   *                    src/problems/slope_stability/support/mesh.py:530-567),
    *                    e2 = eps_p_old [E*nq*3] or NULL (zero),
    *                    e3 = reference tables [dhat1 (nq*np) | dhat2 (nq*np) | w (nq)],
    *                    npe = np (3, 6 or 15), block_size = 2, nq = 1, 7 or 25 */
@@ -152,7 +156,8 @@ typedef struct {
    *   GL        : s[0] = eps, s[1..9] = ip (3x3 row-major), s[10..12] = w
    *   Neo-Hook. : s[0] = C1, s[1] = D1, s[2] = use_abs_det (0/1)
    *   M-C       : s[0] = E, s[1] = nu, s[2] = phi_deg, s[3] = cohesion,
-   *               s[4] = reg, s[5] = elastic (0/1)                           */
+   *               s[4] = reg, s[5] = elastic (0/1),
+   *               s[6] = geometry per quadrature point (0/1, see e0/e1)    */
   double s[16];
   const double* dirichlet;      /* [n_total] full DOF vector (Dirichlet part) */
   const double* rhs_owned;      /* [hi-lo] load vector f (reordered), or NULL */

@@ -99,7 +99,7 @@ def test_mc_oracle_gravity_load_matches_reference_rule():
     p = meshes.slope_problem(level=1, degree=2)
     asm = OracleAssembler("mc", dict(p, elem_B=meshes.slope_elem_B(p)), block_size=2)
     total = float(np.sum(p["force"][1::2]))
-    area = float(np.sum(p["det_j"]) / 2.0)
+    area = float(np.sum(p["quad_weight"]))  # sum_q |det J_q| w_q over the elements
     assert math.isclose(total, -p["gamma"] * area, rel_tol=1e-12)
     assert asm.f_owned.size == asm.layout.hi - asm.layout.lo
 
