@@ -1,12 +1,18 @@
 """Benchmark: fused energy + gradient + Hessian assembly, elements/s.
 
-Default workload (``--workload gl1024_fp32h``, one "step"): Ginzburg-Landau,
+Default workload (``--workload gl1024_fp64``, one "step"): Ginzburg-Landau,
 eps = 0.01 on [-1, 1]^2, structured 1024 x 1024 grid of P1 triangles
 (2,097,152 elements, 1,046,529 free DOFs, 7,317,521 owned COO entries),
-u ~ U[-0.5, 0.5] from a fixed seed; FP32 element gradients / Hessians
-(float32 COO values), FP64 energy reduction.  One step = one fused
-E+grad+Hess pass over every element into the device gradient and the owned
-COO values (the reference's energy_fn + gradient_fn + assemble_hessian_element).
+u ~ U[-0.5, 0.5] from a fixed seed, FP64 throughout (the reference's
+arithmetic).  One step = one fused E+grad+Hess pass over every element into
+the device gradient and the owned COO values (the reference's energy_fn +
+gradient_fn + assemble_hessian_element).  ``gl1024_fp32h`` is the same
+configuration with FP32 element gradients / Hessians.
+
+``error_vs_fp64_oracle`` (outside the timed region): the largest relative
+error of the energy, gradient and COO values of one pass against the FP64
+oracle on the same configuration (every entry; the P4 slope on 400 sampled
+owned rows).
 
 Other workloads (same JSON line, same timing rules; ``--workload NAME``):
 p-Laplace 128x128 P1 (FP64, zero state), Ginzburg-Landau 1024^2 in FP64,
@@ -31,7 +37,14 @@ H2D of u from pinned memory, the pass, D2H of energy, gradient and COO values.
 Multi-GPU: every rank runs its own replica of the workload (weak scaling).
 ``--impl reference``: the CPU restatement of the reference path (the JAX
 element kernels + np.add.at scatter, restated in oracle/) on the host cores,
-on a bounded sample of the same workload family.
+on the same configuration where one pass takes seconds (P1 triangles,
+tetrahedra), else on a bounded sample of the same workload family.
+``cpu_baseline`` (``--impl b200``): for the P1-triangle families a
+numba-parallel CPU assembly of the full configuration on all host threads
+(closed-form element derivatives, parallel deterministic gathers) -- the
+stronger CPU line -- with the autodiff restatement on its sample and the
+reference's archived single-thread figure beside it; for the other families
+the autodiff restatement on a bounded sample.
 """
 
 
@@ -178,16 +191,20 @@ class Workload:
     ``conn_nodes`` / ``geom_values`` are the node-level connectivity entries
     and the per-element geometry values one pass reads (algorithmic bytes);
     ``sample()`` returns ``(family, oracle_kwargs, params, u, n_el, label)`` for
-    the bounded CPU restatement run.
+    the bounded CPU restatement run; ``full()`` (where set) the same for the
+    whole configuration.
     """
 
     def __init__(self, name, family, precision, hess_fp32, conn_nodes, geom_values, geom_bytes, has_rhs, desc,
-                 build, sample, op="egh", newton_kw=None):
+                 build, sample, op="egh", newton_kw=None, full=None):
         self.op = op  # "egh": fused E+grad+Hess pass; "hvp": matrix-free H(u) x; "newton": one Newton solve
         self.newton_kw = dict(newton_kw or {})  # Newton settings of the "newton" workloads
         self.name, self.family, self.precision, self.hess_fp32 = name, family, precision, hess_fp32
         self.conn_nodes, self.geom_values, self.geom_bytes, self.has_rhs = conn_nodes, geom_values, geom_bytes, has_rhs
         self.desc, self.build, self.sample = desc, build, sample
+        # full(): the whole configuration for the CPU restatement (same tuple as sample()),
+        # or None where one CPU pass would take minutes
+        self.full = full if full is not None else (getattr(build, "full", None) if op == "egh" else None)
 
     @property
     def dtype(self):
@@ -256,6 +273,16 @@ def _tri(kind, n, precision, seed_from_rank=True, start_seed=None, sample_n=None
             params, u0 = meshes.plaplace_problem(n=m, seed=start_seed)
         return kind, {}, params, u0, 2 * m * m, f"{m}x{m} P1 grid"
 
+    def full():
+        from fenics_nonlinear_energies_b200 import meshes
+
+        if kind == "gl":
+            params, u0 = meshes.gl_problem(n=n, seed=0)
+        else:
+            params, u0 = meshes.plaplace_problem(n=n, seed=start_seed)
+        return kind, {}, params, u0, 2 * n * n, f"{n}x{n} P1 grid"
+
+    build.full = full
     return build, sample
 
 
@@ -283,6 +310,16 @@ def _he(nx, ny, nz, precision, theta=4.0 * 3.141592653589793 / 24.0):
         return "he", {"block_size": 3, "coordinate_key": "nodes2coord", "dirichlet_key": "u_0_ref"}, params, \
             pos[params["freedofs"]], 6 * sx * ny * nz, f"{sx}x{ny}x{nz}-hex beam"
 
+    def full():
+        from fenics_nonlinear_energies_b200 import meshes
+
+        params, _ = meshes.he_beam_problem(nx=nx, ny=ny, nz=nz)
+        pos = twisted_beam_positions(params, theta)
+        params = dict(params, u_0_ref=pos)
+        return "he", {"block_size": 3, "coordinate_key": "nodes2coord", "dirichlet_key": "u_0_ref"}, params, \
+            pos[params["freedofs"]], 6 * nx * ny * nz, f"{nx}x{ny}x{nz}-hex beam"
+
+    build.full = full
     return build, sample
 
 
@@ -418,10 +455,24 @@ WORKLOADS = {
         "gradients / Hessians (FP32 COO values in the CG), FP64 energy, state and CG arithmetic",
         *_tri("gl", 1024, "fp32", sample_n=96), op="newton"),
 }
-DEFAULT_WORKLOAD = "gl1024_fp32h"
+DEFAULT_WORKLOAD = "gl1024_fp64"
 
-KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri", 5: "k_mc_elem+k_node_gather",
-                6: "k_mc_tc+k_fixup2", 7: "k_he_elem+k_node_gather", 8: "k_push_tri", 9: "k_mc_dmma+k_fixup2"}
+# The reference's own archived per-assembly timings at the 1024^2 GL grid
+# (GL level 9, one MPI rank, one thread, JAX on the CPU; hardware not
+# recorded): element Hessians 42.76 ms + np.add.at scatter 152.3 ms + COO
+# insert 27.17 ms (total 229.9 ms) + gradient 37.4 ms, median per assembly,
+# archive/results/raw_results_historical/experiment_results_cache/
+# gl_final_suite/jax_petsc_element_l9_np1.json.
+REFERENCE_ARCHIVED = {
+    "gl": {"value": 2097152 / (0.2299 + 0.0374), "unit": "elements/s", "cores": 1,
+           "what": "E+grad+Hess assembled into COO values (229.9 ms Hessian assembly + 37.4 ms gradient per pass), "
+                   "reference JAX-CPU, one thread, archived run (gl_final_suite/jax_petsc_element_l9_np1.json), "
+                   "hardware not recorded"},
+}
+
+KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri",
+                5: "k_mc_elem+k_node_gather+k_rowgrad", 6: "k_mc_tc+k_fixup2+k_rowgrad", 7: "k_he_elem+k_node_gather",
+                8: "k_push_tri", 9: "k_mc_dmma+k_fixup2+k_rowgrad"}
 
 
 def algorithmic_bytes(w, asm, n_el, energy_only=False):
@@ -440,7 +491,7 @@ def algorithmic_bytes(w, asm, n_el, energy_only=False):
     return b
 
 
-ENERGY_KERNELS = {"plaplace": "k_energy_tri", "gl": "k_energy_tri", "he": "k_energy_tet", "mc": "k_mc_elem (energy)"}
+ENERGY_KERNELS = {"plaplace": "k_energy_tri", "gl": "k_energy_tri", "he": "k_energy_tet", "mc": "k_mc_eg"}
 
 
 # ---------------------------------------------------------------------------
@@ -483,7 +534,16 @@ def run_reference(args):
 
     torch.set_num_threads(os.cpu_count() or 1)
     w = WORKLOADS[args.workload]
-    asm, u, n_el, label, _, _, _ = _oracle_sample(w)
+    full = w.full is not None and w.op == "egh"
+    if full:  # the whole configuration: one pass takes seconds on the host
+        from oracle.assembler import OracleAssembler
+
+        family, okw, params, u, _, label = w.full()
+        asm = OracleAssembler(family, params, **okw)
+        u = u[asm.layout.perm]
+        n_el = int(asm.local.local_elem_idx.size)
+    else:
+        asm, u, n_el, label, _, _, _ = _oracle_sample(w)
     if w.op == "hvp":
         # the reference's "matfree_element" product: element Hessians of the
         # linearization point (computed once), then sum_e H_e x_e by np.add.at
@@ -532,18 +592,107 @@ def run_reference(args):
             "golden-section line search)" if newton_op else
             "energy pass of the CPU restatement of the reference element energy" if energy_op else
             "CPU restatement of the reference JAX element kernels (torch.func float64 autodiff) + np.add.at scatter")
+    if full:
+        config = workload_config(w, n_el, asm.layout.n_free, asm.layout.owned_rows.size, world)
+    else:
+        config = {"workload": w.name, "description": w.desc, "sample": label, "elements_per_step": n_el}
     line = {
         "impl": "reference", "metric": metric, "value": value, "unit": unit,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
         "higher_is_better": not newton_op, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": w.name, "description": w.desc, "sample": label, "elements_per_step": n_el},
+        "data": "synthetic (seeded / closed-form state on the generated mesh)",
+        "config": config,
         "cpu_baseline": {"value": value, "unit": unit, "cores": int(torch.get_num_threads()),
-                         "kind": "port", "sample": f"{label} ({n_el} elements) per step; {what}"},
+                         "kind": "port", "sample": f"{'full configuration' if full else 'sample'}: {label} "
+                                                   f"({n_el} elements) per step; {what}"},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_config(w, n_el, n_free, nnz, world):
+    """The workload's ``config`` object, identical in both arms."""
+    return {"workload": w.name, "description": w.desc, "elements": int(n_el), "free_dofs": int(n_free),
+            "coo_nnz": int(nnz), "l2": "flushed by a 1 GiB write between passes (outside the timed events)",
+            "parallelism": f"{world} independent replica(s), one per GPU"}
+
+
+# Mohr-Coulomb P4 meshes above this size are checked on sampled rows only.
+ORACLE_FULL_LIMIT = {"mc4": 60_000}
+
+
+def oracle_error(w, asm, u_host, e_dev, g_dev, h_dev):
+    """Largest relative errors of one pass against the FP64 oracle on the
+    same configuration: energy vs max(1, sum |e_e| + |load|), gradient and
+    COO values vs their largest entry.  Returns (dict, oracle assembler or None)."""
+    import numpy as np
+
+    from oracle import energies
+    from oracle.assembler import OracleAssembler, restricted_rows
+
+    fam = w.family
+    okw = {"block_size": asm.block_size, "coordinate_key": asm.coordinate_key, "dirichlet_key": asm.dirichlet_key}
+    params = dict(asm.params)
+    g = g_dev[: asm.n_owned].double().cpu().numpy()
+    h = h_dev.double().cpu().numpy()
+    e = float(e_dev.item())
+    lay = asm.layout
+    t0 = time.perf_counter()
+
+    def rel(a, b):
+        return float(np.abs(a - b).max(initial=0.0) / max(np.abs(b).max(initial=0.0), 1e-300))
+
+    if fam == "mc" and int(asm.npe) == 15 and asm.info["n_elem"] > ORACLE_FULL_LIMIT["mc4"]:
+        from fenics_nonlinear_energies_b200 import meshes
+
+        class _ElemB:
+            def __getitem__(self, idx):
+                return meshes.slope_elem_B({"dhat1": params["dhat1"], "dhat2": params["dhat2"],
+                                            "inv_jac": params["inv_jac"][idx]})
+
+        params["elem_B"] = _ElemB()
+        rows = np.sort(np.random.default_rng(11).choice(np.arange(lay.lo, lay.hi), 400, replace=False))
+        force = np.asarray(params["force"])[params["freedofs"]][lay.perm][lay.lo: lay.hi]
+        g_ref, pos, h_ref = restricted_rows("mc", params, lay, u_host, rows, dirichlet_full=asm.dirichlet_full,
+                                            f_owned=force)
+        return {"energy": None, "grad": rel(g[rows - lay.lo], g_ref), "hess": rel(h[pos], h_ref),
+                "scope": "400 sampled owned rows (all their gradient entries and COO values)",
+                "oracle_s": time.perf_counter() - t0}, None
+    if fam == "mc":
+        from fenics_nonlinear_energies_b200 import meshes
+
+        params["elem_B"] = meshes.slope_elem_B(params)
+    orc = OracleAssembler(fam, params, layout=lay, **okw)
+    if fam == "he":
+        orc.update_dirichlet(asm.dirichlet_full)
+    e_ref, g_ref, h_ref = orc.all_in_one(u_host)
+    v = orc.v_local(u_host)[orc.local.elems_local_np]
+    e_el, _, _ = energies.element_derivatives(fam, v, orc.elem_data, orc.params, want_hessian=False)
+    load = abs(float(orc.f_owned @ u_host[lay.lo: lay.hi])) if orc.f_owned.size else 0.0
+    scale = max(1.0, float(np.abs(e_el).sum()) + load + abs(orc.dirichlet_only_energy))
+    return {"energy": abs(e - e_ref) / scale, "grad": rel(g, g_ref), "hess": rel(h, h_ref),
+            "scope": "every owned gradient entry and COO value", "energy_scale": "sum |e_e| + |load|",
+            "oracle_s": time.perf_counter() - t0}, orc
+
+
+def cpu_fast_baseline(orc, u_host, n_el, label):
+    """The numba-parallel CPU assembly on the full configuration."""
+    from oracle.cpu_fast import FastTriangleAssembler
+
+    fast = FastTriangleAssembler(orc)
+    fast.all_in_one(u_host)  # compile + warm-up
+    times = []
+    while len(times) < 20 and sum(times) < 8.0:
+        t = time.perf_counter()
+        fast.all_in_one(u_host)
+        times.append(time.perf_counter() - t)
+    dt = statistics.median(times)
+    return {"value": n_el / dt, "unit": "elements/s", "cores": fast.threads(), "kind": "port",
+            "sample": f"full configuration ({label}, {n_el} elements), median of {len(times)} fused "
+                      f"E+grad+Hess passes into the owned COO values: numba-parallel closed-form element "
+                      f"derivatives + parallel fixed-order gathers on all host threads",
+            "seconds_per_pass": dt}
 
 
 # ---------------------------------------------------------------------------
@@ -874,18 +1023,30 @@ def run(args):
     traffic = NCU_TRAFFIC.get((w.name, kname))
     nnz = int(asm.owned_values.numel())
 
+    cpu, err, extra = None, None, {}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        orc = None
+        if not energy_only:  # accuracy of this pass against the FP64 oracle (outside the timed region)
+            e_d, g_d, h_d = asm.eval(u, flags)
+            torch.cuda.synchronize()
+            err, orc = oracle_error(w, asm, np.asarray(u0, dtype=np.float64), e_d, g_d, h_d)
+        if orc is not None and w.family in ("gl", "plaplace") and w.full is not None:
+            cpu = cpu_fast_baseline(orc, np.asarray(u0, dtype=np.float64), n_el, w.full()[5])
+            extra["cpu_baseline_autodiff"] = cpu_port_baseline(w)
+            if w.family in REFERENCE_ARCHIVED and n_el >= 2_000_000:
+                extra["reference_archived"] = REFERENCE_ARCHIVED[w.family]
+        else:
+            cpu = cpu_port_baseline(w, energy_only)
     if rank == 0:
-        cpu = cpu_port_baseline(w, energy_only) if (world == 1 and not args.no_cpu_baseline) else None
         line = {
             "metric": "elements/s (energy)" if energy_only else "elements/s (E+grad+Hess)", "value": value,
             "unit": "elements/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": w.dtype,
             "data": "synthetic (seeded / closed-form state on the generated mesh)",
-            "config": {"workload": w.name, "description": w.desc, "elements": n_el, "free_dofs": asm.layout.n_free,
-                       "coo_nnz": nnz, "energy": energy, "setup_s": t_setup,
-                       "l2": "flushed by a 1 GiB write between passes (outside the timed events)",
-                       "parallelism": f"{world} independent replica(s), one per GPU"},
+            "config": workload_config(w, n_el, asm.layout.n_free, nnz, world),
+            "details": {"energy": energy, "setup_s": t_setup},
+            "error_vs_fp64_oracle": err,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": f"{peak_kind} burst copy (hbm_gbs)",
                          "traffic": traffic[0] if traffic else None,
@@ -900,6 +1061,7 @@ def run(args):
             "gpu_launches": args.steps * launches_per_pass,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            **extra,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -87,6 +87,8 @@ def _load():
         "fne_eval_host": (C.c_int, [vp, _f64p, C.c_int, _f64p, _f64p, vp]),
         "fne_destroy": (C.c_int, [vp]),
         "fne_check_device_status": (C.c_int, [vp]),
+        "fne_poll_device_status": (C.c_int, [vp]),
+        "fne_set_wait_limit": (C.c_int, [vp, C.c_int64]),
         "fne_hvp_prepare": (C.c_int, [vp, vp, vp]),
         "fne_hvp": (C.c_int, [vp, vp, vp, vp]),
         "fne_hvp_diagonal": (C.c_int, [vp, vp, vp]),

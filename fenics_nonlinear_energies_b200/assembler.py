@@ -169,6 +169,12 @@ class CudaElementAssemblerBase:
         """Raise if a bounded device wait of an earlier pass gave up (synchronous)."""
         check(lib.fne_check_device_status(self._handle))
 
+    def _poll_status(self):
+        """Raise ``FneError(FNE_ETIMEOUT)`` if the last pass gave up a bounded
+        device wait (its values are then not valid).  Reads the pinned copy
+        the pass left behind: call after the pass's stream has synchronised."""
+        check(lib.fne_poll_device_status(self._handle))
+
     def launches_per_eval(self, flags):
         """Kernel launches one ``eval(u, flags)`` issues: one fused kernel for the
         triangle families and the tet row-gather kernel; element kernel plus one
@@ -236,6 +242,7 @@ class CudaElementAssemblerBase:
         e = self.eval(vec, _lib.FNE_ENERGY)[0]
         self._ev1.record()
         val = float(e.item())
+        self._poll_status()
         st = self._callback_stats["energy"]
         st["calls"] += 1
         st["kernel"] += self._ev0.elapsed_time(self._ev1) * 1e-3
@@ -255,6 +262,7 @@ class CudaElementAssemblerBase:
         st = self._callback_stats["gradient"]
         st["calls"] += 1
         torch.cuda.current_stream(self.device).synchronize()
+        self._poll_status()
         st["kernel"] += self._ev0.elapsed_time(self._ev1) * 1e-3
         st["total"] += time.perf_counter() - t
 
@@ -268,6 +276,7 @@ class CudaElementAssemblerBase:
         self.eval(u_owned, _lib.FNE_HESS)
         self._ev1.record()
         self._ev1.synchronize()
+        self._poll_status()
         t_k = self._ev0.elapsed_time(self._ev1) * 1e-3
         timings = {"elem_hessian_compute": t_k, "scatter": 0.0, "hvp_compute": t_k, "extraction": 0.0,
                    "allgatherv": 0.0, "ghost_exchange": 0.0, "build_v_local": 0.0, "p2p_exchange": 0.0,

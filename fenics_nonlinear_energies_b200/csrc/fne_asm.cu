@@ -2057,6 +2057,17 @@ extern "C" int fne_check_device_status(fne_handle* h) {
   return h->mc ? mc_check_status(h->mc) : FNE_OK;
 }
 
+extern "C" int fne_poll_device_status(fne_handle* h) {
+  if (!h) return set_error(FNE_EINVAL, "fne_poll_device_status: null handle");
+  return h->mc ? mc_poll_status(h->mc) : FNE_OK;
+}
+
+extern "C" int fne_set_wait_limit(fne_handle* h, int64_t polls) {
+  if (!h) return set_error(FNE_EINVAL, "fne_set_wait_limit: null handle");
+  if (!h->mc) return set_error(FNE_EINVAL, "fne_set_wait_limit: the handle runs no tensor-core kernel");
+  return mc_set_wait_limit(h->mc, (long long)polls);
+}
+
 extern "C" int fne_set_dirichlet(fne_handle* h, const double* dirichlet) {
   if (!h || (!dirichlet && h->n_total > 0)) return set_error(FNE_EINVAL, "fne_set_dirichlet: null argument");
   if (h->n_total == 0) return FNE_OK;

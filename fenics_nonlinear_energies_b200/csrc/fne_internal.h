@@ -184,6 +184,8 @@ int mc_eval(McHandle* h, const double* u, int flags, double* energy, double* gra
 int mc_set_dirichlet(McHandle* h, const double* dirichlet);
 void mc_info(const McHandle* h, fne_info* info);
 int mc_check_status(McHandle* h);
+int mc_poll_status(McHandle* h);
+int mc_set_wait_limit(McHandle* h, long long polls);
 int mc_hvp_prepare(McHandle* h, const double* u, void* stream);
 int mc_hvp(McHandle* h, const double* x, double* y, void* stream);
 int mc_hvp_diagonal(McHandle* h, double* diag, void* stream);

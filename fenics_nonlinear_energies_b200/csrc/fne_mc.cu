@@ -596,6 +596,7 @@ struct McTcArgs {
   const float* Phi;  // [KP/4][M][4] constant operand, hi part (core-matrix order)
   const float* Plo;  // same, lo part
   int* err;          // device status word (0 = ok; 1 = MMA completion wait timed out)
+  long long wait_limit;  // polls of each tile's MMA-completion wait (kMcWaitLimit unless a test lowers it)
   // direct-write epilogue (DirectPlan): per element and directed node pair a
   // 16-bit code, shared-slot base, row node of every element node, COO start
   // of every row (row node, component), and the shared-block buffer
@@ -870,7 +871,7 @@ __global__ void __launch_bounds__(McTile<NP, NQ, GQ>::THREADS, McTile<NP, NQ, GQ
     // (5) epilogue: TMEM -> Kbuf[e][pair][c * 2 + d]; warp w reads lanes 32 (w % 4) ..
     // (node pairs) for its share of the tile's elements
     if (WANT & MW_H) {
-      if (tc::mbar_wait(bar, phase, kMcWaitLimit))
+      if (tc::mbar_wait(bar, phase, T.wait_limit))
         phase ^= 1u;
       else if (lane == 0)
         atomicExch(sFail, 1);
@@ -1433,6 +1434,8 @@ struct McHandle {
   int tc = 0, grid_tc = 1;
   float *Phi = nullptr, *Plo = nullptr;
   int* err = nullptr;
+  int* err_host = nullptr;               // pinned copy of *err after each tensor-core pass
+  long long wait_limit = kMcWaitLimit;   // MMA-completion wait bound of the tensor-core kernel
   // direct-write epilogue: per-element codes, shared-block buffer and the
   // fix-up plan over the shared blocks
   uint16_t* dp_code = nullptr;
@@ -1532,7 +1535,7 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
   if constexpr (sizeof(Real) == 4 && NP > 3) {
     if (h->tc && (flags & MW_H)) {
       using G = McTile<NP, NQ, GQ>;
-      McTcArgs T{h->Phi, h->Plo, h->err, h->dp_code, h->dp_sbase, h->dp_elem_rn, h->bp_rn_row,
+      McTcArgs T{h->Phi, h->Plo, h->err, h->wait_limit, h->dp_code, h->dp_sbase, h->dp_elem_rn, h->bp_rn_row,
                  static_cast<float*>(h->dp_sbuf)};
       float* g = static_cast<float*>(h->gbuf);
       HOut* H = static_cast<HOut*>(hess);
@@ -1543,6 +1546,10 @@ cudaError_t mc_launch(McHandle* h, int flags, const double* u, double* energy, d
         case 6: k_mc_tc<NP, NQ, 6, HOut, GQ><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
         default: k_mc_tc<NP, NQ, 7, HOut, GQ><<<h->grid_tc, G::THREADS, G::SMEM, st>>>(A, Mf, T, H, g, h->partials, h->counter, energy); break;
       }
+      // stream-ordered copy of the status word for fne_poll_device_status
+      cudaError_t ce = cudaGetLastError();
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(h->err_host, h->err, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (ce != cudaSuccess) return ce;
       return mc_gathers<float, HOut, NP>(h, flags, static_cast<const float*>(nullptr), g, grad, hess, st);
     }
   }
@@ -1676,6 +1683,7 @@ void mc_destroy(McHandle* h) {
                   h->dp_sbuf, h->fx_con, h->fx_desc, h->lin_wct, h->lin_ebuf};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (h->err_host) cudaFreeHost(h->err_host);
   delete h;
 }
 
@@ -1950,10 +1958,12 @@ int mc_create(const fne_desc* d, McHandle** out) {
     MC_TRY(mc_upload(h, &h->Phi, phi.data(), phi.size()));
     MC_TRY(mc_upload(h, &h->Plo, plo.data(), plo.size()));
     MC_TRY(mc_upload(h, &h->err, (const int*)nullptr, 1));
-    if (cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess) {
+    if (cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess ||
+        cudaHostAlloc((void**)&h->err_host, sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
       mc_destroy(h);
-      return set_error(FNE_ECUDA, "Mohr-Coulomb: cudaMemset");
+      return set_error(FNE_ECUDA, "Mohr-Coulomb: status word");
     }
+    *h->err_host = 0;
   }
 #undef MC_TRY
   *out = h;
@@ -2074,7 +2084,21 @@ int mc_check_status(McHandle* h) {
   if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("fne_check_device_status: ") + cudaGetErrorString(e));
   if (v == 0) return FNE_OK;
   cudaMemset(h->err, 0, sizeof(int));
+  if (h->err_host) *h->err_host = 0;
   return set_error(FNE_ETIMEOUT, "Mohr-Coulomb tensor-core kernel: an MMA completion wait gave up");
+}
+
+int mc_poll_status(McHandle* h) {
+  if (!h->err_host || *(volatile int*)h->err_host == 0) return FNE_OK;
+  *h->err_host = 0;
+  cudaMemset(h->err, 0, sizeof(int));
+  return set_error(FNE_ETIMEOUT, "Mohr-Coulomb tensor-core kernel: an MMA completion wait gave up");
+}
+
+int mc_set_wait_limit(McHandle* h, long long polls) {
+  if (!h->tc) return set_error(FNE_EINVAL, "fne_set_wait_limit: the handle runs no tensor-core kernel");
+  h->wait_limit = polls < 0 ? kMcWaitLimit : polls;
+  return FNE_OK;
 }
 
 void mc_info(const McHandle* h, fne_info* info) {

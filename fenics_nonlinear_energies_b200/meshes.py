@@ -351,24 +351,23 @@ def slope_quadrature(degree):
 
 def same_mesh_lagrange(macro_nodes, macro_elems, degree, decimals=12):
     """Pk nodes on every macro triangle, shared nodes merged by rounded coordinates
-    in element order (the numbering rule of the reference's same-mesh builder)."""
+    in element order (the numbering rule of the reference's same-mesh builder:
+    a node gets the next id when its rounded coordinates first appear, walking
+    the elements and their local points in order)."""
     ref = lagrange_points(degree)
-    lookup = {}
-    coords = []
-    elems = np.zeros((macro_elems.shape[0], ref.shape[0]), dtype=np.int64)
-    v = macro_nodes[macro_elems]
-    for e in range(macro_elems.shape[0]):
-        p0, p1, p2 = v[e, 0], v[e, 1], v[e, 2]
-        for a, (xi, eta) in enumerate(ref):
-            p = (1.0 - xi - eta) * p0 + xi * p1 + eta * p2
-            key = (round(float(p[0]), decimals), round(float(p[1]), decimals))
-            nid = lookup.get(key)
-            if nid is None:
-                nid = len(coords)
-                lookup[key] = nid
-                coords.append(p)
-            elems[e, a] = nid
-    return np.asarray(coords, dtype=np.float64), elems
+    v = macro_nodes[macro_elems]                                  # (E, 3, 2)
+    lam = np.stack((1.0 - ref[:, 0] - ref[:, 1], ref[:, 0], ref[:, 1]), axis=1)  # (n_p, 3)
+    pts = (lam[None, :, 0, None] * v[:, None, 0] + lam[None, :, 1, None] * v[:, None, 1]
+           + lam[None, :, 2, None] * v[:, None, 2])               # (E, n_p, 2)
+    flat = pts.reshape(-1, 2)
+    keys = np.round(flat, decimals)
+    keys[keys == 0.0] = 0.0                                       # -0.0 and 0.0 are one key
+    _, first, inverse = np.unique(keys, axis=0, return_index=True, return_inverse=True)
+    order = np.argsort(first, kind="stable")                      # ids by first appearance
+    new_id = np.empty(order.size, dtype=np.int64)
+    new_id[order] = np.arange(order.size, dtype=np.int64)
+    elems = new_id[inverse.reshape(-1)].reshape(macro_elems.shape[0], ref.shape[0])
+    return flat[first[order]].copy(), elems
 
 
 def affine_triangle_geometry(nodes, elems_scalar):

@@ -223,6 +223,23 @@ int fne_hvp_diagonal(fne_handle* h, double* diag, void* stream);
  * counterpart in the reference, whose element kernels run on the CPU.
  */
 int fne_check_device_status(fne_handle* h);
+/*
+ * The same status without a device synchronisation: every tensor-core pass
+ * ends with a stream-ordered copy of the word into pinned host memory, and
+ * this reads that copy.  Call it after synchronising the stream of the pass
+ * (the assembler callbacks do so after each pass).  FNE_OK, or FNE_ETIMEOUT
+ * (both copies are then cleared).  No counterpart in the reference.
+ */
+int fne_poll_device_status(fne_handle* h);
+/*
+ * Polls of the tensor-core kernel's per-tile MMA-completion wait before it
+ * gives up (records FNE_ETIMEOUT, drains its own MMAs with the full bound,
+ * frees its tensor memory and returns); polls < 0 restores the default
+ * (2^22).  0 makes every pass give up at once: how the tests exercise the
+ * timeout path without a fault.  FNE_EINVAL for a handle without the
+ * tensor-core kernel.  No counterpart in the reference.
+ */
+int fne_set_wait_limit(fne_handle* h, int64_t polls);
 /* Replace the Dirichlet values; ``dirichlet`` is a host array [n_total]. */
 int fne_set_dirichlet(fne_handle* h, const double* dirichlet);
 /*

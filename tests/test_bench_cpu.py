@@ -42,8 +42,12 @@ def test_workload_table():
         assert callable(w.build) and callable(w.sample)
         if w.op == "newton":
             assert set(w.newton_kw) <= {"ksp_rtol", "ksp_max_it", "maxit", "linesearch_tol", "tolf"}
-    assert bench.DEFAULT_WORKLOAD == "gl1024_fp32h"
-    assert bench.KERNEL_NAMES[9] == "k_mc_dmma+k_fixup2"
+    assert bench.DEFAULT_WORKLOAD == "gl1024_fp64"
+    assert bench.WORKLOADS[bench.DEFAULT_WORKLOAD].dtype == "f64"
+    assert bench.KERNEL_NAMES[9] == "k_mc_dmma+k_fixup2+k_rowgrad"
+    assert bench.ENERGY_KERNELS["mc"] == "k_mc_eg"
+    for name in ("gl1024_fp64", "gl1024_fp32h", "plaplace128_fp64", "he160x8x8_fp64"):
+        assert bench.WORKLOADS[name].full is not None, name
     assert set(bench.ENERGY_KERNELS) == {"plaplace", "gl", "he", "mc"}
 
 
@@ -59,3 +63,25 @@ def test_reference_arm_line_for_newton_sample(tmp_path):
     assert line["metric"] == "Newton s to 1e-6 rel-grad" and line["value"] > 0
     for key in ("cpu_baseline", "e2e", "config", "n_gpus", "steps", "warmup", "ms_per_step"):
         assert key in line
+
+
+@pytest.mark.timeout(600)
+def test_reference_arm_runs_the_full_configuration(tmp_path):
+    """For P1 workloads the reference arm times the whole configuration and
+    prints the same ``config`` object the CUDA arm prints."""
+    import bench
+    from oracle.assembler import OracleAssembler
+
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "plaplace128_fp64", "--steps", "2", "--warmup", "1"], capture_output=True, text=True,
+                         cwd=tmp_path, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    w = bench.WORKLOADS["plaplace128_fp64"]
+    family, okw, params, _, _, _ = w.full()
+    orc = OracleAssembler(family, params, **okw)
+    n_el = int(orc.local.local_elem_idx.size)
+    assert line["config"] == bench.workload_config(w, n_el, orc.layout.n_free, orc.layout.owned_rows.size, 1)
+    # elements with a free DOF (the two corner triangles have none), owned COO entries
+    assert line["config"]["elements"] == 32_766 and line["config"]["coo_nnz"] == 111_889
+    assert line["cpu_baseline"]["sample"].startswith("full configuration")

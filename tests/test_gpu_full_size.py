@@ -1,0 +1,178 @@
+"""Parity at the benchmark configurations' full sizes, entry by entry.
+
+Every configuration the benchmark measures, on its full mesh, against the
+FP64 oracle (``oracle/``, itself checked against the reference's own
+outputs in ``test_reference_fixtures.py``): the energy, every owned gradient
+entry and every owned COO Hessian value -- except the P4 slope, whose
+oracle pass over 203,000 elements would take many minutes on the host; it is
+checked on 400 sampled owned rows (every gradient entry and COO value of
+those rows, from all elements touching them).  The oracle reuses the CUDA
+assembler's layout (the layout builders are pinned bit-for-bit to the
+reference's).  Bars: FP64 mode 1e-12 relative (energy vs the sum of
+|element energy| (+ |load term|), gradient / Hessian vs their largest
+entry); FP32-Hessian mode 2e-5 (Hessian), 1e-4 (gradient), 1e-6 (energy,
+reduced in FP64; 1e-5 for Mohr-Coulomb).
+"""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from fenics_nonlinear_energies_b200 import _lib, meshes
+from oracle import energies
+from oracle.assembler import OracleAssembler, restricted_rows
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": (1e-12, 1e-12, 1e-12), "fp32": (1e-6, 1e-4, 2e-5)}
+
+
+def rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.abs(a - b).max(initial=0.0) / max(np.abs(b).max(initial=0.0), 1e-300)
+
+
+def _energy_scale(orc, u):
+    """Sum of |element energy| plus |load term|: the scale of the energy's rounding."""
+    v = orc.v_local(u)[orc.local.elems_local_np]
+    e, _, _ = energies.element_derivatives(orc.family, v, orc.elem_data, orc.params, want_hessian=False)
+    load = abs(float(orc.f_owned @ np.asarray(u)[orc.layout.lo: orc.layout.hi])) if orc.f_owned.size else 0.0
+    return float(np.abs(e).sum()) + load + abs(orc.dirichlet_only_energy)
+
+
+def _run(asm, u):
+    e, g, h = asm.eval(torch.as_tensor(u, device="cuda"), _lib.FNE_ENERGY | _lib.FNE_GRAD | _lib.FNE_HESS)
+    torch.cuda.synchronize()
+    asm.check_device_status()
+    return float(e.item()), g[: asm.n_owned].cpu().numpy(), h.double().cpu().numpy()
+
+
+def _compare(asm, orc, u, precision, *, e_tol_scale=1.0):
+    e_ref, g_ref, h_ref = orc.all_in_one(u)
+    e, g, h = _run(asm, u)
+    te, tg, th = TOL[precision]
+    assert abs(e - e_ref) <= te * e_tol_scale * max(1.0, _energy_scale(orc, u)), (e, e_ref)
+    assert rel(g, g_ref) <= tg, rel(g, g_ref)
+    assert rel(h, h_ref) <= th, rel(h, h_ref)
+    assert h.size == orc.layout.owned_rows.size
+
+
+def _kw(precision):
+    return dict(precision=precision, hess_dtype=torch.float32 if precision == "fp32" else torch.float64)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_plaplace_128_zero_state(precision):
+    """p-Laplace 128 x 128 (32,768 triangles), p = 3, f = -10, u = 0: the
+    Hessian is exactly zero (limit of (s)^(p/2) at s = 0), the gradient is -f."""
+    from fenics_nonlinear_energies_b200.assembler import PLaplaceCudaAssembler
+
+    params, _ = meshes.plaplace_problem(n=128)
+    asm = PLaplaceCudaAssembler(params, **_kw(precision))
+    orc = OracleAssembler("plaplace", params, layout=asm.layout)
+    u = np.zeros(asm.layout.n_free)
+    _compare(asm, orc, u, precision)
+    _, _, h = _run(asm, u)
+    assert not np.any(h)
+
+
+@pytest.fixture(scope="module")
+def gl1024():
+    params, u0 = meshes.gl_problem(n=1024, seed=0)
+    return params, u0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gl_1024(gl1024, precision):
+    """Ginzburg-Landau 1024 x 1024 (2,097,152 triangles, 7,317,521 COO values), seeded state."""
+    from fenics_nonlinear_energies_b200.assembler import GLCudaAssembler
+
+    params, u0 = gl1024
+    asm = GLCudaAssembler(params, **_kw(precision))
+    orc = OracleAssembler("gl", params, layout=asm.layout)
+    _compare(asm, orc, u0, precision)
+
+
+def _he_state(params, asm, k):
+    """Load step k of 24 toward 4 pi: right face rotated, interior twisted
+    linearly along the beam, plus a seeded perturbation."""
+    angle = k * 4.0 * math.pi / 24.0
+    rotated = meshes.rotate_right_face_from_reference(params["u_0_ref"], params["nodes2coord"], angle,
+                                                      params["right_nodes"])
+    X = params["nodes2coord"]
+    a = angle * X[:, 0] / X[:, 0].max()
+    Y = X.copy()
+    Y[:, 1] = np.cos(a) * X[:, 1] + np.sin(a) * X[:, 2]
+    Y[:, 2] = -np.sin(a) * X[:, 1] + np.cos(a) * X[:, 2]
+    y_full = Y.reshape(-1) + 1e-4 * np.random.default_rng(k).standard_normal(Y.size)
+    u = np.zeros(asm.layout.n_free)
+    u[asm.layout.total_to_free_reord[params["freedofs"]]] = y_full[params["freedofs"]]
+    return rotated, u
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_he_beam_160x8x8_twisted(precision):
+    """Neo-Hookean beam 160 x 8 x 8 hexes (61,440 tets), third load step of the 4 pi twist."""
+    from fenics_nonlinear_energies_b200.assembler import HECudaAssembler
+
+    params, _ = meshes.he_beam_problem()
+    asm = HECudaAssembler(params, **_kw(precision))
+    rotated, u = _he_state(params, asm, 3)
+    asm.update_dirichlet(rotated)
+    orc = OracleAssembler("he", params, block_size=3, coordinate_key="nodes2coord", dirichlet_key="u_0_ref",
+                          layout=asm.layout)
+    orc.update_dirichlet(rotated)
+    _compare(asm, orc, u, precision)
+
+
+def _slope_state(params, asm):
+    """A smooth field that drives part of the slope into the plastic branches."""
+    nodes = params["nodes"]
+    ux = 2e-3 * np.sin(0.11 * nodes[:, 0]) * (nodes[:, 1] / 20.0)
+    uy = -4e-3 * (nodes[:, 1] / 20.0) ** 2 + 1e-3 * np.cos(0.07 * nodes[:, 0] + 0.2 * nodes[:, 1])
+    un = np.stack([ux, uy], axis=1).reshape(-1)
+    u = np.zeros(asm.layout.n_free)
+    u[asm.layout.total_to_free_reord[params["freedofs"]]] = un[params["freedofs"]]
+    return u
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_mc_p2_h008(precision):
+    """Mohr-Coulomb slope, P2 at h = 0.08 (the reference's P2 generator and
+    isoparametric map), partly plastic state, every entry."""
+    from fenics_nonlinear_energies_b200.assembler import SlopeStabilityCudaAssembler
+
+    params = meshes.slope_problem(h=0.08, degree=2, with_elem_B=True)
+    asm = SlopeStabilityCudaAssembler(params, **_kw(precision))
+    orc = OracleAssembler("mc", params, block_size=2, layout=asm.layout)
+    u = _slope_state(params, asm)
+    _compare(asm, orc, u, precision, e_tol_scale=10.0 if precision == "fp32" else 1.0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_mc_p4_h008_sampled_rows(precision):
+    """Mohr-Coulomb slope, P4 at h = 0.08 (203,000 elements, 152 M COO values):
+    400 sampled owned rows, all their gradient entries and COO values."""
+    from fenics_nonlinear_energies_b200.assembler import SlopeStabilityCudaAssembler
+
+    params = meshes.slope_problem(h=0.08, degree=4)
+    assert params["elems"].shape[0] == 203_000
+
+    class _ElemB:  # the reference-layout operators of the touched elements only (all of them: 3.7 GB)
+        def __getitem__(self, idx):
+            return meshes.slope_elem_B({k: params[k] for k in ("dhat1", "dhat2")} | {"inv_jac": params["inv_jac"][idx]})
+
+    params["elem_B"] = _ElemB()
+    asm = SlopeStabilityCudaAssembler(params, **_kw(precision))
+    u = _slope_state(params, asm)
+    _, g, h = _run(asm, u)
+    lay = asm.layout
+    rows = np.sort(np.random.default_rng(11).choice(np.arange(lay.lo, lay.hi), 400, replace=False))
+    force = np.asarray(params["force"])[params["freedofs"]][lay.perm][lay.lo: lay.hi]
+    g_ref, pos, h_ref = restricted_rows("mc", params, lay, u, rows, dirichlet_full=params["u_0"], f_owned=force)
+    _, tg, th = TOL[precision]
+    assert pos.size > 400 * 20
+    assert rel(g[rows - lay.lo], g_ref) <= tg
+    assert rel(h[pos], h_ref) <= th

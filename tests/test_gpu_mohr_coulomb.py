@@ -300,3 +300,29 @@ def test_mc_energy_gradient_kernel(degree, precision):
     assert _rel(g2.cpu().numpy(), gc.cpu().numpy()) <= ctol
     assert torch.equal(gpu.eval(ut, _lib.FNE_GRAD)[1], g2)
     assert float(gpu.eval(ut, _lib.FNE_ENERGY)[0].item()) == e1
+
+
+def test_tensor_core_wait_timeout_is_reported():
+    """The tcgen05 kernel's MMA-completion wait, set to give up at once
+    (fne_set_wait_limit 0): the pass returns, the status word reports
+    FNE_ETIMEOUT (polled without a sync by the callbacks, or read
+    synchronously), and with the default bound restored the same handle
+    gives correct values again (the context stayed usable)."""
+    params = meshes.slope_problem(level=1, degree=2, lam=1.2, with_elem_B=True)
+    gpu, ref = _pair(params, precision="fp32", hess_dtype=torch.float32)
+    assert gpu.info["kernel_variant"] == 6
+    u = 0.05 * np.random.default_rng(3).standard_normal(gpu.layout.n_free)
+    ut = torch.as_tensor(u, device="cuda")
+    _lib.check(_lib.lib.fne_set_wait_limit(gpu._handle, 0))
+    gpu.eval(ut, 7)
+    torch.cuda.synchronize()
+    assert _lib.lib.fne_check_device_status(gpu._handle) == _lib.FNE_ETIMEOUT
+    assert _lib.lib.fne_check_device_status(gpu._handle) == _lib.FNE_OK  # cleared
+    with pytest.raises(_lib.FneError) as err:
+        gpu.assemble_hessian(u)
+    assert err.value.code == _lib.FNE_ETIMEOUT
+    _lib.check(_lib.lib.fne_set_wait_limit(gpu._handle, -1))
+    _, _, h_ref = ref.all_in_one(u)
+    gpu.assemble_hessian(u)  # no error now
+    assert _rel(gpu.owned_values.double().cpu().numpy(), h_ref) <= FP32_TOL
+    gpu.check_device_status()

@@ -159,3 +159,47 @@ def test_scalar_cg_oracle(case):
     else:
         assert (it, why) == (0, krylov.ZERO_RHS) and not x.any()
     np.testing.assert_array_equal(krylov.jacobi_scaling([2.0, -4.0, 0.0, np.nan]), [0.5, 0.25, 1.0, 1.0])
+
+
+def test_oracle_adopted_layout_and_restricted_rows():
+    """A precomputed layout gives the same callbacks; ``restricted_rows`` equals
+    the full assembly on the rows it covers (used by the full-size GPU tests)."""
+    from fenics_nonlinear_energies_b200 import _lib
+
+    p = meshes.slope_problem(level=1, degree=4, with_elem_B=True)
+    full = OracleAssembler("mc", p, block_size=2)
+    lay = _lib.build_layout(freedofs=p["freedofs"], elems=p["elems"], n_total=len(p["u_0"]), block_size=2,
+                            coords=p["nodes"])
+    lay["n_free"] = full.layout.n_free
+    adopted = OracleAssembler("mc", p, block_size=2, layout=lay)
+    u = 2e-3 * np.random.default_rng(4).standard_normal(full.layout.n_free)
+    e0, g0, h0 = full.all_in_one(u)
+    e1, g1, h1 = adopted.all_in_one(u)
+    assert e0 == e1 and np.array_equal(g0, g1) and np.array_equal(h0, h1)
+    rows = np.random.default_rng(5).choice(full.layout.n_free, 40, replace=False)
+    g, pos, vals = full.restricted_rows(u, rows)
+    np.testing.assert_allclose(g, g0[np.sort(rows)], rtol=0, atol=1e-13 * np.abs(g0).max())
+    np.testing.assert_array_equal(np.sort(pos), np.flatnonzero(np.isin(full.layout.owned_rows, rows)))
+    np.testing.assert_allclose(vals, h0[pos], rtol=0, atol=1e-13 * np.abs(h0).max())
+
+
+@pytest.mark.parametrize("family", ["gl", "plaplace"])
+def test_numba_cpu_line_matches_oracle(family):
+    """The numba-parallel CPU line of the benchmark equals the oracle."""
+    from oracle.cpu_fast import FastTriangleAssembler
+
+    if family == "gl":
+        params, u = meshes.gl_problem(n=24, seed=4)
+    else:
+        params, _ = meshes.plaplace_problem(n=24)
+        u = None
+    orc = OracleAssembler(family, params)
+    fast = FastTriangleAssembler(orc)
+    states = [u[orc.layout.perm]] if u is not None else [
+        0.3 * np.random.default_rng(2).standard_normal(orc.layout.n_free), np.zeros(orc.layout.n_free)]
+    for s in states:
+        e0, g0, h0 = orc.all_in_one(s)
+        e1, g1, h1 = fast.all_in_one(s)
+        assert abs(e1 - e0) <= 1e-12 * max(1.0, abs(e0))
+        np.testing.assert_allclose(g1, g0, rtol=0, atol=1e-12 * max(1e-300, np.abs(g0).max()))
+        np.testing.assert_allclose(h1, h0, rtol=0, atol=1e-12 * max(1e-300, np.abs(h0).max()))
