@@ -410,7 +410,7 @@ WORKLOADS = {
     "mc_p4_h0.08_fp64": Workload(
         "mc_p4_h0.08_fp64", "mc", "fp64", False, 15, 5, 8, True,
         "Mohr-Coulomb plane-strain slope 40x20 (height 10, 1:1), P4 triangles h=0.08 (203,000 elements), "
-        "c=6, phi=45 deg, E=2e4, nu=0.49, lambda=1 (Davis-B), 25-point rule, smooth synthetic state, FP64",
+        "c=6, phi=45 deg, E=2e4, nu=0.49, lambda=1 (Davis-B), 19-point degree-9 rule, smooth synthetic state, FP64",
         *_mc(4, 0.08, "fp64")),
     "mc_p4_h0.08_fp32": Workload(
         "mc_p4_h0.08_fp32", "mc", "fp32", True, 15, 5, 8, True,

@@ -1599,7 +1599,7 @@ cudaError_t mc_dispatch(McHandle* h, int flags, const double* u, double* energy,
   if (h->np == 6 && h->nq == 7)
     return h->gq ? mc_launch<Real, HOut, 6, 7, true>(h, flags, u, energy, grad, hess, st)
                  : mc_launch<Real, HOut, 6, 7, false>(h, flags, u, energy, grad, hess, st);
-  if (h->np == 15 && h->nq == 25) return mc_launch<Real, HOut, 15, 25, false>(h, flags, u, energy, grad, hess, st);
+  if (h->np == 15 && h->nq == 19) return mc_launch<Real, HOut, 15, 19, false>(h, flags, u, energy, grad, hess, st);
   return cudaErrorInvalidValue;
 }
 
@@ -1691,8 +1691,8 @@ int mc_create(const fne_desc* d, McHandle** out) {
   *out = nullptr;
   const int np = d->npe, nq = d->nq, n = 2 * np;
   if (d->block_size != 2) return set_error(FNE_EINVAL, "Mohr-Coulomb: block_size must be 2");
-  if (!((np == 3 && nq == 1) || (np == 6 && nq == 7) || (np == 15 && nq == 25)))
-    return set_error(FNE_EINVAL, "Mohr-Coulomb: supported (nodes, quadrature points): (3,1), (6,7), (15,25)");
+  if (!((np == 3 && nq == 1) || (np == 6 && nq == 7) || (np == 15 && nq == 19)))
+    return set_error(FNE_EINVAL, "Mohr-Coulomb: supported (nodes, quadrature points): (3,1), (6,7), (15,19)");
   if (d->n_elem > 0 && (!d->e0 || !d->e1 || !d->e3))
     return set_error(FNE_EINVAL, "Mohr-Coulomb: missing element geometry or reference tables");
   const int64_t E = d->n_elem, lo = d->lo, hi = d->hi;
@@ -1939,7 +1939,7 @@ int mc_create(const fne_desc* d, McHandle** out) {
     MC_TRY(mc_upload(h, &h->fx_desc, dp.fdesc.data(), dp.fdesc.size()));
   }
   if (h->dm) {
-    const int rc_dm = np == 15 ? mc_dm_prepare<15, 25, false>(h)
+    const int rc_dm = np == 15 ? mc_dm_prepare<15, 19, false>(h)
                                : (h->gq ? mc_dm_prepare<6, 7, true>(h) : mc_dm_prepare<6, 7, false>(h));
     if (rc_dm) {
       mc_destroy(h);
@@ -1948,7 +1948,7 @@ int mc_create(const fne_desc* d, McHandle** out) {
   }
   if (h->tc) {
     std::vector<float> phi, plo;
-    int rc_tc = np == 15 ? mc_tc_prepare<15, 25, false>(h, d->e3, phi, plo)
+    int rc_tc = np == 15 ? mc_tc_prepare<15, 19, false>(h, d->e3, phi, plo)
                          : (h->gq ? mc_tc_prepare<6, 7, true>(h, d->e3, phi, plo)
                                   : mc_tc_prepare<6, 7, false>(h, d->e3, phi, plo));
     if (rc_tc) {
@@ -2043,7 +2043,7 @@ template <typename Real>
 cudaError_t mc_lin_dispatch(McHandle* h, int op, const double* v, double* out, cudaStream_t st) {
   if (h->np == 3 && h->nq == 1) return mc_lin_launch<Real, 3, 1>(h, op, v, out, st);
   if (h->np == 6 && h->nq == 7) return mc_lin_launch<Real, 6, 7>(h, op, v, out, st);
-  if (h->np == 15 && h->nq == 25) return mc_lin_launch<Real, 15, 25>(h, op, v, out, st);
+  if (h->np == 15 && h->nq == 19) return mc_lin_launch<Real, 15, 19>(h, op, v, out, st);
   return cudaErrorInvalidValue;
 }
 

@@ -341,11 +341,55 @@ def gauss_jacobi_triangle(n):
     return np.array([X, Y]), np.array(W)
 
 
+# Fully symmetric 19-point rule exact to degree 9 on the triangle: the centroid,
+# four (a, a, 1-2a) orbits and one (a, b, 1-a-b) orbit, weights normalised to
+# sum 1.  Values of Dunavant, "High degree efficient symmetrical Gaussian
+# quadrature rules for the triangle", IJNME 21 (1985) 1129-1148, degree 9,
+# refined to double precision by Newton's method on the moment equations of
+# every monomial of degree <= 9 (the refinement moves the published 15-digit
+# values by < 4e-16).  Its orbit structure (1 + 4x3 + 6 = 19 points, 12
+# unknowns for 12 invariant moments) is that of the 19-point degree-9 rule of
+# Xiao & Gimbutas (2010), which basix's make_quadrature(triangle, 9) -- the
+# reference's P4 rule -- returns.
+DEG9_CENTROID_W = 0.09713579628279883
+DEG9_ORBITS_A = (  # (a, w): points (1-2a, a, a) and permutations
+    (0.4896825191987376, 0.03133470022713907),
+    (0.4370895914929366, 0.07782754100477428),
+    (0.1882035356190327, 0.07964773892721025),
+    (0.04472951339445271, 0.02557767565869803),
+)
+DEG9_ORBIT_AB = (0.2219629891607657, 0.03683841205473628, 0.04328353937728938)  # (a, b, w)
+
+
+def triangle_rule_degree9():
+    """(xi (2, 19), w (19,)) of the 19-point degree-9 rule on the reference
+    triangle (area 1/2): centroid, then each (a, a, 1-2a) orbit, then the
+    six points of the (a, b, 1-a-b) orbit."""
+    bary, w = [(1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0)], [DEG9_CENTROID_W]
+    for a, wa in DEG9_ORBITS_A:
+        b = 1.0 - 2.0 * a
+        bary += [(b, a, a), (a, b, a), (a, a, b)]
+        w += [wa] * 3
+    a, b, wab = DEG9_ORBIT_AB
+    c = 1.0 - a - b
+    bary += [(a, b, c), (b, a, c), (a, c, b), (c, a, b), (b, c, a), (c, b, a)]
+    w += [wab] * 6
+    bary = np.asarray(bary, dtype=np.float64)
+    return np.stack([bary[:, 1], bary[:, 2]]), 0.5 * np.asarray(w, dtype=np.float64)
+
+
 def slope_quadrature(degree):
+    """The reference's triangle rule for element degree ``degree``: the
+    13-digit 7-point rule for P2, the centroid for P1, the degree-9 rule for
+    P4 (``make_quadrature(triangle, 2p+1)``,
+    ``src/problems/slope_stability/support/mesh.py:293-296``); a collapsed
+    Gauss-Jacobi rule of the same exactness for other degrees."""
     if degree == 2:
         return P2_QUAD_XI.copy(), P2_QUAD_W.copy()
     if degree == 1:
         return np.array([[1.0 / 3.0], [1.0 / 3.0]]), np.array([0.5])
+    if degree == 4:
+        return triangle_rule_degree9()
     return gauss_jacobi_triangle(degree + 1)  # degree 2*deg+1 exactness
 
 

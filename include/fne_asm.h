@@ -146,7 +146,7 @@ typedef struct {
    *                    src/problems/slope_stability/support/mesh.py:530-567),
    *                    e2 = eps_p_old [E*nq*3] or NULL (zero),
    *                    e3 = reference tables [dhat1 (nq*np) | dhat2 (nq*np) | w (nq)],
-   *                    npe = np (3, 6 or 15), block_size = 2, nq = 1, 7 or 25 */
+   *                    npe = np (3, 6 or 15), block_size = 2, nq = 1, 7 or 19 */
   const double* e0;
   const double* e1;
   const double* e2;

@@ -175,7 +175,8 @@ class OracleAssembler:
         return val, g, vals
 
 
-def restricted_rows(family, params, layout, u_full_reordered, rows, *, dirichlet_full, f_owned=None):
+def restricted_rows(family, params, layout, u_full_reordered, rows, *, dirichlet_full, f_owned=None,
+                    with_scale=False):
     """Gradient entries and owned COO Hessian values of the owned reordered
     rows ``rows`` only, from the elements that touch them: the same sums as
     ``gradient_fn`` / ``assemble_hessian_element`` restricted to those rows
@@ -183,7 +184,9 @@ def restricted_rows(family, params, layout, u_full_reordered, rows, *, dirichlet
     full overlap / scatter data -- for meshes where the full oracle pass is
     too slow.  ``layout`` needs ``lo, n_free, total_to_free_reord,
     owned_rows, owned_cols``.  Returns ``(grad[sorted rows], positions,
-    values)`` with positions into the owned COO order."""
+    values)`` with positions into the owned COO order; with ``with_scale`` also
+    the per-row sum of |element contributions| (+ |load|), the scale of the
+    rounding of a low-precision gradient sum."""
     get = (lambda k: layout[k]) if isinstance(layout, dict) else (lambda k: getattr(layout, k))  # noqa: E731
     lo, n_free = int(get("lo")), int(get("n_free"))
     t2f = np.asarray(get("total_to_free_reord"), dtype=np.int64)
@@ -201,8 +204,11 @@ def restricted_rows(family, params, layout, u_full_reordered, rows, *, dirichlet
     grad = np.zeros(rows.size)
     ei, li = np.nonzero(sel)
     np.add.at(grad, np.searchsorted(rows, er[ei, li]), g_e[ei, li])
+    scale = np.zeros(rows.size)
+    np.add.at(scale, np.searchsorted(rows, er[ei, li]), np.abs(g_e[ei, li]))
     if f_owned is not None and np.size(f_owned):
         grad -= np.asarray(f_owned)[rows - lo]
+        scale += np.abs(np.asarray(f_owned)[rows - lo])
     pos_all = np.flatnonzero(np.isin(orow, rows))
     keys_sub = orow[pos_all] * np.int64(n_free) + ocol[pos_all]
     order = np.argsort(keys_sub, kind="mergesort")
@@ -215,4 +221,6 @@ def restricted_rows(family, params, layout, u_full_reordered, rows, *, dirichlet
     uniq, inv = np.unique(pos, return_inverse=True)
     vals = np.zeros(uniq.size)
     np.add.at(vals, inv, h_e[ei, li, lj])
+    if with_scale:
+        return grad, uniq, vals, scale
     return grad, uniq, vals

@@ -10,8 +10,9 @@ those rows, from all elements touching them).  The oracle reuses the CUDA
 assembler's layout (the layout builders are pinned bit-for-bit to the
 reference's).  Bars: FP64 mode 1e-12 relative (energy vs the sum of
 |element energy| (+ |load term|), gradient / Hessian vs their largest
-entry); FP32-Hessian mode 2e-5 (Hessian), 1e-4 (gradient), 1e-6 (energy,
-reduced in FP64; 1e-5 for Mohr-Coulomb).
+entry); FP32-Hessian mode 2e-5 (Hessian), 1e-4 (gradient; on the sampled P4
+rows against the largest row sum of |element contributions|, the scale of an
+FP32 sum), 1e-6 (energy, reduced in FP64; 1e-5 for Mohr-Coulomb).
 """
 
 import math
@@ -171,8 +172,16 @@ def test_mc_p4_h008_sampled_rows(precision):
     lay = asm.layout
     rows = np.sort(np.random.default_rng(11).choice(np.arange(lay.lo, lay.hi), 400, replace=False))
     force = np.asarray(params["force"])[params["freedofs"]][lay.perm][lay.lo: lay.hi]
-    g_ref, pos, h_ref = restricted_rows("mc", params, lay, u, rows, dirichlet_full=params["u_0"], f_owned=force)
+    g_ref, pos, h_ref, g_scale = restricted_rows("mc", params, lay, u, rows, dirichlet_full=params["u_0"],
+                                                 f_owned=force, with_scale=True)
     _, tg, th = TOL[precision]
     assert pos.size > 400 * 20
-    assert rel(g[rows - lay.lo], g_ref) <= tg
+    err = np.abs(g[rows - lay.lo] - g_ref).max()
+    if precision == "fp64":
+        assert err <= tg * np.abs(g_ref).max()
+    else:
+        # FP32 element gradients summed in FP32: rounding scales with the sum of
+        # |element contributions| of a row, which at nu = 0.49 (lambda / mu = 49)
+        # is far above the net residual of the smooth synthetic state
+        assert err <= tg * g_scale.max(), (err, g_scale.max(), np.abs(g_ref).max())
     assert rel(h[pos], h_ref) <= th

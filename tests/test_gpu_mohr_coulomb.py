@@ -102,7 +102,7 @@ def test_mc_plastic_points_present():
     el = energies.element_derivatives("mc", v, ref.elem_data, dict(params, elastic=True), want_hessian=False)[0]
     pl = energies.element_derivatives("mc", v, ref.elem_data, params, want_hessian=False)[0]
     assert np.mean(np.abs(el - pl) > 1e-12 * np.abs(el)) > 0.1
-    assert strain.shape[1] == 25
+    assert strain.shape[1] == 19
 
 
 def test_mc_fp32():

@@ -54,6 +54,24 @@ def test_gauss_jacobi_exactness(n):
             assert abs((w * xi[0] ** i * xi[1] ** j).sum() - exact) <= 1e-13 * exact
 
 
+def test_p4_rule_degree9():
+    """The P4 rule (the reference's make_quadrature(triangle, 9)): 19 points
+    inside the triangle, positive weights, exact on every monomial of degree
+    <= 9, and within rounding of Dunavant's published 15-digit table."""
+    xi, w = meshes.slope_quadrature(4)
+    assert xi.shape == (2, 19) and w.shape == (19,)
+    assert (w > 0).all() and (xi > 0).all() and (xi.sum(0) < 1).all()
+    for i in range(10):
+        for j in range(10 - i):
+            exact = math.factorial(i) * math.factorial(j) / math.factorial(i + j + 2)
+            assert abs((w * xi[0] ** i * xi[1] ** j).sum() - exact) <= 2e-15 * exact, (i, j)
+    published = [0.097135796282799, 0.489682519198738, 0.031334700227139, 0.437089591492937, 0.077827541004774,
+                 0.188203535619033, 0.079647738927210, 0.044729513394453, 0.025577675658698, 0.221962989160766,
+                 0.036838412054736, 0.043283539377289]
+    ours = [meshes.DEG9_CENTROID_W] + [v for aw in meshes.DEG9_ORBITS_A for v in aw] + list(meshes.DEG9_ORBIT_AB)
+    np.testing.assert_allclose(ours, published, rtol=0, atol=1e-15)
+
+
 def test_lagrange_tabulation_partition_of_unity():
     for k in (1, 2, 4):
         xi, _ = meshes.slope_quadrature(k)
