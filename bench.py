@@ -472,7 +472,7 @@ REFERENCE_ARCHIVED = {
 
 KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri",
                 5: "k_mc_elem+k_node_gather+k_rowgrad", 6: "k_mc_tc+k_fixup2+k_rowgrad", 7: "k_he_elem+k_node_gather",
-                8: "k_push_tri", 9: "k_mc_dmma+k_fixup2+k_rowgrad"}
+                8: "k_push_tri", 9: "k_mc_dmma+k_fixup2+k_rowgrad", 10: "k_cluster_tri"}
 
 
 def algorithmic_bytes(w, asm, n_el, energy_only=False):
@@ -1082,8 +1082,8 @@ def main():
     ap.add_argument("--pass", dest="pass_", default="egh", choices=["egh", "energy"],
                     help="egh: fused energy + gradient + Hessian pass (default); energy: the energy-only pass "
                          "(the line-search callback)")
-    ap.add_argument("--kernel-variant", default="auto", choices=["auto", "row_gather", "incidence", "element", "cuda_cores", "push",
-                                                                  "row_lanes_2", "row_lanes_4", "row_lanes_8"])
+    ap.add_argument("--kernel-variant", default="auto", choices=["auto", "sweep", "cluster", "row_gather", "incidence", "element", "cuda_cores",
+                                                                  "push", "row_lanes_2", "row_lanes_4", "row_lanes_8"])
     args = ap.parse_args()
     KERNEL_VARIANT["value"] = args.kernel_variant
     if args.warmup < 3 and args.impl == "b200":

@@ -128,9 +128,9 @@ class CudaElementAssemblerBase:
             d.s[i] = float(v)
         d.nq = int(self._nq())
         d.dirichlet_only_energy = 1 if (self._adds_dirichlet_only_energy() and self.rank == 0) else 0
-        d.kernel_variant = {"auto": 0, "row_gather": 1, "incidence": 2, "element": 2,
+        d.kernel_variant = {"auto": 0, "cluster": 8, "row_gather": 1, "incidence": 2, "element": 2,
                             "cuda_cores": 1, "push": 3, "row_lanes_2": 4, "row_lanes_4": 5,
-                            "row_lanes_8": 6}[kernel_variant]
+                            "row_lanes_8": 6, "sweep": 7}[kernel_variant]
         self._handle = _lib.C.c_void_p()
         check(lib.fne_create(_lib.C.byref(d), _lib.C.byref(self._handle)))
         del keep

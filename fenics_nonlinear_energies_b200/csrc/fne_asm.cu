@@ -1193,6 +1193,8 @@ __global__ void __launch_bounds__(NB, 2) k_push_tri(RowArgs A, SweepArgs S, cons
   if (WANT & W_E) energy_finalize(eacc, eo);
 }
 
+#include "fne_cluster.cuh"
+
 // ---------------------------------------------------------------------------
 // energy-only kernels (element-centric, grid-stride)
 // ---------------------------------------------------------------------------
@@ -1369,6 +1371,18 @@ struct fne_handle {
   bool use_inc = false;
   bool use_sweep = false;
   bool use_push = false;
+  // row-cluster kernel (P1 triangles, default)
+  bool use_cluster = false;
+  int cl_n_jobs = 0, cl_n_cl = 0, cl_cap_j = 0, cl_cap_r = 0, cl_cap_u = 0, cl_cap_i = 0, cl_cap_w = 0;
+  long long cl_wait_limit = kClWaitLimit;
+  int4* cl_table = nullptr;
+  int* cl_codes = nullptr;
+  void* cl_reals = nullptr;
+  int4* cl_rows = nullptr;
+  int4* cl_runs = nullptr;
+  unsigned* cl_incs = nullptr;
+  int* err = nullptr;       // status word of the row-cluster kernel
+  int* err_host = nullptr;  // pinned copy after each pass
   unsigned long long* sw_eoff = nullptr;
   int* sw_row_of = nullptr;
   int sweep_nb = 0, sweep_win_mask = 0, sweep_rwin_mask = 0;
@@ -1440,9 +1454,11 @@ void free_handle(fne_handle* h) {
                   h->sw_ent_row, h->sw_ent_pos, h->sw_ent_meta, h->sw_inc_word, h->sw_eoff, h->sw_row_of,
                   h->dir, h->rhs, h->partials, h->dir_const, h->counter, h->h_u, h->h_grad, h->h_energy,
                   h->h_hess, h->e2_kbuf, h->e2_gbuf, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row,
-                  h->bp_rn_gpos, h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk};
+                  h->bp_rn_gpos, h->bp_rn_inc, h->bp_con, h->bp_inc, h->bp_blk, h->cl_table,
+                  h->cl_codes, h->cl_reals, h->cl_rows, h->cl_runs, h->cl_incs, h->err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (h->err_host) cudaFreeHost(h->err_host);
   delete h;
 }
 
@@ -1520,6 +1536,26 @@ void pack_tet(const fne_desc* d, bool f32, const std::vector<int64_t>& elems, co
   }
 }
 
+// job records of the row-cluster kernel (layout in fne_cluster.cuh)
+template <typename Real>
+void pack_cluster_jobs(const fne_desc* d, const RowPlan& P, const ClusterPlan& Q, std::vector<int32_t>& codes,
+                       std::vector<Real>& reals) {
+  const size_t n = Q.job_elem.size();
+  codes.assign(3 * n, -1);  // padding jobs: a valid gather code (the Dirichlet value of DOF 0)
+  reals.assign(7 * n, Real(0));
+  for (size_t j = 0; j < n; ++j) {
+    const int32_t le = Q.job_elem[j];
+    if (le < 0) continue;
+    const int64_t e = P.local_elems[le];
+    reals[j] = (Real)d->e2[e];
+    for (int a = 0; a < 3; ++a) {
+      codes[a * n + j] = P.elem_code[(size_t)le * 3 + a];
+      reals[(1 + a) * n + j] = (Real)d->e0[e * 3 + a];
+      reals[(4 + a) * n + j] = (Real)d->e1[e * 3 + a];
+    }
+  }
+}
+
 bool is_tri(int fam) { return fam == FNE_PLAPLACE || fam == FNE_GINZBURG_LANDAU; }
 
 // ---- kernel dispatch -------------------------------------------------------
@@ -1527,12 +1563,20 @@ template <typename Real, int FAM, typename HOut>
 cudaError_t launch_tri_t(fne_handle* h, int want, const RowArgs& A, const IncArgs& Q, const SweepArgs& SW,
                          double* grad, void* hess, EnergyOut eo, cudaStream_t st, bool set_attr) {
   HOut* H = static_cast<HOut*>(hess);
+  const ClusterArgs CL{h->cl_table,  h->cl_codes, h->cl_reals, h->cl_rows,  h->cl_runs,
+                       h->cl_incs,   h->err,      h->cl_wait_limit, h->cl_n_jobs, h->cl_cap_j,
+                       h->cl_cap_r,  h->cl_cap_u, h->cl_cap_i, h->cl_cap_w};
   const size_t sm = h->smem_bytes;
   const dim3 grid(h->grid_rows);
   constexpr int NBS = sizeof(Real) == 4 ? 512 : 256;
 #define FNE_TRI_CASE(W)                                                                                        \
   case W:                                                                                                      \
-    if (h->use_push) {                                                                                         \
+    if (h->use_cluster) {                                                                                      \
+      if (set_attr)                                                                                            \
+        return cudaFuncSetAttribute(k_cluster_tri<Real, FAM, W, HOut>,                                        \
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                     \
+      k_cluster_tri<Real, FAM, W, HOut><<<grid, kClThreads, sm, st>>>(A, CL, h->phys, grad, H, eo, h->cl_n_cl); \
+    } else if (h->use_push) {                                                                                  \
       if (set_attr)                                                                                            \
         return cudaFuncSetAttribute(k_push_tri<Real, FAM, W, HOut, NBS>,                                      \
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);                     \
@@ -1790,7 +1834,46 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   if (is_tri(d->family) && plan.n_rows > 0 && d->kernel_variant == 2)
     use_inc = build_inc_plan(plan, kIncThreads, inc);
   const bool want_push = is_tri(d->family) && d->kernel_variant == 3;
-  if (is_tri(d->family) && plan.n_rows > 0 && (d->kernel_variant == 0 || want_push)) {
+  // row clusters for triangles (default): windows of at most 8191 slots, sized
+  // for three CTAs per SM, and about as many clusters as a whole number of
+  // waves of them
+  ClusterPlan cplan;
+  bool use_cluster = false;
+  if (is_tri(d->family) && plan.n_rows > 0 && d->kernel_variant == 8) {
+    // one persistent CTA per SM holding two staging buffers and the window:
+    // the buffers (jobs, row / run records, incidence words) and the window
+    // share the shared memory in the proportion the mesh needs (jobs per row
+    // ~ local elements per row plus the cluster border, incidences per row ~
+    // 3 x local elements per row), with 10 % slack for irregular clusters;
+    // small meshes get smaller clusters so that every SM has several
+    const int64_t budget = (int64_t)smem_optin - 1024;
+    const double epr = (double)plan.local_elems.size() / (double)plan.n_rows;
+    const double jobs_per_row = 1.15 * epr + 0.05, incs_per_row = 3.0 * epr + 0.5;
+    const double vals_per_row = (double)d->nnz / (double)plan.n_rows;
+    int64_t rows = 4096;
+    rows = std::min<int64_t>(rows, std::max<int64_t>(1, plan.n_rows / (4 * (int64_t)n_sms)));
+    ClLayout<double> lay{};
+    auto fit = [&](int64_t r) {
+      lay.cj = (int)std::min<int64_t>(1 << kClJobBits, ((int64_t)(1.1 * r * jobs_per_row) + 19) / 4 * 4);
+      lay.ci = (int)(((int64_t)(1.1 * r * incs_per_row) + 19) / 4 * 4);
+      lay.cr = (int)(r + r / 4 + 8);
+      lay.cu = 128;
+      lay.cw = (int)((int64_t)(1.1 * r * vals_per_row) + 16);
+      const size_t b = f32 ? ClLayout<float>{lay.cj, lay.cr, lay.cu, lay.ci, lay.cw}.bytes() : lay.bytes();
+      return (int64_t)b <= budget;
+    };
+    for (int it = 0; it < 80 && rows > 1 && !fit(rows); ++it) rows = std::max<int64_t>(1, rows * 19 / 20);
+    const bool gid = [&] {
+      for (int32_t k = 0; k < plan.n_rows; ++k)
+        if (plan.row_gpos[k] != k) return false;
+      return true;
+    }();
+    if (fit(rows))
+      use_cluster = build_cluster_plan(plan, d->lo, d->hi, lay.cr, lay.cj, lay.ci, lay.cw, gid, cplan);
+    if (use_cluster && cplan.max_runs > lay.cu) use_cluster = false;
+  }
+  if (is_tri(d->family) && plan.n_rows > 0 &&
+      (d->kernel_variant == 0 || (d->kernel_variant == 8 && !use_cluster) || d->kernel_variant == 7 || want_push)) {
     // shared memory per CTA: 12*nb element quantities (pull sweep only) +
     // entry window + row window, sized so that two CTAs fit on one SM
     const int64_t budget = std::min<int64_t>(smem_optin, (228 * 1024) / 2 - 1024) / (int64_t)real_size;
@@ -1842,7 +1925,8 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   h->n_inc = (int64_t)plan.inc_elem.size();
   h->max_row_len = plan.max_row_len;
   h->use_inc = use_inc;
-  h->use_sweep = use_sweep;
+  h->use_cluster = use_cluster;
+  h->use_sweep = use_sweep && !use_cluster;
   h->use_push = use_push;
   h->phys.p = d->s[0];
   h->phys.eps = d->s[0];
@@ -1861,7 +1945,18 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   cudaGetDevice(&h->device);
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
 
-  if (use_sweep) {
+  if (use_cluster) {
+    h->cl_n_cl = cplan.n_cl;
+    h->grid_rows = std::min(cplan.n_cl, n_sms);
+    h->cl_n_jobs = (int)cplan.job_elem.size();
+    h->cl_cap_j = cplan.max_jobs;
+    h->cl_cap_r = cplan.max_rows;
+    h->cl_cap_i = cplan.max_incs;
+    h->cl_cap_u = cplan.max_runs;
+    h->cl_cap_w = cplan.max_win;
+    h->smem_bytes = f32 ? ClLayout<float>{h->cl_cap_j, h->cl_cap_r, h->cl_cap_u, h->cl_cap_i, h->cl_cap_w}.bytes()
+                        : ClLayout<double>{h->cl_cap_j, h->cl_cap_r, h->cl_cap_u, h->cl_cap_i, h->cl_cap_w}.bytes();
+  } else if (use_sweep) {
     h->grid_rows = sweep.n_seg;
     h->sweep_nb = sweep.nb;
     h->sweep_win_mask = sweep.win_entries - 1;
@@ -1927,7 +2022,35 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
   FNE_TRY(upload(h, &h->row_comp, plan.row_comp.data(), plan.row_comp.size()));
   FNE_TRY(upload(h, &h->row_gpos, plan.row_gpos.data(), plan.row_gpos.size()));
   FNE_TRY(upload(h, &h->inc_ptr, plan.inc_ptr.data(), plan.inc_ptr.size()));
-  if (use_sweep) {
+  if (use_cluster) {
+    std::vector<int32_t> codes;
+    if (f32) {
+      std::vector<float> reals;
+      pack_cluster_jobs(d, plan, cplan, codes, reals);
+      float* dr = nullptr;
+      FNE_TRY(upload(h, &dr, reals.data(), reals.size()));
+      h->cl_reals = dr;
+    } else {
+      std::vector<double> reals;
+      pack_cluster_jobs(d, plan, cplan, codes, reals);
+      double* dr = nullptr;
+      FNE_TRY(upload(h, &dr, reals.data(), reals.size()));
+      h->cl_reals = dr;
+    }
+    FNE_TRY(upload(h, &h->cl_codes, codes.data(), codes.size()));
+    FNE_TRY(upload(h, &h->cl_table, reinterpret_cast<const int4*>(cplan.table.data()), cplan.table.size() / 4));
+    FNE_TRY(upload(h, &h->cl_rows, reinterpret_cast<const int4*>(cplan.rows.data()), cplan.rows.size() / 4));
+    FNE_TRY(upload(h, &h->cl_runs, reinterpret_cast<const int4*>(cplan.runs.data()), cplan.runs.size() / 4));
+    FNE_TRY(upload(h, &h->cl_incs, cplan.incs.data(), cplan.incs.size()));
+    FNE_TRY(dalloc(h, &h->err, 1));
+    if (cudaMemset(h->err, 0, sizeof(int)) != cudaSuccess ||
+        cudaHostAlloc((void**)&h->err_host, sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+      free_handle(h);
+      return set_error(FNE_ECUDA, "fne_create: status word");
+    }
+    *h->err_host = 0;
+  }
+  if (use_sweep && !use_cluster) {
     FNE_TRY(upload(h, &h->sw_seg_row, sweep.seg_row.data(), sweep.seg_row.size()));
     FNE_TRY(upload(h, &h->sw_seg_elem, sweep.seg_elem.data(), sweep.seg_elem.size()));
     FNE_TRY(upload(h, &h->sw_seg_batch, sweep.seg_batch.data(), sweep.seg_batch.size()));
@@ -2027,7 +2150,7 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
   info->n_incidences = h->n_inc;
   info->device_bytes = h->device_bytes;
   info->max_row_len = h->max_row_len;
-  info->kernel_variant = is_tri(h->family) ? (h->use_push ? 8 : (h->use_sweep ? 4 : (h->use_inc ? 3 : 1)))
+  info->kernel_variant = is_tri(h->family) ? (h->use_cluster ? 10 : h->use_push ? 8 : (h->use_sweep ? 4 : (h->use_inc ? 3 : 1)))
                                            : (h->use_elem2 ? 7 : 2);
   if (h->use_elem2) info->n_incidences = h->e2_contrib;
   info->row_lanes = h->tet_lanes;
@@ -2054,17 +2177,33 @@ extern "C" int fne_hvp_diagonal(fne_handle* h, double* diag, void* stream) {
 
 extern "C" int fne_check_device_status(fne_handle* h) {
   if (!h) return set_error(FNE_EINVAL, "fne_check_device_status: null handle");
-  return h->mc ? mc_check_status(h->mc) : FNE_OK;
+  if (h->mc) return mc_check_status(h->mc);
+  if (!h->err) return FNE_OK;
+  int v = 0;
+  cudaError_t e = cudaMemcpy(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "fne_check_device_status");
+  if (v == 0) return FNE_OK;
+  cudaMemset(h->err, 0, sizeof(int));
+  if (h->err_host) *h->err_host = 0;
+  return set_error(FNE_ETIMEOUT, "row-cluster kernel: a wait for its staging copies gave up");
 }
 
 extern "C" int fne_poll_device_status(fne_handle* h) {
   if (!h) return set_error(FNE_EINVAL, "fne_poll_device_status: null handle");
-  return h->mc ? mc_poll_status(h->mc) : FNE_OK;
+  if (h->mc) return mc_poll_status(h->mc);
+  if (!h->err_host || *(volatile int*)h->err_host == 0) return FNE_OK;
+  *h->err_host = 0;
+  cudaMemset(h->err, 0, sizeof(int));
+  return set_error(FNE_ETIMEOUT, "row-cluster kernel: a wait for its staging copies gave up");
 }
 
 extern "C" int fne_set_wait_limit(fne_handle* h, int64_t polls) {
   if (!h) return set_error(FNE_EINVAL, "fne_set_wait_limit: null handle");
-  if (!h->mc) return set_error(FNE_EINVAL, "fne_set_wait_limit: the handle runs no tensor-core kernel");
+  if (h->use_cluster) {
+    h->cl_wait_limit = polls < 0 ? kClWaitLimit : (long long)polls;
+    return FNE_OK;
+  }
+  if (!h->mc) return set_error(FNE_EINVAL, "fne_set_wait_limit: the handle runs no kernel with a bounded wait");
   return mc_set_wait_limit(h->mc, (long long)polls);
 }
 
@@ -2115,6 +2254,9 @@ extern "C" int fne_eval(fne_handle* h, const double* u, int flags, double* energ
                  h->sw_gpos_identity, h->sw_eoff, h->sw_row_of};
     e = h->use_elem2 ? launch_elem2(h, flags, u, grad, hess, eo, st)
                      : launch_rows(h, flags, A, Q, SW, grad, hess, eo, st, false);
+    // stream-ordered copy of the status word for fne_poll_device_status
+    if (e == cudaSuccess && h->use_cluster)
+      e = cudaMemcpyAsync(h->err_host, h->err, sizeof(int), cudaMemcpyDeviceToHost, st);
   }
   if (e != cudaSuccess) return cuda_fail(e, "fne_eval launch");
   return FNE_OK;

@@ -129,6 +129,51 @@ struct SweepPlan {
 // does not fit (window larger than max_win_entries, rows longer than 126...).
 bool build_sweep_plan(RowPlan& P, int nb, int n_seg, int max_win_entries, int max_win_rows, SweepPlan& Q);
 
+// Row-cluster plan (scalar P1 triangles).  The owned rows are split into
+// compact clusters (graph-grown over the element graph); CTA c evaluates
+// every element that touches cluster c's rows (the cluster's "jobs"; an
+// element on a cluster border is a job of each neighbouring cluster) into
+// shared memory, then one thread per row sums, in a fixed order, the
+// contributions its incidence list names into the row's slots of a
+// shared-memory window, which is streamed out run by run: deterministic, no
+// atomics, every COO value and gradient entry written to HBM once.
+//   cluster table, 8 ints per cluster: {first job, end of the
+//     energy-counting jobs, end of the jobs (padded to a multiple of 4),
+//     first row, end of the rows, first incidence, end of the incidences
+//     (padded to a multiple of 4), first run}; the first job and first
+//     incidence are multiples of 4; the run range ends where the next
+//     cluster's begins (run_end of the last cluster = number of runs);
+//   job j: the local element job_elem[j] (-1 = padding job);
+//   row i: {gradient slot, window offset, row length | incidences << 16,
+//     first incidence relative to the cluster's first};
+//   run: {window offset, first COO position, values, 0} -- consecutive rows
+//     whose COO ranges are adjacent;
+//   incidence word: bits 0-10 the job's index inside the cluster, bits 11-12
+//     the row's node a in that element, bits 13-24 the 4-bit column offsets
+//     (inside the row) of element nodes 0..2 (15 = no column).
+struct ClusterPlan {
+  int32_t n_cl = 0;
+  int32_t max_jobs = 0;              // most jobs of one cluster (padded)
+  int32_t max_rows = 0;              // most rows of one cluster
+  int32_t max_incs = 0;              // most incidences of one cluster (padded)
+  int32_t max_win = 0;               // most COO values of one cluster
+  int32_t max_runs = 0;              // most runs of one cluster
+  std::vector<int32_t> table;        // [(n_cl + 1) * 8]; the extra entry closes the run ranges
+  std::vector<int32_t> job_elem;     // [n_jobs]
+  std::vector<int32_t> rows;         // [n_rows_total * 4]
+  std::vector<int32_t> runs;         // [n_runs * 4]
+  std::vector<uint32_t> incs;        // [n_incs_total]
+};
+constexpr int kClJobBits = 11;
+constexpr uint32_t kClNoCol = 15u;
+
+// Builds Q from P (P is not modified); a cluster stops growing at max_rows
+// rows, max_jobs jobs or max_incs incidences (both counted padded) or
+// max_win COO values.  Returns false when the mesh does not fit the packed
+// format (a row longer than 14 entries, a row alone beyond a budget).
+bool build_cluster_plan(const RowPlan& P, int64_t lo, int64_t hi, int max_rows, int max_jobs, int max_incs,
+                        int max_win, bool gpos_identity, ClusterPlan& Q);
+
 // Node-block gather plan: the element matrices (stored per element as node
 // pairs a <= b of bs x bs blocks) are summed per output block (row node A,
 // column node B) -- the bs x bs values of rows (A, c) at columns (B, d).

@@ -727,3 +727,167 @@ int build_direct_plan(const BlockPlan& bp, int64_t n_local, int npn, int bs, Dir
 }
 
 }  // namespace fne
+
+// ---------------------------------------------------------------------------
+// Row-cluster plan (see ClusterPlan in fne_internal.h).
+// ---------------------------------------------------------------------------
+namespace fne {
+
+bool build_cluster_plan(const RowPlan& P, int64_t lo, int64_t hi, int max_rows, int max_jobs, int max_incs,
+                        int max_win, bool gpos_identity, ClusterPlan& Q) {
+  const int32_t n_local = (int32_t)P.local_elems.size();
+  const int32_t n_rows = P.n_rows;
+  if (n_local == 0 || n_rows == 0 || P.elem_code.size() != (size_t)n_local * 3) return false;
+  if (max_rows < 1 || max_jobs < 8 || max_jobs > (1 << kClJobBits) || max_incs < 8) return false;
+  if ((int64_t)n_rows != hi - lo || P.n_nodes != n_rows) return false;  // scalar rows: one per owned node
+  std::vector<int32_t> row_of((size_t)(hi - lo), -1);
+  for (int32_t k = 0; k < n_rows; ++k) {
+    row_of[P.row_gpos[k]] = k;
+    if (P.row_ptr[k + 1] - P.row_ptr[k] > 14) return false;  // 4-bit column offsets
+  }
+  auto inc_begin = [&](int32_t k) { return P.inc_ptr[P.row_node[k]]; };
+  auto inc_end = [&](int32_t k) { return P.inc_ptr[P.row_node[k] + 1]; };
+  auto row_len = [&](int32_t k) { return P.row_ptr[k + 1] - P.row_ptr[k]; };
+  for (int32_t k = 0; k < n_rows; ++k)
+    if (inc_end(k) - inc_begin(k) + 3 > std::min(max_jobs, max_incs) || row_len(k) > max_win) return false;
+  // jobs a row adds to cluster c (its elements not yet in c)
+  std::vector<int32_t> estamp(n_local, -1);
+  auto new_jobs = [&](int32_t k, int32_t c, bool commit) {
+    int32_t n = 0;
+    for (int32_t i = inc_begin(k); i < inc_end(k); ++i) {
+      const int32_t le = P.inc_elem[i];
+      if (estamp[le] != c) {
+        ++n;
+        if (commit) estamp[le] = c;
+      }
+    }
+    return n;
+  };
+
+  // ---- graph-grown clusters: BFS from the lowest unassigned row ------------
+  std::vector<int32_t> cl_of(n_rows, -1), queue;
+  std::vector<std::vector<int32_t>> clusters;
+  queue.reserve(n_rows);
+  int32_t seed = 0;
+  while (true) {
+    while (seed < n_rows && cl_of[seed] >= 0) ++seed;
+    if (seed >= n_rows) break;
+    const int32_t c = (int32_t)clusters.size();
+    clusters.emplace_back();
+    std::vector<int32_t>& rows = clusters.back();
+    int64_t njobs = new_jobs(seed, c, true);
+    int64_t nincs = inc_end(seed) - inc_begin(seed);
+    int64_t nwin = row_len(seed);
+    cl_of[seed] = c;
+    rows.push_back(seed);
+    queue.clear();
+    queue.push_back(seed);
+    bool full = false;
+    for (size_t qh = 0; qh < queue.size() && !full; ++qh) {
+      const int32_t k = queue[qh];
+      for (int32_t i = inc_begin(k); i < inc_end(k) && !full; ++i) {
+        const int32_t le = P.inc_elem[i];
+        for (int b = 0; b < 3; ++b) {
+          const int32_t cb = P.elem_code[(size_t)le * 3 + b];
+          if (cb < lo || cb >= hi) continue;
+          const int32_t kb = row_of[cb - lo];
+          if (kb < 0 || cl_of[kb] >= 0) continue;
+          const int32_t ni = inc_end(kb) - inc_begin(kb);
+          // + 3: padding to a multiple of 4
+          if ((int)rows.size() >= max_rows || njobs + new_jobs(kb, c, false) + 3 > max_jobs ||
+              nincs + ni + 3 > max_incs || nwin + row_len(kb) > max_win) {
+            full = true;
+            break;
+          }
+          cl_of[kb] = c;
+          rows.push_back(kb);
+          njobs += new_jobs(kb, c, true);
+          nincs += ni;
+          nwin += row_len(kb);
+          queue.push_back(kb);
+        }
+      }
+    }
+  }
+  const int32_t n_cl = (int32_t)clusters.size();
+
+  // ---- per cluster: jobs (energy-counting first), rows, incidences ---------
+  Q = ClusterPlan{};
+  Q.n_cl = n_cl;
+  Q.table.reserve((size_t)n_cl * 8);
+  std::vector<int32_t> stamp(n_local, -1), slot(n_local, -1);
+  std::vector<std::pair<int32_t, int32_t>> jobs;  // (energy ? 0 : 1, local element)
+  for (int32_t c = 0; c < n_cl; ++c) {
+    std::vector<int32_t>& rows = clusters[c];
+    std::sort(rows.begin(), rows.end());
+    jobs.clear();
+    for (int32_t k : rows)
+      for (int32_t i = inc_begin(k); i < inc_end(k); ++i) {
+        const int32_t le = P.inc_elem[i];
+        if (stamp[le] != c) {
+          stamp[le] = c;
+          slot[le] = (int32_t)jobs.size();
+          jobs.emplace_back(1, le);
+        }
+      }
+    // the element energy is counted where the element's energy row (its
+    // first owned node, energy weight 1) lies
+    for (int32_t k : rows)
+      for (int32_t i = inc_begin(k); i < inc_end(k); ++i)
+        if (P.inc_info[i] & kEnergyFlag) jobs[slot[P.inc_elem[i]]].first = 0;
+    std::sort(jobs.begin(), jobs.end());
+    const int32_t j0 = (int32_t)Q.job_elem.size();
+    int32_t je = j0;
+    for (const auto& jb : jobs) {
+      slot[jb.second] = (int32_t)Q.job_elem.size() - j0;
+      Q.job_elem.push_back(jb.second);
+      if (jb.first == 0) je = (int32_t)Q.job_elem.size();
+    }
+    while (Q.job_elem.size() % 4) Q.job_elem.push_back(-1);
+    const int32_t j1 = (int32_t)Q.job_elem.size();
+    const int32_t r0 = (int32_t)(Q.rows.size() / 4), i0 = (int32_t)Q.incs.size();
+    const int32_t u0 = (int32_t)(Q.runs.size() / 4);
+    int32_t wo = 0;
+    for (int32_t k : rows) {
+      const int32_t n_inc = inc_end(k) - inc_begin(k), len = row_len(k);
+      if (n_inc > 0x7fff) return false;
+      Q.rows.insert(Q.rows.end(), {gpos_identity ? k : P.row_gpos[k], wo, len | (n_inc << 16),
+                                   (int32_t)Q.incs.size() - i0});
+      // runs of rows whose COO ranges are adjacent
+      const size_t nu = Q.runs.size() / 4;
+      if (len > 0) {
+        if ((int32_t)nu > u0 && Q.runs[4 * (nu - 1) + 1] + Q.runs[4 * (nu - 1) + 2] == P.row_ptr[k])
+          Q.runs[4 * (nu - 1) + 2] += len;
+        else
+          Q.runs.insert(Q.runs.end(), {wo, P.row_ptr[k], len, 0});
+      }
+      wo += len;
+      for (int32_t i = inc_begin(k); i < inc_end(k); ++i) {
+        const uint32_t info = P.inc_info[i];
+        uint32_t w = (uint32_t)slot[P.inc_elem[i]] | ((info & 3u) << kClJobBits);
+        for (int b = 0; b < 3; ++b) {
+          uint32_t off = (info >> (kOffShift + kOffBits * b)) & 127u;
+          if (off == kNoCol) off = kClNoCol;
+          w |= off << (kClJobBits + 2 + 4 * b);
+        }
+        Q.incs.push_back(w);
+      }
+    }
+    while (Q.incs.size() % 4) Q.incs.push_back(0u);
+    const int32_t r1 = (int32_t)(Q.rows.size() / 4), i1 = (int32_t)Q.incs.size();
+    Q.table.insert(Q.table.end(), {j0, je, j1, r0, r1, i0, i1, u0});
+    Q.max_win = std::max(Q.max_win, wo);
+    Q.max_runs = std::max(Q.max_runs, (int32_t)(Q.runs.size() / 4) - u0);
+    Q.max_jobs = std::max(Q.max_jobs, j1 - j0);
+    Q.max_rows = std::max(Q.max_rows, r1 - r0);
+    Q.max_incs = std::max(Q.max_incs, i1 - i0);
+    if (Q.max_jobs > max_jobs || Q.max_incs > max_incs) return false;
+    if (Q.job_elem.size() >= (size_t)INT32_MAX / 8 || Q.incs.size() >= (size_t)INT32_MAX / 8) return false;
+  }
+  const int32_t nj = (int32_t)Q.job_elem.size(), nr = (int32_t)(Q.rows.size() / 4);
+  const int32_t ni = (int32_t)Q.incs.size(), nu = (int32_t)(Q.runs.size() / 4);
+  Q.table.insert(Q.table.end(), {nj, nj, nj, nr, nr, ni, ni, nu});
+  return true;
+}
+
+}  // namespace fne

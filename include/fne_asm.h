@@ -165,10 +165,13 @@ typedef struct {
                                  * free DOF (Ginzburg-Landau assembler,
                                  * src/problems/ginzburg_landau/jax_petsc/
                                  * reordered_element_assembler.py:34-52, 96-97) */
-  int32_t kernel_variant;       /* P1 triangles: 0 = automatic (banded sweep);
-                                 * 1 = row-gather; 2 = incidence-parallel;
-                                 * 3 = banded sweep with shared-memory atomics
-                                 * (push; not bit-reproducible).
+  int32_t kernel_variant;       /* P1 triangles: 0 = automatic (banded
+                                 * sweep); 1 = row-gather; 2 = incidence-
+                                 * parallel; 3 = banded sweep with shared-
+                                 * memory atomics (push; not bit-reproducible);
+                                 * 7 = banded sweep; 8 = persistent row-cluster
+                                 * kernel (TMA-staged; the banded sweep when
+                                 * the mesh does not fit its packed format).
                                  * P1 tets: 0 = row-gather with automatic lanes
                                  * per row; 1 = row-gather, one lane per row;
                                  * 2 = element-parallel pass + node-block
@@ -194,7 +197,8 @@ typedef struct {
                            * 5 Mohr-Coulomb CUDA cores, 6 Mohr-Coulomb tcgen05,
                            * 7 element-parallel tets + node-block gather,
                            * 8 banded sweep, push variant,
-                           * 9 Mohr-Coulomb FP64 DMMA (mma.sync f64) */
+                           * 9 Mohr-Coulomb FP64 DMMA (mma.sync f64),
+                           * 10 row clusters (P1 triangles) */
   int32_t row_lanes;      /* lanes per output row of the tet row kernel, else 1 */
 } fne_info;
 
@@ -218,14 +222,16 @@ int fne_hvp(fne_handle* h, const double* x, double* y, void* stream);
 int fne_hvp_diagonal(fne_handle* h, double* diag, void* stream);
 /*
  * Synchronous read of the handle's device status word (kernels that wait on
- * the tensor core record a bounded wait that gave up there instead of
- * hanging).  FNE_OK, or FNE_ETIMEOUT (the word is then cleared).  No
- * counterpart in the reference, whose element kernels run on the CPU.
+ * the tensor core, or on their own bulk copies into shared memory -- the
+ * Mohr-Coulomb tensor-core kernel and the P1-triangle row-cluster kernel --
+ * record a bounded wait that gave up there instead of hanging).  FNE_OK, or
+ * FNE_ETIMEOUT (the word is then cleared).  No counterpart in the reference,
+ * whose element kernels run on the CPU.
  */
 int fne_check_device_status(fne_handle* h);
 /*
- * The same status without a device synchronisation: every tensor-core pass
- * ends with a stream-ordered copy of the word into pinned host memory, and
+ * The same status without a device synchronisation: every pass of those
+ * kernels ends with a stream-ordered copy of the word into pinned host memory, and
  * this reads that copy.  Call it after synchronising the stream of the pass
  * (the assembler callbacks do so after each pass).  FNE_OK, or FNE_ETIMEOUT
  * (both copies are then cleared).  No counterpart in the reference.
@@ -234,10 +240,12 @@ int fne_poll_device_status(fne_handle* h);
 /*
  * Polls of the tensor-core kernel's per-tile MMA-completion wait before it
  * gives up (records FNE_ETIMEOUT, drains its own MMAs with the full bound,
- * frees its tensor memory and returns); polls < 0 restores the default
- * (2^22).  0 makes every pass give up at once: how the tests exercise the
- * timeout path without a fault.  FNE_EINVAL for a handle without the
- * tensor-core kernel.  No counterpart in the reference.
+ * frees its tensor memory and returns), or of the row-cluster kernel's waits
+ * for its staging copies (records FNE_ETIMEOUT, waits for its own copies
+ * with the full bound, writes no output and makes the energy NaN); polls < 0
+ * restores the default (2^22).  0 makes every pass give up at once: how the
+ * tests exercise the timeout path without a fault.  FNE_EINVAL for a handle
+ * without either kernel.  No counterpart in the reference.
  */
 int fne_set_wait_limit(fne_handle* h, int64_t polls);
 /* Replace the Dirichlet values; ``dirichlet`` is a host array [n_total]. */

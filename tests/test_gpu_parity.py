@@ -67,7 +67,7 @@ def _abs_energy_scale(ref, u):
     return float(np.abs(e).sum() + np.abs(ref.f_owned @ np.asarray(u)[: ref.f_owned.size]) + 1e-300)
 
 
-@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence", "push"])
+@pytest.mark.parametrize("variant", ["auto", "cluster", "row_gather", "incidence", "push"])
 @pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
 def test_plaplace_fp64(numbering, variant):
     params, _ = meshes.plaplace_problem(n=40, numbering=numbering)
@@ -84,7 +84,7 @@ def test_plaplace_zero_initial_guess():
     assert torch.all(gpu.owned_values == 0)
 
 
-@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence", "push"])
+@pytest.mark.parametrize("variant", ["auto", "cluster", "row_gather", "incidence", "push"])
 @pytest.mark.parametrize("numbering", ["x_slow", "x_fast"])
 def test_gl_fp64(numbering, variant):
     params, u0 = meshes.gl_problem(n=16, seed=3, numbering=numbering)
@@ -92,7 +92,7 @@ def test_gl_fp64(numbering, variant):
     _check(gpu, ref, u0, FP64_TOL, energy_scale=_abs_energy_scale(ref, u0))
 
 
-@pytest.mark.parametrize("variant", ["auto", "row_gather", "incidence", "push"])
+@pytest.mark.parametrize("variant", ["auto", "cluster", "row_gather", "incidence", "push"])
 def test_gl_fp32(variant):
     params, u0 = meshes.gl_problem(n=40, seed=4)
     gpu, ref = _make("gl", params, precision="fp32", hess_dtype=torch.float32, kernel_variant=variant)
@@ -333,3 +333,42 @@ def test_rank_split_matches_oracle(family, size):
     u1 = u[np.asarray(one.layout.perm)] if family != "he" else u
     e1 = one.all_in_one(u1)[0]
     assert abs(total - e1) <= 1e-11 * max(1.0, abs(e1))
+
+
+def test_cluster_kernel_copy_wait_timeout_is_reported():
+    """The row-cluster kernel's (kernel_variant "cluster") waits for its TMA
+    bulk copies, set to give up at once (fne_set_wait_limit 0): the pass returns with a NaN energy, the
+    status word reports FNE_ETIMEOUT (polled by the callbacks, or read
+    synchronously), and with the default bound restored the same handle gives
+    the oracle's values again (the context stayed usable)."""
+    params, _ = meshes.gl_problem(n=24, seed=0)
+    gpu, ref = _make("gl", params, kernel_variant="cluster")
+    assert gpu.info["kernel_variant"] == 10
+    u = np.random.default_rng(4).uniform(-0.5, 0.5, gpu.layout.n_free)
+    ut = torch.as_tensor(u, device="cuda")
+    _lib.check(_lib.lib.fne_set_wait_limit(gpu._handle, 0))
+    e, _, _ = gpu.eval(ut, 7)
+    torch.cuda.synchronize()
+    assert np.isnan(float(e.item()))
+    assert _lib.lib.fne_check_device_status(gpu._handle) == _lib.FNE_ETIMEOUT
+    assert _lib.lib.fne_check_device_status(gpu._handle) == _lib.FNE_OK  # cleared
+    with pytest.raises(_lib.FneError) as err:
+        gpu.assemble_hessian(u)
+    assert err.value.code == _lib.FNE_ETIMEOUT
+    _lib.check(_lib.lib.fne_set_wait_limit(gpu._handle, -1))
+    _check(gpu, ref, u, FP64_TOL)
+    gpu.check_device_status()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_cluster_kernel_is_bit_reproducible(precision):
+    """Two passes of the row-cluster kernel give identical bits."""
+    params, u0 = meshes.gl_problem(n=96, seed=1)
+    hd = torch.float32 if precision == "fp32" else torch.float64
+    gpu, _ = _make("gl", params, precision=precision, hess_dtype=hd, kernel_variant="cluster")
+    assert gpu.info["kernel_variant"] == 10
+    ut = torch.as_tensor(np.random.default_rng(5).uniform(-0.5, 0.5, gpu.layout.n_free), device="cuda")
+    a = [t.clone() for t in gpu.eval(ut, 7)]
+    b = gpu.eval(ut, 7)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
