@@ -16,7 +16,7 @@ _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libfne_asm.so"
 
 FNE_OK, FNE_EINVAL, FNE_ECUDA, FNE_EBOUNDS, FNE_ETIMEOUT, FNE_ENOMEM, FNE_ELAYOUT = range(7)
-FNE_PLAPLACE, FNE_GINZBURG_LANDAU, FNE_NEOHOOKEAN, FNE_MOHR_COULOMB = 1, 2, 3, 4
+FNE_PLAPLACE, FNE_GINZBURG_LANDAU, FNE_NEOHOOKEAN, FNE_MOHR_COULOMB, FNE_MOHR_COULOMB_3D = 1, 2, 3, 4, 5
 FNE_FP64, FNE_FP32 = 0, 1
 FNE_REORDER_NONE, FNE_REORDER_BLOCK_XYZ = 0, 1
 FNE_ENERGY, FNE_GRAD, FNE_HESS = 1, 2, 4

@@ -182,9 +182,9 @@ class CudaElementAssemblerBase:
         the element kernel, the Hessian gather or shared-block fix-up, and the
         gradient rows."""
         kv = self.info["kernel_variant"]
-        if flags == _lib.FNE_ENERGY or kv not in (5, 6, 7, 9):
+        if flags == _lib.FNE_ENERGY or kv not in (5, 6, 7, 9, 11):
             return 1
-        if kv == 7:
+        if kv in (7, 11):
             return 2
         return 1 + bool(flags & _lib.FNE_HESS) + bool(flags & _lib.FNE_GRAD)
 
@@ -480,6 +480,53 @@ class SlopeStabilityCudaAssembler(CudaElementAssemblerBase):
         else:
             arr[:] = t.cpu().numpy()
         return dest
+
+    def _build_rhs_owned(self):
+        force = np.asarray(self.params["force"], dtype=np.float64)
+        free = np.asarray(self.params["freedofs"], dtype=np.int64)
+        return np.ascontiguousarray(force[free][self.layout.perm][self.layout.lo: self.layout.hi])
+
+
+class SlopeStability3DCudaAssembler(CudaElementAssemblerBase):
+    """``SlopeStability3DReorderedElementAssembler``
+    (slope_stability_3d/jax_petsc/reordered_element_assembler.py:189-206,
+    377-560): 3-D Mohr-Coulomb (``constitutive_mode="mc"``, the reference's
+    "plastic" mode) or linear elastic (``"elastic"``) on P1 / P2 tetrahedra.
+
+    Takes the reference's local element data as is: ``dphix``, ``dphiy``,
+    ``dphiz`` (E, nq, n_p), ``quad_weight`` and the per-point material fields
+    ``c_bar_q``, ``sin_phi_q``, ``shear_q``, ``bulk_q``, ``lame_q`` (E, nq)
+    (the names without the ``_q`` suffix are accepted too), and the gravity
+    ``force`` as the load vector.
+    """
+
+    family = _lib.FNE_MOHR_COULOMB_3D
+    block_size = 3
+    coordinate_key, dirichlet_key = "nodes", "u_0"
+    _MATERIAL = ("c_bar", "sin_phi", "shear", "bulk", "lame")
+
+    def __init__(self, params, comm=None, adjacency=None, *, constitutive_mode="mc", **kw):
+        self.constitutive_mode = {"plastic": "mc"}.get(str(constitutive_mode), str(constitutive_mode))
+        if self.constitutive_mode not in ("mc", "elastic"):
+            raise ValueError(f"Unsupported constitutive_mode {constitutive_mode!r}")
+        self.npe = int(np.asarray(params["elems_scalar"]).shape[1])
+        super().__init__(params, comm, adjacency, **kw)
+
+    def _field(self, name):
+        p = self.params
+        return np.asarray(p[name + "_q"] if name + "_q" in p else p[name], dtype=np.float64)
+
+    def _element_arrays(self):
+        p = self.params
+        w = np.asarray(p["quad_weight"], dtype=np.float64)
+        pts = np.stack([w] + [np.broadcast_to(self._field(k), w.shape) for k in self._MATERIAL], axis=-1)
+        return [np.asarray(p[k], dtype=np.float64) for k in ("dphix", "dphiy", "dphiz")] + [pts]
+
+    def _nq(self):
+        return int(np.asarray(self.params["quad_weight"]).shape[1])
+
+    def _scalars(self):
+        return [1.0e-15, 0.0, 0.0, 0.0, 0.0, 1.0 if self.constitutive_mode == "elastic" else 0.0]
 
     def _build_rhs_owned(self):
         force = np.asarray(self.params["force"], dtype=np.float64)

@@ -13,7 +13,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libfne_asm.so"
-SOURCES = ["fne_asm.cu", "fne_mc.cu", "fne_mlp.cu", "fne_krylov.cu", "fne_layout_dev.cu", "fne_plan.cpp", "fne_layout.cpp"]
+SOURCES = ["fne_asm.cu", "fne_mc.cu", "fne_mc3d.cu", "fne_mlp.cu", "fne_krylov.cu", "fne_layout_dev.cu", "fne_plan.cpp", "fne_layout.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

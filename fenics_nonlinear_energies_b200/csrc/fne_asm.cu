@@ -1360,6 +1360,7 @@ extern "C" int fne_energy_p1tri_noalloc(int32_t family, int64_t n_elem, const in
 // ---------------------------------------------------------------------------
 struct fne_handle {
   McHandle* mc = nullptr;  // Mohr-Coulomb handles delegate to fne_mc.cu
+  Mc3dHandle* mc3 = nullptr;  // 3-D Mohr-Coulomb handles delegate to fne_mc3d.cu
   int family = 0, precision = 0, hess_fp32 = 0, npe = 0, bs = 0;
   int64_t n_total = 0, n_free = 0, lo = 0, hi = 0, nnz = 0;
   int n_rows = 0, n_local = 0, n_dir_only = 0, rows_per_cta = 0, grid_rows = 0;
@@ -1448,6 +1449,7 @@ int upload(fne_handle* h, T** p, const T* src, size_t count) {
 void free_handle(fne_handle* h) {
   if (!h) return;
   if (h->mc) mc_destroy(h->mc);
+  if (h->mc3) mc3d_destroy(h->mc3);
   void* ptrs[] = {h->rec, h->rec_dir_only, h->row_ptr, h->row_node, h->row_gpos, h->inc_ptr, h->inc_elem,
                   h->row_comp, h->inc_info, h->cta_row, h->cta_inc, h->inc_elem2, h->inc_word, h->inc_rowl,
                   h->sw_seg_row, h->sw_seg_elem, h->sw_seg_batch, h->sw_batch_done, h->sw_ent_ptr, h->sw_inc_base,
@@ -1801,6 +1803,31 @@ extern "C" int fne_create(const fne_desc* d, fne_handle** out) {
     h->nnz = d->nnz;
     *out = h;
     return FNE_OK;
+  } else if (d->family == FNE_MOHR_COULOMB_3D) {
+    if (d->n_elem < 0 || d->n_total < 0 || d->nnz < 0 || (d->n_elem > 0 && !d->elems) || !d->total_to_free_reord ||
+        (d->nnz > 0 && (!d->owned_rows || !d->owned_cols)) || (d->n_total > 0 && !d->dirichlet))
+      return set_error(FNE_EINVAL, "fne_create: missing array");
+    if (d->precision != FNE_FP64 && d->precision != FNE_FP32)
+      return set_error(FNE_EINVAL, "fne_create: precision must be FNE_FP64 or FNE_FP32");
+    Mc3dHandle* m3 = nullptr;
+    int rc = mc3d_create(d, &m3);
+    if (rc) return rc;
+    auto* h = new (std::nothrow) fne_handle();
+    if (!h) {
+      mc3d_destroy(m3);
+      return set_error(FNE_ENOMEM, "fne_create: out of host memory");
+    }
+    h->mc3 = m3;
+    h->family = d->family;
+    h->precision = d->precision;
+    h->hess_fp32 = d->precision == FNE_FP32 && d->hess_fp32;
+    h->n_total = d->n_total;
+    h->n_free = d->n_free;
+    h->lo = d->lo;
+    h->hi = d->hi;
+    h->nnz = d->nnz;
+    *out = h;
+    return FNE_OK;
   } else {
     return set_error(FNE_EINVAL, "fne_create: unknown family");
   }
@@ -2144,6 +2171,10 @@ extern "C" int fne_info_get(const fne_handle* h, fne_info* info) {
     mc_info(h->mc, info);
     return FNE_OK;
   }
+  if (h->mc3) {
+    mc3d_info(h->mc3, info);
+    return FNE_OK;
+  }
   info->n_rows = h->n_rows;
   info->nnz = h->nnz;
   info->n_elem = h->n_local;
@@ -2211,6 +2242,7 @@ extern "C" int fne_set_dirichlet(fne_handle* h, const double* dirichlet) {
   if (!h || (!dirichlet && h->n_total > 0)) return set_error(FNE_EINVAL, "fne_set_dirichlet: null argument");
   if (h->n_total == 0) return FNE_OK;
   if (h->mc) return mc_set_dirichlet(h->mc, dirichlet);
+  if (h->mc3) return mc3d_set_dirichlet(h->mc3, dirichlet);
   cudaError_t e = cudaMemcpy(h->dir, dirichlet, h->n_total * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "fne_set_dirichlet");
   return refresh_dir_const(h);
@@ -2225,6 +2257,7 @@ extern "C" int fne_eval(fne_handle* h, const double* u, int flags, double* energ
   if ((flags & FNE_HESS) && !hess && h->nnz > 0) return set_error(FNE_EINVAL, "fne_eval: hess output missing");
   if (!u && h->n_free > 0) return set_error(FNE_EINVAL, "fne_eval: u missing");
   if (h->mc) return mc_eval(h->mc, u, flags, energy, grad, hess, stream);
+  if (h->mc3) return mc3d_eval(h->mc3, u, flags, energy, grad, hess, stream);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   EnergyOut eo{h->partials, h->counter, energy, h->dir_const};
   cudaError_t e = cudaSuccess;

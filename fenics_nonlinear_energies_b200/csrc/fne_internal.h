@@ -236,6 +236,14 @@ int mc_hvp(McHandle* h, const double* x, double* y, void* stream);
 int mc_hvp_diagonal(McHandle* h, double* diag, void* stream);
 void mc_destroy(McHandle* h);
 
+// 3-D Mohr-Coulomb (P1 / P2 tetrahedra) handle, csrc/fne_mc3d.cu.
+struct Mc3dHandle;
+int mc3d_create(const fne_desc* d, Mc3dHandle** out);
+int mc3d_eval(Mc3dHandle* h, const double* u, int flags, double* energy, double* grad, void* hess, void* stream);
+int mc3d_set_dirichlet(Mc3dHandle* h, const double* dirichlet);
+void mc3d_info(const Mc3dHandle* h, fne_info* info);
+void mc3d_destroy(Mc3dHandle* h);
+
 // Gather code of one element node: >= 0 reordered id of component 0 (free
 // node); < 0: -1 - total DOF of component 0 (Dirichlet node).
 }  // namespace fne

@@ -1,0 +1,493 @@
+// 3-D Mohr-Coulomb slope family (P1 / P2 tetrahedra, 3 DOFs per node):
+// element energy, gradient and constitutive Hessian on the GPU, scattered
+// into the owned gradient and COO values.
+//
+// Replaces the element kernels of SlopeStability3DReorderedElementAssembler
+// (src/problems/slope_stability_3d/jax_petsc/reordered_element_assembler.py:
+// 189-206, 377-560): the density of src/problems/slope_stability_3d/jax/
+// jax_energy_3d.py:38-191, its stress, and the element Hessian
+// K_e = sum_q w_q B_q^T D_q B_q of constitutive_element_hessian_3d
+// (jax_energy_3d.py:262-357), where the reference differentiates through
+// eigvalsh with JAX and here the hand-written spectral derivatives of
+// fne_mc3d_point.cuh are used.  Inputs are the reference's per-element,
+// per-quadrature-point arrays: dphix / dphiy / dphiz (E, nq, n_p),
+// quad_weight and the material fields c_bar_q, sin_phi_q, shear_q, bulk_q,
+// lame_q (E, nq).
+//
+// k_mc3d_elem: one warp per element.  Lanes over quadrature points form the
+// strain and run the constitutive point function (FP64: eigen-decomposition
+// by fixed-sweep Jacobi, branch potentials, spectral tangent) and store
+// w sigma and the upper triangle of w D in shared memory; lanes over
+// (node, component) form the element gradient; lanes over node pairs a <= b
+// form the 3 x 3 blocks of B^T (w D) B.  Blocks and gradients go to
+// per-element buffers that the node-block gather (fne_gather.cuh: per output
+// block, contributions in element order, no atomics) sums into the COO values
+// and the gradient.  FP32 mode keeps the point function in FP64 and runs the
+// contraction, the buffers and the Hessian output in FP32.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fne_gather.cuh"
+#include "fne_internal.h"
+#include "fne_mc3d_point.cuh"
+
+namespace fne {
+
+namespace {
+
+constexpr int kM3Warps = 4;      // warps (elements in flight) per CTA
+constexpr int kM3MaxQ = 16;      // quadrature points per element (kernel limit)
+constexpr int kM3Pt = 6;         // per-point inputs: w, c_bar, sin_phi, shear, bulk, lame
+
+struct Mc3dArgs {
+  int n_el;                        // local elements
+  int nq;
+  const int* __restrict__ codes;   // [n_el][3 NP] gather codes
+  const double* __restrict__ grad; // [n_el][3][nq][NP] physical basis gradients
+  const double* __restrict__ pt;   // [n_el][nq][6] per-point inputs
+  const unsigned char* __restrict__ wflag;
+  const double* __restrict__ u;
+  const double* __restrict__ dir;
+  const double* __restrict__ rhs;  // [n_owned] or null
+  int n_owned;
+  long long lo;
+  double tiny;
+  int elastic;
+  double* partials;
+  unsigned* counter;
+  double* energy;
+};
+
+__device__ __forceinline__ double m3_block_sum(double v, double* ws) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) ws[wid] = v;
+  __syncthreads();
+  v = 0.0;
+  if (wid == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+// per-CTA partial, then the last CTA to finish sums the partials in index
+// order (deterministic, no spin-waits)
+__device__ void m3_energy_finalize(double v, const Mc3dArgs& A) {
+  __shared__ double ws[32];
+  __shared__ int is_last;
+  v = m3_block_sum(v, ws);
+  if (threadIdx.x == 0) {
+    A.partials[blockIdx.x] = v;
+    __threadfence();
+    is_last = atomicAdd(A.counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  double s = 0.0;
+  for (int j = threadIdx.x; j < (int)gridDim.x; j += blockDim.x) s += __ldcg(A.partials + j);
+  s = m3_block_sum(s, ws);
+  if (threadIdx.x == 0) {
+    A.energy[0] = s;
+    *A.counter = 0u;
+  }
+}
+
+// linear elastic point: psi = lame/2 I1^2 + mu Q (the reference's elastic mode)
+__device__ __forceinline__ void m3_elastic(const double e[6], double mu, double lame, double& psi, double sig[6],
+                                           double D[6][6]) {
+  const double I1 = e[0] + e[1] + e[2];
+  psi = 0.5 * lame * I1 * I1 + mu * (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] +
+                                     0.5 * (e[3] * e[3] + e[4] * e[4] + e[5] * e[5]));
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) D[i][j] = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    sig[i] = lame * I1 + 2.0 * mu * e[i];
+    sig[3 + i] = mu * e[3 + i];
+    for (int j = 0; j < 3; ++j) D[i][j] = lame + (i == j ? 2.0 * mu : 0.0);
+    D[3 + i][3 + i] = mu;
+  }
+}
+
+// strain-vector component of DOF (node a, component c): the gradient entry
+// on each of the six strain rows (xx, yy, zz, xy, yz, xz)
+template <typename Real>
+__device__ __forceinline__ void m3_bcol(Real gx, Real gy, Real gz, int c, Real b[6]) {
+  b[0] = c == 0 ? gx : Real(0);
+  b[1] = c == 1 ? gy : Real(0);
+  b[2] = c == 2 ? gz : Real(0);
+  b[3] = c == 0 ? gy : (c == 1 ? gx : Real(0));
+  b[4] = c == 1 ? gz : (c == 2 ? gy : Real(0));
+  b[5] = c == 0 ? gz : (c == 2 ? gx : Real(0));
+}
+
+template <typename Real, int NP, int WANT>
+__global__ void __launch_bounds__(32 * kM3Warps) k_mc3d_elem(Mc3dArgs A, Real* __restrict__ kbuf,
+                                                             Real* __restrict__ gbuf) {
+  constexpr int N = 3 * NP, NPAIR = NP * (NP + 1) / 2;
+  __shared__ double s_u[kM3Warps][N];
+  __shared__ Real s_g[kM3Warps][3][kM3MaxQ * NP];   // gx, gy, gz per point
+  __shared__ Real s_sig[kM3Warps][kM3MaxQ][6];      // w sigma
+  __shared__ Real s_D[kM3Warps][kM3MaxQ][21];       // w D, upper triangle row-major
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nq = A.nq;
+  double eacc = 0.0;
+  for (int el = blockIdx.x * kM3Warps + warp; el < A.n_el; el += gridDim.x * kM3Warps) {
+    // nodal values and basis gradients
+    for (int i = lane; i < N; i += 32) {
+      const int code = __ldg(A.codes + (long long)el * N + i);
+      s_u[warp][i] = code >= 0 ? __ldg(A.u + code) : __ldg(A.dir + (-1 - code));
+    }
+    const double* gsrc = A.grad + (long long)el * 3 * nq * NP;
+    for (int i = lane; i < 3 * nq * NP; i += 32) {
+      const int k = i / (nq * NP), r = i - k * nq * NP;
+      s_g[warp][k][r] = (Real)__ldg(gsrc + i);
+    }
+    __syncwarp();
+    // constitutive update, one lane per quadrature point (FP64)
+    if (lane < nq) {
+      const int q = lane;
+      const double* gq = gsrc + q * NP;
+      double e[6] = {0, 0, 0, 0, 0, 0};
+      for (int a = 0; a < NP; ++a) {
+        const double gx = __ldg(gq + a), gy = __ldg(gq + nq * NP + a), gz = __ldg(gq + 2 * nq * NP + a);
+        const double ux = s_u[warp][3 * a], uy = s_u[warp][3 * a + 1], uz = s_u[warp][3 * a + 2];
+        e[0] += gx * ux;
+        e[1] += gy * uy;
+        e[2] += gz * uz;
+        e[3] += gy * ux + gx * uy;
+        e[4] += gz * uy + gy * uz;
+        e[5] += gz * ux + gx * uz;
+      }
+      const double* m = A.pt + ((long long)el * nq + q) * kM3Pt;
+      const double w = __ldg(m);
+      double psi, sig[6], D[6][6];
+      if (A.elastic)
+        m3_elastic(e, __ldg(m + 3), __ldg(m + 5), psi, sig, D);
+      else
+        mc3d::point(e, __ldg(m + 1), __ldg(m + 2), __ldg(m + 3), __ldg(m + 4), __ldg(m + 5), A.tiny, psi, sig, D);
+      if ((WANT & 1) && __ldg(A.wflag + el)) eacc += w * psi;
+      for (int i = 0; i < 6; ++i) s_sig[warp][q][i] = (Real)(w * sig[i]);
+      int t = 0;
+      for (int i = 0; i < 6; ++i)
+        for (int j = i; j < 6; ++j) s_D[warp][q][t++] = (Real)(w * D[i][j]);
+    }
+    __syncwarp();
+    // element gradient: lanes over (node, component)
+    if (WANT & 2) {
+      for (int i = lane; i < N; i += 32) {
+        const int a = i / 3, c = i - 3 * a;
+        Real s = Real(0);
+        for (int q = 0; q < nq; ++q) {
+          Real b[6];
+          m3_bcol<Real>(s_g[warp][0][q * NP + a], s_g[warp][1][q * NP + a], s_g[warp][2][q * NP + a], c, b);
+#pragma unroll
+          for (int k = 0; k < 6; ++k) s += b[k] * s_sig[warp][q][k];
+        }
+        gbuf[(long long)el * N + i] = s;
+      }
+    }
+    // Hessian blocks: lanes over node pairs a <= b
+    if (WANT & 4) {
+      for (int p = lane; p < NPAIR; p += 32) {
+        int a = 0, rem = p;
+        while (rem >= NP - a) {
+          rem -= NP - a;
+          ++a;
+        }
+        const int b = a + rem;
+        Real K[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int q = 0; q < nq; ++q) {
+          const Real* Dq = s_D[warp][q];
+          Real Dm[6][6];
+          int t = 0;
+#pragma unroll
+          for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int j = i; j < 6; ++j) {
+              Dm[i][j] = Dq[t];
+              Dm[j][i] = Dq[t];
+              ++t;
+            }
+          const Real ax = s_g[warp][0][q * NP + a], ay = s_g[warp][1][q * NP + a], az = s_g[warp][2][q * NP + a];
+          const Real bx = s_g[warp][0][q * NP + b], by = s_g[warp][1][q * NP + b], bz = s_g[warp][2][q * NP + b];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            Real bb[6], T[6];
+            m3_bcol<Real>(bx, by, bz, d, bb);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+              Real s = Real(0);
+#pragma unroll
+              for (int j = 0; j < 6; ++j) s += Dm[i][j] * bb[j];
+              T[i] = s;
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              Real ba[6];
+              m3_bcol<Real>(ax, ay, az, c, ba);
+              Real s = Real(0);
+#pragma unroll
+              for (int i = 0; i < 6; ++i) s += ba[i] * T[i];
+              K[c][d] += s;
+            }
+          }
+        }
+        Real* o = kbuf + ((long long)el * NPAIR + p) * 9;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) o[c * 3 + d] = K[c][d];
+      }
+    }
+    __syncwarp();
+  }
+  if (WANT & 1) {
+    if (A.rhs)  // load term -f.u of the owned DOFs
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_owned; i += gridDim.x * blockDim.x)
+        eacc -= A.rhs[i] * A.u[A.lo + i];
+    m3_energy_finalize(eacc, A);
+  }
+}
+
+}  // namespace
+
+struct Mc3dHandle {
+  int precision = 0, hess_fp32 = 0, np = 0, nq = 0, n_local = 0, num_sms = 148;
+  int64_t nnz = 0, lo = 0, hi = 0, n_free = 0, n_total = 0;
+  double tiny = 1.0e-15;
+  int elastic = 0;
+  int *codes = nullptr;
+  double *grad = nullptr, *pt = nullptr, *dir = nullptr, *rhs = nullptr, *partials = nullptr;
+  unsigned char* wflag = nullptr;
+  unsigned* counter = nullptr;
+  void *kbuf = nullptr, *gbuf = nullptr;
+  int grid_elem = 1, n_rnodes = 0;
+  int *bp_rn_blk = nullptr, *bp_rn_con = nullptr, *bp_rn_row = nullptr, *bp_rn_gpos = nullptr,
+      *bp_rn_inc = nullptr, *bp_con = nullptr, *bp_inc = nullptr;
+  unsigned* bp_blk = nullptr;
+  int64_t device_bytes = 0, n_contrib = 0;
+};
+
+namespace {
+
+template <typename T>
+int m3_upload(Mc3dHandle* h, T** p, const T* src, size_t count) {
+  *p = nullptr;
+  if (count == 0) return FNE_OK;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) return set_error(FNE_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  h->device_bytes += (int64_t)(count * sizeof(T));
+  if (src) {
+    e = cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+  }
+  return FNE_OK;
+}
+
+template <typename Real, typename HOut, int NP>
+cudaError_t m3_launch(Mc3dHandle* h, int flags, const double* u, double* energy, double* grad, void* hess,
+                      cudaStream_t st) {
+  Mc3dArgs A{h->n_local, h->nq,    h->codes, h->grad,    h->pt,  h->wflag, u,
+             h->dir,     h->rhs,   (int)(h->hi - h->lo), h->lo,  h->tiny,  h->elastic,
+             h->partials, h->counter, energy};
+  Real* kb = static_cast<Real*>(h->kbuf);
+  Real* gb = static_cast<Real*>(h->gbuf);
+  const dim3 grid(h->grid_elem), block(32 * kM3Warps);
+  switch (flags) {
+    case 1: k_mc3d_elem<Real, NP, 1><<<grid, block, 0, st>>>(A, kb, gb); break;
+    case 2: k_mc3d_elem<Real, NP, 2><<<grid, block, 0, st>>>(A, kb, gb); break;
+    case 3: k_mc3d_elem<Real, NP, 3><<<grid, block, 0, st>>>(A, kb, gb); break;
+    case 4: k_mc3d_elem<Real, NP, 4><<<grid, block, 0, st>>>(A, kb, gb); break;
+    case 5: k_mc3d_elem<Real, NP, 5><<<grid, block, 0, st>>>(A, kb, gb); break;
+    case 6: k_mc3d_elem<Real, NP, 6><<<grid, block, 0, st>>>(A, kb, gb); break;
+    default: k_mc3d_elem<Real, NP, 7><<<grid, block, 0, st>>>(A, kb, gb); break;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !(flags & 6) || h->n_rnodes == 0) return e;
+  NodeGatherArgs G{h->n_rnodes, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
+                   h->bp_rn_inc, h->bp_blk,   h->bp_con,    h->bp_inc,    h->rhs};
+  HOut* H = static_cast<HOut*>(hess);
+  if (flags & 4) {
+    const int gg = std::max(1, std::min(h->num_sms * 16, (h->n_rnodes + 7) / 8));
+    if (flags & 2)
+      k_node_gather<Real, HOut, 3, NP, true, true><<<gg, 256, 0, st>>>(G, kb, gb, H, grad);
+    else
+      k_node_gather<Real, HOut, 3, NP, true, false><<<gg, 256, 0, st>>>(G, kb, gb, H, grad);
+  } else {
+    const int gr = std::max(1, std::min(h->num_sms * 8, (h->n_rnodes + 255) / 256));
+    k_rowgrad<Real, 3><<<gr, 256, 0, st>>>(h->n_rnodes, h->bp_rn_inc, h->bp_inc, h->bp_rn_gpos, gb, h->rhs, grad);
+  }
+  return cudaGetLastError();
+}
+
+template <typename Real, typename HOut>
+cudaError_t m3_dispatch(Mc3dHandle* h, int flags, const double* u, double* energy, double* grad, void* hess,
+                        cudaStream_t st) {
+  if (h->np == 10) return m3_launch<Real, HOut, 10>(h, flags, u, energy, grad, hess, st);
+  return m3_launch<Real, HOut, 4>(h, flags, u, energy, grad, hess, st);
+}
+
+}  // namespace
+
+void mc3d_destroy(Mc3dHandle* h) {
+  if (!h) return;
+  void* ptrs[] = {h->codes, h->grad, h->pt, h->dir, h->rhs, h->partials, h->wflag, h->counter, h->kbuf, h->gbuf,
+                  h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos, h->bp_rn_inc, h->bp_con, h->bp_inc,
+                  h->bp_blk};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete h;
+}
+
+int mc3d_create(const fne_desc* d, Mc3dHandle** out) {
+  *out = nullptr;
+  const int np = d->npe, nq = d->nq, n = 3 * np;
+  if (d->block_size != 3) return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: block_size must be 3");
+  if (np != 4 && np != 10) return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: P1 (4 nodes) or P2 (10 nodes) tetrahedra");
+  if (nq < 1 || nq > kM3MaxQ) return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: 1 to 16 quadrature points");
+  if (d->n_elem > 0 && (!d->e0 || !d->e1 || !d->e2 || !d->e3))
+    return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: missing basis gradients or per-point inputs");
+  const int64_t E = d->n_elem, lo = d->lo, hi = d->hi;
+  const int64_t* t2f = d->total_to_free_reord;
+  const int npair = np * (np + 1) / 2;
+  if (E * (int64_t)npair * 9 >= (int64_t)INT32_MAX * 4 || d->nnz >= (int64_t)INT32_MAX)
+    return set_error(FNE_EBOUNDS, "Mohr-Coulomb 3-D: sizes beyond the supported indexing");
+  std::vector<int32_t> codes;
+  std::vector<double> grad, pt;
+  std::vector<uint8_t> wflag;
+  std::vector<int64_t> local;
+  for (int64_t e = 0; e < E; ++e) {
+    bool own = false;
+    for (int i = 0; i < n; ++i) {
+      const int64_t dof = d->elems[e * n + i];
+      if (dof < 0 || dof >= d->n_total) return set_error(FNE_EBOUNDS, "Mohr-Coulomb 3-D: element DOF out of range");
+      const int64_t r = t2f[dof];
+      own |= r >= lo && r < hi;
+    }
+    if (!own) continue;
+    local.push_back(e);
+    for (int i = 0; i < n; ++i) {
+      const int64_t dof = d->elems[e * n + i];
+      if (dof + 1 >= (int64_t)INT32_MAX) return set_error(FNE_EBOUNDS, "Mohr-Coulomb 3-D: DOF id beyond int32");
+      codes.push_back(t2f[dof] >= 0 ? (int32_t)t2f[dof] : (int32_t)(-1 - dof));
+    }
+    for (const double* g : {d->e0, d->e1, d->e2})
+      grad.insert(grad.end(), g + e * nq * np, g + (e + 1) * nq * np);
+    pt.insert(pt.end(), d->e3 + e * nq * kM3Pt, d->e3 + (e + 1) * nq * kM3Pt);
+    const double w = d->energy_weights ? d->energy_weights[e] : 1.0;
+    if (w != 0.0 && w != 1.0) return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: energy weights must be 0 or 1");
+    wflag.push_back(w != 0.0 ? 1 : 0);
+  }
+  const int64_t nl = (int64_t)local.size();
+  BlockPlan bp;
+  {
+    std::vector<int64_t> edofs((size_t)nl * n);
+    for (int64_t le = 0; le < nl; ++le)
+      for (int i = 0; i < n; ++i) edofs[(size_t)le * n + i] = d->elems[local[le] * n + i];
+    const int rc = build_block_plan(nl, np, 3, edofs.data(), d, bp);
+    if (rc) return rc;
+  }
+  auto* h = new (std::nothrow) Mc3dHandle();
+  if (!h) return set_error(FNE_ENOMEM, "Mohr-Coulomb 3-D: out of host memory");
+  h->precision = d->precision;
+  h->hess_fp32 = d->precision == FNE_FP32 && d->hess_fp32;
+  h->np = np;
+  h->nq = nq;
+  h->n_local = (int)nl;
+  h->nnz = d->nnz;
+  h->lo = lo;
+  h->hi = hi;
+  h->n_free = d->n_free;
+  h->n_total = d->n_total;
+  h->tiny = d->s[0] > 0.0 ? d->s[0] : 1.0e-15;
+  h->elastic = d->s[5] != 0.0;
+  h->n_rnodes = bp.n_rnodes;
+  h->n_contrib = (int64_t)bp.con.size();
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    mc3d_destroy(h);
+    return set_error(FNE_ECUDA, "Mohr-Coulomb 3-D: device query");
+  }
+  h->grid_elem = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)h->num_sms * 16, (nl + kM3Warps - 1) / kM3Warps));
+  const size_t rsz = d->precision == FNE_FP32 ? sizeof(float) : sizeof(double);
+  int rc = FNE_OK;
+#define M3_TRY(x)       \
+  do {                  \
+    rc = (x);           \
+    if (rc) {           \
+      mc3d_destroy(h);  \
+      return rc;        \
+    }                   \
+  } while (0)
+  M3_TRY(m3_upload(h, &h->codes, codes.data(), codes.size()));
+  M3_TRY(m3_upload(h, &h->grad, grad.data(), grad.size()));
+  M3_TRY(m3_upload(h, &h->pt, pt.data(), pt.size()));
+  M3_TRY(m3_upload(h, &h->wflag, wflag.data(), wflag.size()));
+  M3_TRY(m3_upload(h, &h->dir, d->dirichlet, (size_t)d->n_total));
+  if (d->rhs_owned) M3_TRY(m3_upload(h, &h->rhs, d->rhs_owned, (size_t)(hi - lo)));
+  M3_TRY(m3_upload(h, &h->partials, (const double*)nullptr, (size_t)h->grid_elem));
+  M3_TRY(m3_upload(h, &h->counter, (const unsigned*)nullptr, 1));
+  if (cudaMemset(h->counter, 0, sizeof(unsigned)) != cudaSuccess) {
+    mc3d_destroy(h);
+    return set_error(FNE_ECUDA, "Mohr-Coulomb 3-D: cudaMemset");
+  }
+  M3_TRY(m3_upload(h, &h->bp_rn_blk, bp.rn_blk.data(), bp.rn_blk.size()));
+  M3_TRY(m3_upload(h, &h->bp_rn_con, bp.rn_con.data(), bp.rn_con.size()));
+  M3_TRY(m3_upload(h, &h->bp_rn_row, bp.rn_row.data(), bp.rn_row.size()));
+  M3_TRY(m3_upload(h, &h->bp_rn_gpos, bp.rn_gpos.data(), bp.rn_gpos.size()));
+  M3_TRY(m3_upload(h, &h->bp_rn_inc, bp.rn_inc.data(), bp.rn_inc.size()));
+  M3_TRY(m3_upload(h, &h->bp_blk, bp.blk.data(), bp.blk.size()));
+  M3_TRY(m3_upload(h, &h->bp_con, bp.con.data(), bp.con.size()));
+  M3_TRY(m3_upload(h, &h->bp_inc, bp.inc.data(), bp.inc.size()));
+  unsigned char* kb = nullptr;
+  M3_TRY(m3_upload(h, &kb, (const unsigned char*)nullptr, std::max<size_t>(1, (size_t)nl * npair * 9 * rsz)));
+  h->kbuf = kb;
+  unsigned char* gb = nullptr;
+  M3_TRY(m3_upload(h, &gb, (const unsigned char*)nullptr, std::max<size_t>(1, (size_t)nl * n * rsz)));
+  h->gbuf = gb;
+#undef M3_TRY
+  *out = h;
+  return FNE_OK;
+}
+
+int mc3d_eval(Mc3dHandle* h, const double* u, int flags, double* energy, double* grad, void* hess, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e;
+  if (h->precision == FNE_FP64)
+    e = m3_dispatch<double, double>(h, flags, u, energy, grad, hess, st);
+  else if (h->hess_fp32)
+    e = m3_dispatch<float, float>(h, flags, u, energy, grad, hess, st);
+  else
+    e = m3_dispatch<float, double>(h, flags, u, energy, grad, hess, st);
+  if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("fne_eval launch: ") + cudaGetErrorString(e));
+  return FNE_OK;
+}
+
+int mc3d_set_dirichlet(Mc3dHandle* h, const double* dirichlet) {
+  cudaError_t e = cudaMemcpy(h->dir, dirichlet, h->n_total * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("fne_set_dirichlet: ") + cudaGetErrorString(e));
+  return FNE_OK;
+}
+
+void mc3d_info(const Mc3dHandle* h, fne_info* info) {
+  info->n_rows = h->hi - h->lo;
+  info->nnz = h->nnz;
+  info->n_elem = h->n_local;
+  info->n_incidences = h->n_contrib;
+  info->device_bytes = h->device_bytes;
+  info->max_row_len = 0;
+  info->kernel_variant = 11;
+  info->row_lanes = 1;
+}
+
+}  // namespace fne

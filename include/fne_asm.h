@@ -55,7 +55,8 @@ typedef enum {
   FNE_PLAPLACE = 1,        /* P1 triangles, scalar, (1/p)|grad u|^p      */
   FNE_GINZBURG_LANDAU = 2, /* P1 triangles, scalar, eps/2|grad u|^2+W(u) */
   FNE_NEOHOOKEAN = 3,      /* P1 tetrahedra, 3 dofs per node            */
-  FNE_MOHR_COULOMB = 4     /* Pk triangles, plane strain, 2 dofs/node   */
+  FNE_MOHR_COULOMB = 4,    /* Pk triangles, plane strain, 2 dofs/node   */
+  FNE_MOHR_COULOMB_3D = 5  /* P1 / P2 tetrahedra, 3 dofs/node           */
 } fne_family;
 
 typedef enum { FNE_FP64 = 0, FNE_FP32 = 1 } fne_precision;
@@ -151,13 +152,23 @@ typedef struct {
   const double* e1;
   const double* e2;
   const double* e3;
+  /*   Mohr-Coulomb 3-D (SlopeStability3DReorderedElementAssembler,
+   *                    src/problems/slope_stability_3d/jax_petsc/
+   *                    reordered_element_assembler.py:189-206): the
+   *                    reference's per-element, per-quadrature-point arrays
+   *                    e0 = dphix, e1 = dphiy, e2 = dphiz [E*nq*npe],
+   *                    e3 = [E*nq*6] (quad_weight, c_bar_q, sin_phi_q,
+   *                    shear_q, bulk_q, lame_q) per point,
+   *                    npe = 4 or 10, block_size = 3, nq <= 16          */
   /* scalars:
    *   p-Laplace : s[0] = p
    *   GL        : s[0] = eps, s[1..9] = ip (3x3 row-major), s[10..12] = w
    *   Neo-Hook. : s[0] = C1, s[1] = D1, s[2] = use_abs_det (0/1)
    *   M-C       : s[0] = E, s[1] = nu, s[2] = phi_deg, s[3] = cohesion,
    *               s[4] = reg, s[5] = elastic (0/1),
-   *               s[6] = geometry per quadrature point (0/1, see e0/e1)    */
+   *               s[6] = geometry per quadrature point (0/1, see e0/e1)
+   *   M-C 3-D   : s[0] = the density's guard constant (0: 1e-15),
+   *               s[5] = elastic (0/1)                                       */
   double s[16];
   const double* dirichlet;      /* [n_total] full DOF vector (Dirichlet part) */
   const double* rhs_owned;      /* [hi-lo] load vector f (reordered), or NULL */
@@ -198,7 +209,9 @@ typedef struct {
                            * 7 element-parallel tets + node-block gather,
                            * 8 banded sweep, push variant,
                            * 9 Mohr-Coulomb FP64 DMMA (mma.sync f64),
-                           * 10 row clusters (P1 triangles) */
+                           * 10 row clusters (P1 triangles),
+                           * 11 3-D Mohr-Coulomb warp-per-element kernel +
+                           * node-block gather */
   int32_t row_lanes;      /* lanes per output row of the tet row kernel, else 1 */
 } fne_info;
 
