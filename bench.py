@@ -383,6 +383,44 @@ def _mc(degree, h, precision):
     return build, sample
 
 
+def slope3d_state(params, amplitude=0.05):
+    """A smooth closed-form displacement of the 3-D slope (zero on the fixed
+    faces by the factor z x (L - x) y (W - y) in the constrained components),
+    large enough to reach the plastic branches."""
+    import numpy as np
+
+    X = np.asarray(params["nodes"], dtype=np.float64)
+    L, W, H = X[:, 0].max(), X[:, 1].max(), X[:, 2].max()
+    x, y, z = X[:, 0] / L, X[:, 1] / W, X[:, 2] / H
+    u = np.zeros((X.shape[0], 3))
+    u[:, 0] = amplitude * z * x * (1 - x) * np.sin(3.0 * y + 1.0)
+    u[:, 1] = amplitude * z * y * (1 - y) * np.cos(2.0 * x)
+    u[:, 2] = -amplitude * z * (1.0 + 0.5 * np.sin(4.0 * x) * np.cos(3.0 * y))
+    return u.ravel()
+
+
+def _mc3d(nx, ny, nz, precision):
+    def build(rank):
+        import torch
+
+        from fenics_nonlinear_energies_b200 import meshes
+        from fenics_nonlinear_energies_b200.assembler import SlopeStability3DCudaAssembler
+
+        params = meshes.slope3d_problem(nx=nx, ny=ny, nz=nz, degree=2, lam=1.0)
+        hd = torch.float32 if precision == "fp32" else torch.float64
+        asm = SlopeStability3DCudaAssembler(params, precision=precision, hess_dtype=hd)
+        return asm, _reordered(asm, slope3d_state(params)[params["freedofs"]])
+
+    def sample():
+        from fenics_nonlinear_energies_b200 import meshes
+
+        params = meshes.slope3d_problem(nx=2, ny=2, nz=1, degree=2, lam=1.0)
+        return "mc3d", {}, params, slope3d_state(params)[params["freedofs"]], int(params["elems"].shape[0]), \
+            "3-D slope 2x2x1 hexes, P2 tets"
+
+    return build, sample
+
+
 WORKLOADS = {
     "gl1024_fp32h": Workload(
         "gl1024_fp32h", "gl", "fp32", True, 3, 7, 4, False,
@@ -433,6 +471,11 @@ WORKLOADS = {
     "mc_p2_h0.08_fp64": Workload(
         "mc_p2_h0.08_fp64", "mc", "fp64", False, 6, 5, 8, True,
         "Mohr-Coulomb slope P2 h=0.08 (203,000 elements), 7-point rule, FP64", *_mc(2, 0.08, "fp64")),
+    "mc3d_p2_fp64": Workload(
+        "mc3d_p2_fp64", "mc3d", "fp64", False, 10, 396, 8, True,
+        "Mohr-Coulomb 3-D slope (length 40, width 10, heights 20 / 10), 40x16x16 hexes x 6 P2 tetrahedra "
+        "(61,440 elements), reference 11-point rule, c=6, phi=45 deg, E=2e4, nu=0.3, lambda=1 (Davis-B), smooth "
+        "synthetic state, FP64", *_mc3d(40, 16, 16, "fp64")),
     "plaplace128_newton_fp64": Workload(
         "plaplace128_newton_fp64", "plaplace", "fp64", False, 3, 7, 8, True,
         "Newton to ||g|| <= 1e-6 ||g_0||: p-Laplace p=3, f=-10, unit square 128x128 P1 triangles (32,768 "
@@ -472,7 +515,8 @@ REFERENCE_ARCHIVED = {
 
 KERNEL_NAMES = {1: "k_rows_tri", 2: "k_rows_tet", 3: "k_inc_tri", 4: "k_sweep_tri",
                 5: "k_mc_elem+k_node_gather+k_rowgrad", 6: "k_mc_tc+k_fixup2+k_rowgrad", 7: "k_he_elem+k_node_gather",
-                8: "k_push_tri", 9: "k_mc_dmma+k_fixup2+k_rowgrad", 10: "k_cluster_tri"}
+                8: "k_push_tri", 9: "k_mc_dmma+k_fixup2+k_rowgrad", 10: "k_cluster_tri",
+                11: "k_mc3d_elem+k_node_gather"}
 
 
 def algorithmic_bytes(w, asm, n_el, energy_only=False):
@@ -491,7 +535,8 @@ def algorithmic_bytes(w, asm, n_el, energy_only=False):
     return b
 
 
-ENERGY_KERNELS = {"plaplace": "k_energy_tri", "gl": "k_energy_tri", "he": "k_energy_tet", "mc": "k_mc_eg"}
+ENERGY_KERNELS = {"plaplace": "k_energy_tri", "gl": "k_energy_tri", "he": "k_energy_tet", "mc": "k_mc_eg",
+                  "mc3d": "k_mc3d_elem (energy)"}
 
 
 # ---------------------------------------------------------------------------
@@ -508,8 +553,50 @@ def _oracle_sample(w, min_seconds=8.0, max_passes=5):
     return asm, u, n_el, label, min_seconds, max_passes, int(torch.get_num_threads())
 
 
+def cpu_mc3d_baseline(w, energy_only=False):
+    """3-D Mohr-Coulomb: the oracle's element derivatives (the reference's
+    density restated, stress and tangent by torch float64 autodiff through
+    eigvalsh) over every element of a small slope, plus the np.add.at
+    scatter of the element blocks."""
+    import numpy as np
+    import torch
+
+    from oracle import energies3d as E3
+
+    _, _, p, u_free, n_el, label = w.sample()
+    u = p["u_0"].copy()
+    u[p["freedofs"]] = u_free
+    n = u.size
+
+    def step():
+        g, e_tot = np.zeros(n), 0.0
+        vals = []
+        for e in range(p["elems"].shape[0]):
+            args = (p["dphix"][e], p["dphiy"][e], p["dphiz"][e], p["quad_weight"][e],
+                    *[p[k][e] for k in ("c_bar", "sin_phi", "shear", "bulk", "lame")])
+            if energy_only:
+                eps = E3.strain6(u[p["elems"][e]], *args[:3])
+                e_tot += float(np.sum(args[3] * E3.mc_density(eps, *args[4:])[0]))
+                continue
+            ee, ge, He, _ = E3.element_derivatives(u[p["elems"][e]], *args)
+            e_tot += ee
+            np.add.at(g, p["elems"][e], ge)
+            vals.append(He)
+        return e_tot
+
+    t = time.perf_counter()
+    step()
+    dt = time.perf_counter() - t
+    what = "energy passes" if energy_only else "fused E+grad+Hess passes (element derivatives + np.add.at)"
+    return {"value": n_el / dt, "unit": "elements/s", "cores": int(torch.get_num_threads()), "kind": "port",
+            "sample": f"{label} ({n_el} elements), 1 of the {what} of the CPU restatement",
+            "seconds_per_pass": dt}
+
+
 def cpu_port_baseline(w, energy_only=False):
     """The oracle (CPU restatement of the reference path) on a bounded sample."""
+    if w.family == "mc3d":
+        return cpu_mc3d_baseline(w, energy_only)
     asm, u, n_el, label, min_s, max_p, cores = _oracle_sample(w)
     step = (lambda: asm.energy_fn(u)) if energy_only else (lambda: asm.all_in_one(u))  # noqa: E731
     step()  # warm-up
@@ -534,6 +621,21 @@ def run_reference(args):
 
     torch.set_num_threads(os.cpu_count() or 1)
     w = WORKLOADS[args.workload]
+    if w.family == "mc3d":  # the 3-D restatement: element loop of the oracle on a small slope
+        times = [cpu_mc3d_baseline(w, args.pass_ == "energy") for _ in range(max(1, min(args.steps, 3)))]
+        dt = sum(t["seconds_per_pass"] for t in times) / len(times)
+        base = times[0]
+        value = base["value"] * base["seconds_per_pass"] / dt
+        print(json.dumps({
+            "impl": "reference", "metric": "elements/s (energy)" if args.pass_ == "energy" else "elements/s (E+grad+Hess)",
+            "value": value, "unit": "elements/s", "n_gpus": world, "steps": len(times), "warmup": 0,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (closed-form state on the generated mesh)",
+            "config": {"workload": w.name, "description": w.desc, "sample": base["sample"]},
+            "cpu_baseline": dict(base, value=value),
+            "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+            flush=True)
+        return 0
     full = w.full is not None and w.op == "egh"
     if full:  # the whole configuration: one pass takes seconds on the host
         from oracle.assembler import OracleAssembler
@@ -632,6 +734,8 @@ def oracle_error(w, asm, u_host, e_dev, g_dev, h_dev):
     from oracle.assembler import OracleAssembler, restricted_rows
 
     fam = w.family
+    if fam == "mc3d":  # the autodiff oracle takes ~0.4 s per P2 element: checked by the parity tests instead
+        return None, None
     okw = {"block_size": asm.block_size, "coordinate_key": asm.coordinate_key, "dirichlet_key": asm.dirichlet_key}
     params = dict(asm.params)
     g = g_dev[: asm.n_owned].double().cpu().numpy()

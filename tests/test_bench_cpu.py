@@ -48,7 +48,8 @@ def test_workload_table():
     assert bench.ENERGY_KERNELS["mc"] == "k_mc_eg"
     for name in ("gl1024_fp64", "gl1024_fp32h", "plaplace128_fp64", "he160x8x8_fp64"):
         assert bench.WORKLOADS[name].full is not None, name
-    assert set(bench.ENERGY_KERNELS) == {"plaplace", "gl", "he", "mc"}
+    assert set(bench.ENERGY_KERNELS) == {"plaplace", "gl", "he", "mc", "mc3d"}
+    assert bench.KERNEL_NAMES[11] == "k_mc3d_elem+k_node_gather"
 
 
 @pytest.mark.timeout(600)
@@ -85,3 +86,15 @@ def test_reference_arm_runs_the_full_configuration(tmp_path):
     # elements with a free DOF (the two corner triangles have none), owned COO entries
     assert line["config"]["elements"] == 32_766 and line["config"]["coo_nnz"] == 111_889
     assert line["cpu_baseline"]["sample"].startswith("full configuration")
+
+
+@pytest.mark.timeout(300)
+def test_reference_arm_line_for_mc3d(tmp_path):
+    """--impl reference on the 3-D Mohr-Coulomb workload: the oracle's element loop on a small slope."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "mc3d_p2_fp64", "--steps", "1", "--warmup", "0"], capture_output=True, text=True,
+                         cwd=tmp_path, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    assert line["impl"] == "reference" and line["unit"] == "elements/s" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
