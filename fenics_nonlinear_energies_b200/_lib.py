@@ -101,6 +101,8 @@ def _load():
                                                C.c_int64, C.c_int64, vp, vp]),
         "fne_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, C.c_int64, C.c_int64, vp, C.c_int64, C.c_int64,
                                     vp, C.c_int64, C.c_float, vp]),
+        "fne_gemm_check_status": (C.c_int, []),
+        "fne_gemm_set_wait_limit": (C.c_int, [C.c_int64]),
         "fne_mlp_bias_act": (C.c_int, [C.c_int64, C.c_int, vp, vp, C.c_int, vp, vp, vp]),
         "fne_mlp_act_bwd": (C.c_int, [C.c_int64, vp, vp, C.c_int, vp, vp, vp]),
         "fne_mlp_colsum": (C.c_int, [C.c_int64, C.c_int, vp, vp, vp]),

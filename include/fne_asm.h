@@ -352,9 +352,19 @@ int fne_cg_destroy(fne_cg* cg);
  * ------------------------------------------------------------------------- */
 /* C[m, n] = sum_k A(m, k) B(k, n) + beta C[m, n], A(m, k) = A[m*sam + k*sak],
  * B(k, n) = B[k*sbk + n*sbn] (BF16), C row-major with leading dimension ldc
- * (FP32).  Tensor cores (mma.sync m16n8k16), 64x64 tiles. */
+ * (FP32).  5th-generation tensor cores (tcgen05.mma kind::f16, FP32
+ * accumulator in tensor memory), 128 x 128 (N > 32) or 128 x 32 tiles.
+ * The MMA-completion waits are bounded: a CTA that gives up writes nothing
+ * and sets the status fne_gemm_check_status reports. */
 int fne_gemm_bf16(int M, int N, int K, const void* A, int64_t sam, int64_t sak, const void* B, int64_t sbk,
                   int64_t sbn, float* C, int64_t ldc, float beta, void* stream);
+/* Synchronous read of the GEMM's status: FNE_OK, or FNE_ETIMEOUT when a wait
+ * gave up since the last call (the status is then cleared). */
+int fne_gemm_check_status(void);
+/* Polls of each MMA-completion wait of later fne_gemm_bf16 calls; < 0
+ * restores the default (2^22); 0 makes every tile give up at once (how the
+ * tests exercise the timeout path without a fault). */
+int fne_gemm_set_wait_limit(int64_t polls);
 /* Z += bias (per column); H = silu(Z) (act = 1) or Z (act = 0); H32 / H16 may be NULL. */
 int fne_mlp_bias_act(int64_t rows, int cols, float* Z, const float* bias, int act, float* H32, void* H16,
                      void* stream);

@@ -20,7 +20,8 @@ from fenics_nonlinear_energies_b200 import meshes
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("M,N,K", [(64, 64, 32), (200, 96, 40), (1, 7, 300), (513, 257, 129)])
+@pytest.mark.parametrize("M,N,K", [(64, 64, 32), (200, 96, 40), (1, 7, 300), (513, 257, 129), (8192, 256, 256),
+                                   (300, 3, 256), (5, 33, 12), (130, 32, 0)])
 @pytest.mark.parametrize("transA", [False, True])
 @pytest.mark.parametrize("transB", [False, True])
 def test_gemm_bf16(M, N, K, transA, transB):
@@ -38,6 +39,31 @@ def test_gemm_bf16(M, N, K, transA, transB):
     gemm(Ad, sam, sak, Bd, sbk, sbn, M, N, K, C, beta=0.5)
     got = C.double().cpu() - 1.5
     assert (got - ref).abs().max() <= 1e-5 * ref.abs().max() + 1e-5
+
+
+def test_gemm_wait_timeout_is_reported():
+    """The tensor-core GEMM's MMA-completion wait, set to give up at once:
+    fne_gemm_check_status reports FNE_ETIMEOUT (then cleared), and with the
+    default bound restored the next product is exact again."""
+    from fenics_nonlinear_energies_b200 import _lib
+    from fenics_nonlinear_energies_b200.warmstart import gemm
+
+    A = torch.randn(256, 64).to(torch.bfloat16)
+    B = torch.randn(64, 128).to(torch.bfloat16)
+    C = torch.zeros(256, 128, dtype=torch.float32, device="cuda")
+    _lib.check(_lib.lib.fne_gemm_set_wait_limit(0))
+    try:
+        gemm(A.cuda(), 64, 1, B.cuda(), 128, 1, 256, 128, 64, C)
+        torch.cuda.synchronize()
+        assert _lib.lib.fne_gemm_check_status() == _lib.FNE_ETIMEOUT
+        assert _lib.lib.fne_gemm_check_status() == _lib.FNE_OK
+    finally:
+        _lib.check(_lib.lib.fne_gemm_set_wait_limit(-1))
+    gemm(A.cuda(), 64, 1, B.cuda(), 128, 1, 256, 128, 64, C)
+    torch.cuda.synchronize()
+    assert _lib.lib.fne_gemm_check_status() == _lib.FNE_OK
+    ref = A.double() @ B.double()
+    assert (C.double().cpu() - ref).abs().max() <= 1e-5 * ref.abs().max()
 
 
 def test_mlp_forward_backward_match_oracle():
