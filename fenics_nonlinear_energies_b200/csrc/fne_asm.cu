@@ -244,10 +244,12 @@ __device__ __forceinline__ double tri_energy(const Phys& P, const double v[3], c
 }
 
 // All three rows at once: gradient g[3] and the symmetric Hessian as its upper
-// triangle H = {H00, H01, H02, H11, H12, H22}.
-template <typename Real, int FAM>
+// triangle H = {H00, H01, H02, H11, H12, H22}; with WITH_E also the element
+// energy, formed from the same intermediates in the arithmetic (and to the
+// bit) of tri_energy_r.
+template <typename Real, int FAM, bool WITH_E = false>
 __device__ __forceinline__ void tri_full(const Phys& P, const Real v[3], const TriElem<Real>& t, Real g[3],
-                                         Real H[6]) {
+                                         Real H[6], double* energy = nullptr) {
   const Real fx = v[0] * t.dvx[0] + v[1] * t.dvx[1] + v[2] * t.dvx[2];
   const Real fy = v[0] * t.dvy[0] + v[1] * t.dvy[1] + v[2] * t.dvy[2];
   Real G[3];
@@ -276,6 +278,10 @@ __device__ __forceinline__ void tri_full(const Phys& P, const Real v[3], const T
       t1 = P.p == 2.0 ? Real(1) : (P.p > 2.0 ? Real(0) : Real(INFINITY));
       t2 = Real(0);
     }
+    if (WITH_E) {
+      const Real ps = P.p_is3 ? s * sqrt(s) : pow(s, Real(0.5) * p);
+      *energy = (double)(ps * t.vol / p);
+    }
     const Real vt1 = t.vol * t1, vt2 = t.vol * t2;
 #pragma unroll
     for (int b = 0; b < 3; ++b) g[b] = vt1 * G[b];
@@ -291,11 +297,20 @@ __device__ __forceinline__ void tri_full(const Phys& P, const Real v[3], const T
 #pragma unroll
     for (int k = 0; k < 9; ++k) ip[k] = prm<Real>(P.ip[k], P.ipf[k]);
     Real c1[3], c2[3];
+    Real pot = Real(0);
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const Real n = v[0] * ip[q] + v[1] * ip[3 + q] + v[2] * ip[6 + q];
       c1[q] = prm<Real>(P.w[q], P.wf[q]) * (n * n - Real(1)) * n;
       c2[q] = prm<Real>(P.w[q], P.wf[q]) * (Real(3) * n * n - Real(1));
+      if (WITH_E) {
+        const Real m = n * n - Real(1);
+        pot += m * m * prm<Real>(P.w[q], P.wf[q]);
+      }
+    }
+    if (WITH_E) {
+      const Real s = fx * fx + fy * fy;
+      *energy = (double)((Real(0.5) * eps * s + Real(0.25) * pot) * t.vol);
     }
 #pragma unroll
     for (int b = 0; b < 3; ++b)
@@ -974,7 +989,13 @@ __global__ void __launch_bounds__(NB, 2) k_sweep_tri(RowArgs A, SweepArgs S, con
     // (2) phase A: element gradient / Hessian of batch b into shared memory
     if (cur.elem_ok) {
       Real g[3], H[6];
-      tri_full<Real, FAM>(P, cur.v, cur.t, g, H);
+      if ((WANT & W_E) && e >= o_lo && cur.t.wflag) {
+        double ee;
+        tri_full<Real, FAM, true>(P, cur.v, cur.t, g, H, &ee);
+        eacc += ee;
+      } else {
+        tri_full<Real, FAM>(P, cur.v, cur.t, g, H);
+      }
       if (WANT & W_H) {
         Real* hs = sH + threadIdx.x;
         hs[0 * NB] = H[0]; hs[1 * NB] = H[1]; hs[2 * NB] = H[2];
@@ -985,7 +1006,6 @@ __global__ void __launch_bounds__(NB, 2) k_sweep_tri(RowArgs A, SweepArgs S, con
 #pragma unroll
         for (int k = 0; k < 3; ++k) sG[k * NB + threadIdx.x] = g[k];
       }
-      if ((WANT & W_E) && e >= o_lo && cur.t.wflag) eacc += tri_energy_r<Real, FAM>(P, cur.v, cur.t);
     }
     // (3) level-2 loads of batch b+1
     if (has_next) {

@@ -127,3 +127,32 @@ def test_device_cg_argument_checks_on_host():
     with pytest.raises(_lib.FneError) as ei:
         DeviceCG(3, np.array([0, 1, 2]), np.array([0, 1, 2]), device="cpu", chunk=0)
     assert ei.value.code == _lib.FNE_EINVAL
+
+
+def test_mc3d_descriptor_checks_on_host():
+    """fne_create for the 3-D Mohr-Coulomb family checks its descriptor on the
+    host before any device call: nodes per element (4 or 10), block size 3,
+    1 to 16 quadrature points and the presence of the per-point arrays."""
+    import ctypes as C
+
+    p = meshes.slope3d_problem(nx=2, ny=2, nz=1, degree=1)
+    el, pel = _lib.i64(p["elems"])
+    t2f, pt2f = _lib.i64(np.full(p["u_0"].size, -1, dtype=np.int64))
+    dirv, pdir = _lib.f64(p["u_0"])
+    keep = [el, t2f, dirv]
+
+    def desc(**kw):
+        d = _lib.Desc()
+        d.family, d.precision, d.n_elem, d.npe, d.block_size = _lib.FNE_MOHR_COULOMB_3D, 0, el.shape[0], 4, 3
+        d.elems, d.n_total, d.total_to_free_reord, d.dirichlet, d.nq = pel, p["u_0"].size, pt2f, pdir, 1
+        for k, v in kw.items():
+            setattr(d, k, v)
+        return d
+
+    h = C.c_void_p()
+    for kw, what in (({"npe": 6}, "tetrahedra"), ({"block_size": 2}, "block_size"), ({"nq": 17}, "quadrature"),
+                     ({}, "missing")):
+        rc = _lib.lib.fne_create(C.byref(desc(**kw)), C.byref(h))
+        assert rc == _lib.FNE_EINVAL, (kw, rc)
+        assert what in _lib.lib.fne_last_error().decode(), _lib.lib.fne_last_error()
+    del keep
