@@ -82,6 +82,7 @@ FLUSH_BYTES = 1 << 30
 # with the profile summary that records it.  Keyed by (workload, kernel).
 NCU_TRAFFIC = {
     ("gl1024_fp32h", "k_sweep_tri"): (213.2e6, "profiles/k_sweep_tri_gl1024_fp32.md"),
+    ("gl1024_fp64", "k_sweep_tri"): (330.6e6, "profiles/k_sweep_tri_gl1024_fp64.md"),
     # one CG iteration: k_cg_spmv 117.4 MB + k_cg_update 41.9 MB
     ("gl1024_newton_fp64", "k_cg_spmv+k_cg_update"): (159.3e6, "profiles/k_cg_gl1024_newton_fp64.md"),
 }

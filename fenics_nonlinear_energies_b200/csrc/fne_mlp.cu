@@ -6,7 +6,8 @@
 //    operands and an FP32 accumulator in tensor memory (TMEM).  One CTA per
 //    128 x BN tile of C (BN = 32 or 128); the 128 threads stage each 64-deep K
 //    slice of A and B into shared memory in the no-swizzle K-major
-//    core-matrix layout (8 rows x 16 bytes; zero-filled at the edges), one
+//    core-matrix layout (8 rows x 16 bytes; zero-filled at the edges; eight
+//    values per load where an operand's K direction is contiguous), one
 //    thread issues the four K = 16 MMAs of the slice and commits them to an
 //    mbarrier (bounded wait), and the epilogue reads the accumulator back
 //    with tcgen05.ld (each warp its 32-lane quadrant).  Operands are
@@ -116,8 +117,21 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const __nv
   constexpr uint32_t idesc = tcg::idesc_bf16(kTcBM, BN);
   const __nv_bfloat16 zero = __float2bfloat16(0.f);
   uint32_t phase = 0;
+  // operands whose K direction is contiguous and 16-byte aligned are staged
+  // eight values (one core-matrix row of 16 bytes) per load
+  const bool a_vec = sak == 1 && (K & 7) == 0 && (sam & 7) == 0 && ((uintptr_t)A & 15) == 0;
+  const bool b_vec = sbk == 1 && (K & 7) == 0 && (sbn & 7) == 0 && ((uintptr_t)B & 15) == 0;
   for (int k0 = 0; k0 < K; k0 += kTcBK) {
     // stage the slices (walking the operand's contiguous direction fastest)
+    if (a_vec) {
+      for (int idx = tid; idx < kTcBM * (kTcBK / 8); idx += 128) {
+        const int r = idx / (kTcBK / 8), c8 = idx - r * (kTcBK / 8);
+        const int m = m0 + r, k = k0 + 8 * c8;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (m < M && k < K) v = __ldg(reinterpret_cast<const uint4*>(A + (long long)m * sam + k));
+        *reinterpret_cast<uint4*>(&sA[c8][r][0]) = v;
+      }
+    } else
     for (int idx = tid; idx < kTcBM * kTcBK; idx += 128) {
       int r, c;
       if (sak == 1) {
@@ -128,6 +142,15 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const __nv
       const int m = m0 + r, k = k0 + c;
       sA[c >> 3][r][c & 7] = (m < M && k < K) ? A[(long long)m * sam + (long long)k * sak] : zero;
     }
+    if (b_vec) {
+      for (int idx = tid; idx < BN * (kTcBK / 8); idx += 128) {
+        const int r = idx / (kTcBK / 8), c8 = idx - r * (kTcBK / 8);
+        const int n = n0 + r, k = k0 + 8 * c8;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (n < N && k < K) v = __ldg(reinterpret_cast<const uint4*>(B + (long long)n * sbn + k));
+        *reinterpret_cast<uint4*>(&sB[c8][r][0]) = v;
+      }
+    } else
     for (int idx = tid; idx < BN * kTcBK; idx += 128) {
       int r, c;
       if (sbk == 1) {
