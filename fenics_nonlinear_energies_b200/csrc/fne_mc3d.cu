@@ -14,15 +14,17 @@
 // quad_weight and the material fields c_bar_q, sin_phi_q, shear_q, bulk_q,
 // lame_q (E, nq).
 //
-// k_mc3d_elem: one warp per element.  Lanes over quadrature points form the
-// strain and run the constitutive point function (FP64: eigen-decomposition
-// by fixed-sweep Jacobi, branch potentials, spectral tangent) and store
-// w sigma and the upper triangle of w D in shared memory; lanes over
-// (node, component) form the element gradient; lanes over node pairs a <= b
-// form the 3 x 3 blocks of B^T (w D) B.  Blocks and gradients go to
-// per-element buffers that the node-block gather (fne_gather.cuh: per output
-// block, contributions in element order, no atomics) sums into the COO values
-// and the gradient.  FP32 mode keeps the point function in FP64 and runs the
+// k_mc3d_elem: a CTA of 128 threads takes a tile of 128 / nq elements.  One
+// thread per (element, quadrature point) forms the strain and runs the
+// constitutive point function (FP64: eigen-decomposition by fixed-sweep
+// Jacobi, branch potentials, spectral tangent) and stores w sigma and the
+// upper triangle of w D in shared memory.  Then one warp per element: lanes
+// over (node, component) form the element gradient; per quadrature point,
+// lanes over nodes form (w D) B(b) from the three nonzeros of each column of
+// B and lanes over node pairs a <= b add B(a)^T (w D) B(b) to their 3 x 3
+// blocks.  Blocks and gradients go to per-element buffers that the
+// node-block gather (fne_gather.cuh: per output block, contributions in
+// element order, no atomics) sums into the COO values and the gradient.  FP32 mode keeps the point function in FP64 and runs the
 // contraction, the buffers and the Hessian output in FP32.
 #include <cuda_runtime.h>
 
@@ -39,7 +41,7 @@ namespace fne {
 
 namespace {
 
-constexpr int kM3Warps = 4;      // warps (elements in flight) per CTA
+constexpr int kM3Warps = 4;      // warps per CTA
 constexpr int kM3MaxQ = 16;      // quadrature points per element (kernel limit)
 constexpr int kM3Pt = 6;         // per-point inputs: w, c_bar, sin_phi, shear, bulk, lame
 
@@ -129,126 +131,174 @@ __device__ __forceinline__ void m3_bcol(Real gx, Real gy, Real gz, int c, Real b
   b[5] = c == 0 ? gz : (c == 2 ? gx : Real(0));
 }
 
+// One quadrature point (FP64): strain from the nodal values, the point
+// function, w sigma and the upper triangle of w D to shared memory; returns
+// w psi.  Not inlined, so every instantiation of the element kernel runs the
+// same machine code here and the separate energy / gradient / Hessian passes
+// reproduce the fused pass bit for bit.
+template <typename Real, int NP>
+__device__ __noinline__ double m3_point_update(const double* __restrict__ grad, const int* __restrict__ codes,
+                                               const double* __restrict__ u, const double* __restrict__ dir,
+                                               const double* __restrict__ pt, int el, int q, int nq, double tiny,
+                                               int elastic, Real* sig_out, Real* D_out) {
+  const double* gq = grad + (long long)el * 3 * nq * NP + q * NP;
+  const int* cd = codes + (long long)el * 3 * NP;
+  double e[6] = {0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < NP; ++a) {
+    double uc[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int code = __ldg(cd + 3 * a + c);
+      uc[c] = code >= 0 ? __ldg(u + code) : __ldg(dir + (-1 - code));
+    }
+    const double gx = __ldg(gq + a), gy = __ldg(gq + nq * NP + a), gz = __ldg(gq + 2 * nq * NP + a);
+    e[0] += gx * uc[0];
+    e[1] += gy * uc[1];
+    e[2] += gz * uc[2];
+    e[3] += gy * uc[0] + gx * uc[1];
+    e[4] += gz * uc[1] + gy * uc[2];
+    e[5] += gz * uc[0] + gx * uc[2];
+  }
+  const double* m = pt + ((long long)el * nq + q) * kM3Pt;
+  const double w = __ldg(m);
+  double psi, sig[6], D[6][6];
+  if (elastic)
+    m3_elastic(e, __ldg(m + 3), __ldg(m + 5), psi, sig, D);
+  else
+    mc3d::point(e, __ldg(m + 1), __ldg(m + 2), __ldg(m + 3), __ldg(m + 4), __ldg(m + 5), tiny, psi, sig, D);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) sig_out[i] = (Real)(w * sig[i]);
+  int t = 0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = i; j < 6; ++j) D_out[t++] = (Real)(w * D[i][j]);
+  return w * psi;
+}
+
 template <typename Real, int NP, int WANT>
-__global__ void __launch_bounds__(32 * kM3Warps) k_mc3d_elem(Mc3dArgs A, Real* __restrict__ kbuf,
+__global__ void __launch_bounds__(32 * kM3Warps, 3) k_mc3d_elem(Mc3dArgs A, Real* __restrict__ kbuf,
                                                              Real* __restrict__ gbuf) {
-  constexpr int N = 3 * NP, NPAIR = NP * (NP + 1) / 2;
-  __shared__ double s_u[kM3Warps][N];
-  __shared__ Real s_g[kM3Warps][3][kM3MaxQ * NP];   // gx, gy, gz per point
-  __shared__ Real s_sig[kM3Warps][kM3MaxQ][6];      // w sigma
-  __shared__ Real s_D[kM3Warps][kM3MaxQ][21];       // w D, upper triangle row-major
+  constexpr int N = 3 * NP, NPAIR = NP * (NP + 1) / 2, NT = 32 * kM3Warps;
+  __shared__ Real s_sig[NT][6];                      // w sigma per point of the tile
+  __shared__ Real s_D[NT][21];                       // w D, upper triangle row-major
+  __shared__ Real s_g[kM3Warps][3][kM3MaxQ * NP];    // gx, gy, gz of the warp's element
+  __shared__ Real s_T[kM3Warps][NP][18];             // (w D) B(b) of one point, per node
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nq = A.nq;
+  const int nq = A.nq, epc = NT / nq;                // elements per tile: all their points in one pass
   double eacc = 0.0;
-  for (int el = blockIdx.x * kM3Warps + warp; el < A.n_el; el += gridDim.x * kM3Warps) {
-    // nodal values and basis gradients
-    for (int i = lane; i < N; i += 32) {
-      const int code = __ldg(A.codes + (long long)el * N + i);
-      s_u[warp][i] = code >= 0 ? __ldg(A.u + code) : __ldg(A.dir + (-1 - code));
+  for (int el0 = blockIdx.x * epc; el0 < A.n_el; el0 += gridDim.x * epc) {
+    const int ne = min(epc, A.n_el - el0);
+    // constitutive update, one thread per (element, quadrature point) of the
+    // tile (FP64): strain from the nodal values, then the point function
+    if ((int)threadIdx.x < ne * nq) {
+      const int j = threadIdx.x / nq, q = threadIdx.x - j * nq, el = el0 + j;
+      const double wpsi = m3_point_update<Real, NP>(A.grad, A.codes, A.u, A.dir, A.pt, el, q, nq, A.tiny,
+                                                    A.elastic, s_sig[threadIdx.x], s_D[threadIdx.x]);
+      if ((WANT & 1) && __ldg(A.wflag + el)) eacc += wpsi;
     }
-    const double* gsrc = A.grad + (long long)el * 3 * nq * NP;
-    for (int i = lane; i < 3 * nq * NP; i += 32) {
-      const int k = i / (nq * NP), r = i - k * nq * NP;
-      s_g[warp][k][r] = (Real)__ldg(gsrc + i);
-    }
-    __syncwarp();
-    // constitutive update, one lane per quadrature point (FP64)
-    if (lane < nq) {
-      const int q = lane;
-      const double* gq = gsrc + q * NP;
-      double e[6] = {0, 0, 0, 0, 0, 0};
-      for (int a = 0; a < NP; ++a) {
-        const double gx = __ldg(gq + a), gy = __ldg(gq + nq * NP + a), gz = __ldg(gq + 2 * nq * NP + a);
-        const double ux = s_u[warp][3 * a], uy = s_u[warp][3 * a + 1], uz = s_u[warp][3 * a + 2];
-        e[0] += gx * ux;
-        e[1] += gy * uy;
-        e[2] += gz * uz;
-        e[3] += gy * ux + gx * uy;
-        e[4] += gz * uy + gy * uz;
-        e[5] += gz * ux + gx * uz;
+    __syncthreads();
+    // contraction: one warp per element of the tile
+    for (int j = warp; (WANT & 6) && j < ne; j += kM3Warps) {
+      const int el = el0 + j;
+      const Real(*sg)[6] = s_sig + j * nq;
+      const Real(*sD)[21] = s_D + j * nq;
+      const double* gsrc = A.grad + (long long)el * 3 * nq * NP;
+      for (int i = lane; i < 3 * nq * NP; i += 32) {
+        const int k = i / (nq * NP), r = i - k * nq * NP;
+        s_g[warp][k][r] = (Real)__ldg(gsrc + i);
       }
-      const double* m = A.pt + ((long long)el * nq + q) * kM3Pt;
-      const double w = __ldg(m);
-      double psi, sig[6], D[6][6];
-      if (A.elastic)
-        m3_elastic(e, __ldg(m + 3), __ldg(m + 5), psi, sig, D);
-      else
-        mc3d::point(e, __ldg(m + 1), __ldg(m + 2), __ldg(m + 3), __ldg(m + 4), __ldg(m + 5), A.tiny, psi, sig, D);
-      if ((WANT & 1) && __ldg(A.wflag + el)) eacc += w * psi;
-      for (int i = 0; i < 6; ++i) s_sig[warp][q][i] = (Real)(w * sig[i]);
-      int t = 0;
-      for (int i = 0; i < 6; ++i)
-        for (int j = i; j < 6; ++j) s_D[warp][q][t++] = (Real)(w * D[i][j]);
-    }
-    __syncwarp();
-    // element gradient: lanes over (node, component)
-    if (WANT & 2) {
-      for (int i = lane; i < N; i += 32) {
-        const int a = i / 3, c = i - 3 * a;
-        Real s = Real(0);
-        for (int q = 0; q < nq; ++q) {
-          Real b[6];
-          m3_bcol<Real>(s_g[warp][0][q * NP + a], s_g[warp][1][q * NP + a], s_g[warp][2][q * NP + a], c, b);
+      __syncwarp();
+      // element gradient: lanes over (node, component)
+      if (WANT & 2) {
+        for (int i = lane; i < N; i += 32) {
+          const int a = i / 3, c = i - 3 * a;
+          Real s = Real(0);
+          for (int q = 0; q < nq; ++q) {
+            Real b[6];
+            m3_bcol<Real>(s_g[warp][0][q * NP + a], s_g[warp][1][q * NP + a], s_g[warp][2][q * NP + a], c, b);
 #pragma unroll
-          for (int k = 0; k < 6; ++k) s += b[k] * s_sig[warp][q][k];
+            for (int k = 0; k < 6; ++k) s += b[k] * sg[q][k];
+          }
+          gbuf[(long long)el * N + i] = s;
         }
-        gbuf[(long long)el * N + i] = s;
       }
-    }
-    // Hessian blocks: lanes over node pairs a <= b
-    if (WANT & 4) {
-      for (int p = lane; p < NPAIR; p += 32) {
-        int a = 0, rem = p;
-        while (rem >= NP - a) {
-          rem -= NP - a;
-          ++a;
+      // Hessian blocks B(a)^T (w D) B(b) over the node pairs a <= b.  Each
+      // column of B has three nonzeros (DOF (b, d) feeds three strain rows), so
+      // per quadrature point the lanes over nodes first form T_b = (w D) B(b)
+      // (6 x 3, 18 products of three terms) and the lanes over pairs then add
+      // B(a)^T T_b (9 sums of three terms)
+      if (WANT & 4) {
+        constexpr int PPL = (NPAIR + 31) / 32;  // pairs per lane
+        Real K[PPL][3][3];
+        int pa[PPL], pb[PPL];
+#pragma unroll
+        for (int k = 0; k < PPL; ++k) {
+          int a = 0, rem = lane + 32 * k;
+          while (a < NP && rem >= NP - a) {
+            rem -= NP - a;
+            ++a;
+          }
+          pa[k] = a;
+          pb[k] = a + rem;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) K[k][c][d] = Real(0);
         }
-        const int b = a + rem;
-        Real K[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         for (int q = 0; q < nq; ++q) {
-          const Real* Dq = s_D[warp][q];
-          Real Dm[6][6];
-          int t = 0;
+          if (lane < NP) {
+            const Real* Dq = sD[q];
+            Real D[6][6];
+            int t = 0;
 #pragma unroll
-          for (int i = 0; i < 6; ++i)
+            for (int i = 0; i < 6; ++i)
 #pragma unroll
-            for (int j = i; j < 6; ++j) {
-              Dm[i][j] = Dq[t];
-              Dm[j][i] = Dq[t];
-              ++t;
-            }
-          const Real ax = s_g[warp][0][q * NP + a], ay = s_g[warp][1][q * NP + a], az = s_g[warp][2][q * NP + a];
-          const Real bx = s_g[warp][0][q * NP + b], by = s_g[warp][1][q * NP + b], bz = s_g[warp][2][q * NP + b];
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            Real bb[6], T[6];
-            m3_bcol<Real>(bx, by, bz, d, bb);
+              for (int j = i; j < 6; ++j) {
+                D[i][j] = Dq[t];
+                D[j][i] = Dq[t];
+                ++t;
+              }
+            const Real gx = s_g[warp][0][q * NP + lane], gy = s_g[warp][1][q * NP + lane],
+                       gz = s_g[warp][2][q * NP + lane];
+            Real* T = s_T[warp][lane];
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
-              Real s = Real(0);
-#pragma unroll
-              for (int j = 0; j < 6; ++j) s += Dm[i][j] * bb[j];
-              T[i] = s;
-            }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              Real ba[6];
-              m3_bcol<Real>(ax, ay, az, c, ba);
-              Real s = Real(0);
-#pragma unroll
-              for (int i = 0; i < 6; ++i) s += ba[i] * T[i];
-              K[c][d] += s;
+              T[i * 3 + 0] = D[i][0] * gx + D[i][3] * gy + D[i][5] * gz;
+              T[i * 3 + 1] = D[i][1] * gy + D[i][3] * gx + D[i][4] * gz;
+              T[i * 3 + 2] = D[i][2] * gz + D[i][4] * gy + D[i][5] * gx;
             }
           }
+          __syncwarp();
+#pragma unroll
+          for (int k = 0; k < PPL; ++k) {
+            if (lane + 32 * k >= NPAIR) continue;
+            const Real ax = s_g[warp][0][q * NP + pa[k]], ay = s_g[warp][1][q * NP + pa[k]],
+                       az = s_g[warp][2][q * NP + pa[k]];
+            const Real* T = s_T[warp][pb[k]];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              K[k][0][d] += ax * T[0 * 3 + d] + ay * T[3 * 3 + d] + az * T[5 * 3 + d];
+              K[k][1][d] += ay * T[1 * 3 + d] + ax * T[3 * 3 + d] + az * T[4 * 3 + d];
+              K[k][2][d] += az * T[2 * 3 + d] + ay * T[4 * 3 + d] + ax * T[5 * 3 + d];
+            }
+          }
+          __syncwarp();
         }
-        Real* o = kbuf + ((long long)el * NPAIR + p) * 9;
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
+        for (int k = 0; k < PPL; ++k) {
+          const int p = lane + 32 * k;
+          if (p >= NPAIR) continue;
+          Real* o = kbuf + ((long long)el * NPAIR + p) * 9;
 #pragma unroll
-          for (int d = 0; d < 3; ++d) o[c * 3 + d] = K[c][d];
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) o[c * 3 + d] = K[k][c][d];
+        }
       }
+      __syncwarp();
     }
-    __syncwarp();
+    __syncthreads();
   }
   if (WANT & 1) {
     if (A.rhs)  // load term -f.u of the owned DOFs
@@ -291,6 +341,16 @@ int m3_upload(Mc3dHandle* h, T** p, const T* src, size_t count) {
     if (e != cudaSuccess) return set_error(FNE_ECUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
   }
   return FNE_OK;
+}
+
+// resident CTAs per SM of the fused pass (registers and shared memory)
+template <typename Real>
+int m3_ctas_per_sm(int np) {
+  int n = 0;
+  const cudaError_t e =
+      np == 10 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mc3d_elem<Real, 10, 7>, 32 * kM3Warps, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mc3d_elem<Real, 4, 7>, 32 * kM3Warps, 0);
+  return e == cudaSuccess && n > 0 ? n : 2;
 }
 
 template <typename Real, typename HOut, int NP>
@@ -418,7 +478,11 @@ int mc3d_create(const fne_desc* d, Mc3dHandle** out) {
     mc3d_destroy(h);
     return set_error(FNE_ECUDA, "Mohr-Coulomb 3-D: device query");
   }
-  h->grid_elem = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)h->num_sms * 16, (nl + kM3Warps - 1) / kM3Warps));
+  // tiles of 128 / nq elements (all their points in one pass of the CTA);
+  // one wave of resident CTAs, each striding over the tiles
+  const int64_t epc = 32 * kM3Warps / nq;
+  const int per_sm = d->precision == FNE_FP64 ? m3_ctas_per_sm<double>(h->np) : m3_ctas_per_sm<float>(h->np);
+  h->grid_elem = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)h->num_sms * per_sm, (nl + epc - 1) / epc));
   const size_t rsz = d->precision == FNE_FP32 ? sizeof(float) : sizeof(double);
   int rc = FNE_OK;
 #define M3_TRY(x)       \

@@ -46,6 +46,7 @@ FNE_HD void eigh3(const double A0[3][3], double w[3], double V[3][3]) {
     }
   const int P[3] = {0, 0, 1}, Qi[3] = {1, 2, 2};
   for (int sweep = 0; sweep < 6; ++sweep) {
+#pragma unroll
     for (int r = 0; r < 3; ++r) {
       const int p = P[r], q = Qi[r];
       const double apq = a[p][q];
@@ -72,22 +73,26 @@ FNE_HD void eigh3(const double A0[3][3], double w[3], double V[3][3]) {
       }
     }
   }
-  // sort descending (three elements)
-  int o[3] = {0, 1, 2};
-  for (int i = 0; i < 2; ++i)
-    for (int j = 0; j < 2 - i; ++j)
-      if (a[o[j]][o[j]] < a[o[j + 1]][o[j + 1]]) {
-        const int tmp = o[j];
-        o[j] = o[j + 1];
-        o[j + 1] = tmp;
+  // sort descending: compare-swaps (0, 1), (1, 2), (0, 1) on the diagonal
+  // and the eigenvector columns (constant indices, so everything stays in
+  // registers)
+  double d[3] = {a[0][0], a[1][1], a[2][2]};
+  auto cswap = [&](int i, int j) {
+    if (d[i] < d[j]) {
+      const double t = d[i];
+      d[i] = d[j];
+      d[j] = t;
+      for (int k = 0; k < 3; ++k) {
+        const double v = V[k][i];
+        V[k][i] = V[k][j];
+        V[k][j] = v;
       }
-  double Vs[3][3];
-  for (int k = 0; k < 3; ++k) {
-    w[k] = a[o[k]][o[k]];
-    for (int i = 0; i < 3; ++i) Vs[i][k] = V[i][o[k]];
-  }
-  for (int i = 0; i < 3; ++i)
-    for (int k = 0; k < 3; ++k) V[i][k] = Vs[i][k];
+    }
+  };
+  cswap(0, 1);
+  cswap(1, 2);
+  cswap(0, 1);
+  for (int k = 0; k < 3; ++k) w[k] = d[k];
 }
 
 FNE_HD double safe_denom(double x, double tiny) {
@@ -191,39 +196,56 @@ FNE_HD int point(const double e[6], double c_bar, double sp, double mu, double K
   // d z / d eps: eigenvalues g_k[m] = v_k^T dA_m v_k, I1 = (1, 1, 1, 0, 0, 0)
   const int mi[6] = {0, 1, 2, 0, 1, 0}, mj[6] = {0, 1, 2, 1, 2, 2};
   const double mw[6] = {1.0, 1.0, 1.0, 0.5, 0.5, 0.5};
-  // X[k][l][m] = v_k^T dA_m v_l
-  double X[3][3][6];
-  for (int k = 0; k < 3; ++k)
-    for (int l = 0; l < 3; ++l)
-      for (int m = 0; m < 6; ++m) {
-        const int i = mi[m], j = mj[m];
-        X[k][l][m] = i == j ? V[i][k] * V[i][l] : mw[m] * (V[i][k] * V[j][l] + V[j][k] * V[i][l]);
-      }
-  double dz[4][6];
-  for (int k = 0; k < 3; ++k)
-    for (int m = 0; m < 6; ++m) dz[k][m] = X[k][k][m];
-  for (int m = 0; m < 6; ++m) dz[3][m] = m < 3 ? 1.0 : 0.0;
+  // dz[k][m] = v_k^T dA_m v_k (eigenvalue k), dz[3] = d I1; Xp[r][m] =
+  // v_k^T dA_m v_j for the pairs (k, j) = (0, 1), (0, 2), (1, 2)
+  const int pk[3] = {0, 0, 1}, pj[3] = {1, 2, 2};
+  double dz[4][6], Xp[3][6];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const int i = mi[m], j = mj[m];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dz[k][m] = i == j ? V[i][k] * V[i][k] : 2.0 * mw[m] * V[i][k] * V[j][k];
+    dz[3][m] = m < 3 ? 1.0 : 0.0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int k = pk[r], l = pj[r];
+      Xp[r][m] = i == j ? V[i][k] * V[i][l] : mw[m] * (V[i][k] * V[j][l] + V[j][k] * V[i][l]);
+    }
+  }
+#pragma unroll
   for (int m = 0; m < 6; ++m) {
     double s = wQ * (m < 3 ? 2.0 * e[m] : e[m]);
     for (int a = 0; a < 4; ++a) s += Fz[a] * dz[a][m];
     sig[m] = s;
   }
+  // eigenvalue curvature, one term per pair k < j:
+  // 2 (Fz_k - Fz_j) / (lambda_k - lambda_j) Xp[m] Xp[n].  Summing the pair
+  // once avoids the cancellation of two ~1/(lambda_k - lambda_j) terms; a
+  // pair with Fz_k == Fz_j, or with coincident eigenvalues (tie-break
+  // absorbed), contributes 0 instead of 0/0.
+  double cp[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const double dF = Fz[pk[r]] - Fz[pj[r]], dl = lam[pk[r]] - lam[pj[r]];
+    cp[r] = (dF != 0.0 && dl != 0.0) ? 2.0 * dF / dl : 0.0;
+  }
+  // D = dz^T Fzz dz + wQ diag(2, 2, 2, 1, 1, 1) + curvature, through
+  // G = Fzz dz; the upper triangle, mirrored
+  double G[4][6];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int n = 0; n < 6; ++n) G[a][n] = Fzz[a][0] * dz[0][n] + Fzz[a][1] * dz[1][n] + Fzz[a][2] * dz[2][n] +
+                                          Fzz[a][3] * dz[3][n];
+#pragma unroll
   for (int m = 0; m < 6; ++m)
-    for (int n = 0; n < 6; ++n) {
+#pragma unroll
+    for (int n = m; n < 6; ++n) {
       double s = (m == n) ? wQ * (m < 3 ? 2.0 : 1.0) : 0.0;
-      for (int a = 0; a < 4; ++a)
-        for (int b = 0; b < 4; ++b) s += Fzz[a][b] * dz[a][m] * dz[b][n];
-      // eigenvalue curvature, one term per pair k < j (X[k][j] = X[j][k]):
-      // 2 (Fz_k - Fz_j) / (lambda_k - lambda_j) X_kj[m] X_kj[n].  Summing the
-      // pair once avoids the cancellation of two ~1/(lambda_k - lambda_j)
-      // terms; a pair with Fz_k == Fz_j, or with coincident eigenvalues
-      // (tie-break absorbed), contributes 0 instead of 0/0.
-      for (int k = 0; k < 2; ++k)
-        for (int j = k + 1; j < 3; ++j) {
-          const double dF = Fz[k] - Fz[j], dl = lam[k] - lam[j];
-          if (dF != 0.0 && dl != 0.0) s += 2.0 * dF / dl * X[k][j][m] * X[k][j][n];
-        }
+      s += dz[0][m] * G[0][n] + dz[1][m] * G[1][n] + dz[2][m] * G[2][n] + dz[3][m] * G[3][n];
+      s += cp[0] * Xp[0][m] * Xp[0][n] + cp[1] * Xp[1][m] * Xp[1][n] + cp[2] * Xp[2][m] * Xp[2][n];
       D[m][n] = s;
+      D[n][m] = s;
     }
   return br;
 }

@@ -287,7 +287,7 @@ def mc3d_host(tmp_path_factory):
 
 @pytest.mark.parametrize("branch", [0, 1, 2, 3, 4])
 def test_device_point_function_on_host(mc3d_host, branch):
-    """fne_mc3d_point.cuh (the future kernel's per-point code: Jacobi eigen
+    """fne_mc3d_point.cuh (k_mc3d_elem's per-point code: Jacobi eigen
     solve, branch potentials as quadratic forms, spectral chain rule), compiled
     for the host, against the oracle: branch, psi, sigma and D."""
     eps, c, sp, br = _sample_branches()
