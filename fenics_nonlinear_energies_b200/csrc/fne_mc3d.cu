@@ -308,6 +308,118 @@ __global__ void __launch_bounds__(32 * kM3Warps, 3) k_mc3d_elem(Mc3dArgs A, Real
   }
 }
 
+// P4 tetrahedra (35 nodes, up to kM3MaxQHi points): the same point tiles;
+// the contraction keeps one node b at a time, (w D) B(b) at every point of
+// the element in shared memory, and lanes over the nodes a <= b accumulate
+// B(a)^T (w D) B(b) over the points, reading the basis gradients of a from
+// global memory (the 3 x nq x 35 gradient table of one element does not fit
+// beside the point tiles).
+constexpr int kM3MaxQHi = 32;
+
+template <typename Real, int NP, int WANT>
+__global__ void __launch_bounds__(32 * kM3Warps) k_mc3d_elem_hi(Mc3dArgs A, Real* __restrict__ kbuf,
+                                                                Real* __restrict__ gbuf) {
+  constexpr int N = 3 * NP, NPAIR = NP * (NP + 1) / 2, NT = 32 * kM3Warps;
+  __shared__ Real s_sig[NT][6];
+  __shared__ Real s_D[NT][21];
+  __shared__ Real s_T[kM3Warps][kM3MaxQHi][18];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nq = A.nq, epc = NT / nq;
+  double eacc = 0.0;
+  for (int el0 = blockIdx.x * epc; el0 < A.n_el; el0 += gridDim.x * epc) {
+    const int ne = min(epc, A.n_el - el0);
+    if ((int)threadIdx.x < ne * nq) {
+      const int j = threadIdx.x / nq, q = threadIdx.x - j * nq, el = el0 + j;
+      const double wpsi = m3_point_update<Real, NP>(A.grad, A.codes, A.u, A.dir, A.pt, el, q, nq, A.tiny,
+                                                    A.elastic, s_sig[threadIdx.x], s_D[threadIdx.x]);
+      if ((WANT & 1) && __ldg(A.wflag + el)) eacc += wpsi;
+    }
+    __syncthreads();
+    for (int j = warp; (WANT & 6) && j < ne; j += kM3Warps) {
+      const int el = el0 + j;
+      const Real(*sg)[6] = s_sig + j * nq;
+      const Real(*sD)[21] = s_D + j * nq;
+      const double* gx_ = A.grad + (long long)el * 3 * nq * NP;
+      const double* gy_ = gx_ + nq * NP;
+      const double* gz_ = gy_ + nq * NP;
+      if (WANT & 2) {
+        for (int i = lane; i < N; i += 32) {
+          const int a = i / 3, c = i - 3 * a;
+          Real s = Real(0);
+          for (int q = 0; q < nq; ++q) {
+            Real b[6];
+            m3_bcol<Real>((Real)__ldg(gx_ + q * NP + a), (Real)__ldg(gy_ + q * NP + a), (Real)__ldg(gz_ + q * NP + a),
+                          c, b);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) s += b[k] * sg[q][k];
+          }
+          gbuf[(long long)el * N + i] = s;
+        }
+      }
+      if (WANT & 4) {
+        for (int b = 0; b < NP; ++b) {
+          for (int q = lane; q < nq; q += 32) {
+            const Real* Dq = sD[q];
+            Real D[6][6];
+            int t = 0;
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+#pragma unroll
+              for (int k = i; k < 6; ++k) {
+                D[i][k] = Dq[t];
+                D[k][i] = Dq[t];
+                ++t;
+              }
+            const Real gx = (Real)__ldg(gx_ + q * NP + b), gy = (Real)__ldg(gy_ + q * NP + b),
+                       gz = (Real)__ldg(gz_ + q * NP + b);
+            Real* T = s_T[warp][q];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+              T[i * 3 + 0] = D[i][0] * gx + D[i][3] * gy + D[i][5] * gz;
+              T[i * 3 + 1] = D[i][1] * gy + D[i][3] * gx + D[i][4] * gz;
+              T[i * 3 + 2] = D[i][2] * gz + D[i][4] * gy + D[i][5] * gx;
+            }
+          }
+          __syncwarp();
+          for (int a = lane; a <= b; a += 32) {
+            Real K[3][3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+              for (int d = 0; d < 3; ++d) K[c][d] = Real(0);
+            for (int q = 0; q < nq; ++q) {
+              const Real ax = (Real)__ldg(gx_ + q * NP + a), ay = (Real)__ldg(gy_ + q * NP + a),
+                         az = (Real)__ldg(gz_ + q * NP + a);
+              const Real* T = s_T[warp][q];
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                K[0][d] += ax * T[0 * 3 + d] + ay * T[3 * 3 + d] + az * T[5 * 3 + d];
+                K[1][d] += ay * T[1 * 3 + d] + ax * T[3 * 3 + d] + az * T[4 * 3 + d];
+                K[2][d] += az * T[2 * 3 + d] + ay * T[4 * 3 + d] + ax * T[5 * 3 + d];
+              }
+            }
+            // pair (a, b), a <= b, in row-major upper-triangle order
+            const int p = a * NP - a * (a - 1) / 2 + (b - a);
+            Real* o = kbuf + ((long long)el * NPAIR + p) * 9;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+              for (int d = 0; d < 3; ++d) o[c * 3 + d] = K[c][d];
+          }
+          __syncwarp();
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (WANT & 1) {
+    if (A.rhs)  // load term -f.u of the owned DOFs
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n_owned; i += gridDim.x * blockDim.x)
+        eacc -= A.rhs[i] * A.u[A.lo + i];
+    m3_energy_finalize(eacc, A);
+  }
+}
+
 }  // namespace
 
 struct Mc3dHandle {
@@ -348,8 +460,9 @@ template <typename Real>
 int m3_ctas_per_sm(int np) {
   int n = 0;
   const cudaError_t e =
-      np == 10 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mc3d_elem<Real, 10, 7>, 32 * kM3Warps, 0)
-               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mc3d_elem<Real, 4, 7>, 32 * kM3Warps, 0);
+      np == 35   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mc3d_elem_hi<Real, 35, 7>, 32 * kM3Warps, 0)
+      : np == 10 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mc3d_elem<Real, 10, 7>, 32 * kM3Warps, 0)
+                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mc3d_elem<Real, 4, 7>, 32 * kM3Warps, 0);
   return e == cudaSuccess && n > 0 ? n : 2;
 }
 
@@ -362,15 +475,24 @@ cudaError_t m3_launch(Mc3dHandle* h, int flags, const double* u, double* energy,
   Real* kb = static_cast<Real*>(h->kbuf);
   Real* gb = static_cast<Real*>(h->gbuf);
   const dim3 grid(h->grid_elem), block(32 * kM3Warps);
+#define M3_CASE(W)                                                    \
+  case W:                                                             \
+    if constexpr (NP > 10)                                            \
+      k_mc3d_elem_hi<Real, NP, W><<<grid, block, 0, st>>>(A, kb, gb); \
+    else                                                              \
+      k_mc3d_elem<Real, NP, W><<<grid, block, 0, st>>>(A, kb, gb);    \
+    break;
   switch (flags) {
-    case 1: k_mc3d_elem<Real, NP, 1><<<grid, block, 0, st>>>(A, kb, gb); break;
-    case 2: k_mc3d_elem<Real, NP, 2><<<grid, block, 0, st>>>(A, kb, gb); break;
-    case 3: k_mc3d_elem<Real, NP, 3><<<grid, block, 0, st>>>(A, kb, gb); break;
-    case 4: k_mc3d_elem<Real, NP, 4><<<grid, block, 0, st>>>(A, kb, gb); break;
-    case 5: k_mc3d_elem<Real, NP, 5><<<grid, block, 0, st>>>(A, kb, gb); break;
-    case 6: k_mc3d_elem<Real, NP, 6><<<grid, block, 0, st>>>(A, kb, gb); break;
-    default: k_mc3d_elem<Real, NP, 7><<<grid, block, 0, st>>>(A, kb, gb); break;
+    M3_CASE(1)
+    M3_CASE(2)
+    M3_CASE(3)
+    M3_CASE(4)
+    M3_CASE(5)
+    M3_CASE(6)
+    M3_CASE(7)
+    default: return cudaErrorInvalidValue;
   }
+#undef M3_CASE
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !(flags & 6) || h->n_rnodes == 0) return e;
   NodeGatherArgs G{h->n_rnodes, h->bp_rn_blk, h->bp_rn_con, h->bp_rn_row, h->bp_rn_gpos,
@@ -392,6 +514,7 @@ cudaError_t m3_launch(Mc3dHandle* h, int flags, const double* u, double* energy,
 template <typename Real, typename HOut>
 cudaError_t m3_dispatch(Mc3dHandle* h, int flags, const double* u, double* energy, double* grad, void* hess,
                         cudaStream_t st) {
+  if (h->np == 35) return m3_launch<Real, HOut, 35>(h, flags, u, energy, grad, hess, st);
   if (h->np == 10) return m3_launch<Real, HOut, 10>(h, flags, u, energy, grad, hess, st);
   return m3_launch<Real, HOut, 4>(h, flags, u, energy, grad, hess, st);
 }
@@ -412,8 +535,10 @@ int mc3d_create(const fne_desc* d, Mc3dHandle** out) {
   *out = nullptr;
   const int np = d->npe, nq = d->nq, n = 3 * np;
   if (d->block_size != 3) return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: block_size must be 3");
-  if (np != 4 && np != 10) return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: P1 (4 nodes) or P2 (10 nodes) tetrahedra");
-  if (nq < 1 || nq > kM3MaxQ) return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: 1 to 16 quadrature points");
+  if (np != 4 && np != 10 && np != 35)
+    return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: P1 (4 nodes), P2 (10 nodes) or P4 (35 nodes) tetrahedra");
+  if (nq < 1 || nq > (np == 35 ? kM3MaxQHi : kM3MaxQ))
+    return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: 1 to 16 quadrature points (P1, P2) or 1 to 32 (P4)");
   if (d->n_elem > 0 && (!d->e0 || !d->e1 || !d->e2 || !d->e3))
     return set_error(FNE_EINVAL, "Mohr-Coulomb 3-D: missing basis gradients or per-point inputs");
   const int64_t E = d->n_elem, lo = d->lo, hi = d->hi;

@@ -636,15 +636,15 @@ def slope3d_problem(nx=8, ny=2, nz=4, *, degree=2, length=40.0, width=10.0, h_le
     """Synthetic 3-D slope: x in [0, length], y in [0, width], z in [0, H(x)] with
     H = h_left up to x1, linear to h_right at x2, h_right after; a structured
     nx x ny x nz hex grid mapped to that profile, every hex split into six
-    tetrahedra (positively oriented), P1 or P2 nodes in the tetrahedral
+    tetrahedra (positively oriented), P1, P2 or P4 nodes in the tetrahedral
     Lagrange order of ``tet_lagrange_counts``.  Fixed: all components at
     z = 0, u_x at x = 0 and x = length, u_y at y = 0 and y = width.  Davis-B
     reduced strength at ``lam``; gravity ``gamma`` along -z.  Quadrature:
     the reference's rule for the degree (``tet_quadrature_reference``) unless
     ``quad_n`` asks for a Gauss-Jacobi rule.  Returns the element data the
     3-D density needs per element and quadrature point."""
-    if degree not in (1, 2):
-        raise ValueError("degree must be 1 or 2")
+    if degree not in (1, 2, 4):
+        raise ValueError("degree must be 1, 2 or 4")
     xs = np.linspace(0.0, length, nx + 1)
     hx = np.interp(xs, [0.0, x1, x2, length], [h_left, h_left, h_right, h_right])
     nid = np.arange((nx + 1) * (ny + 1) * (nz + 1)).reshape(nx + 1, ny + 1, nz + 1)
@@ -676,6 +676,25 @@ def slope3d_problem(nx=8, ny=2, nz=4, *, degree=2, length=40.0, width=10.0, h_le
                     mids.append(0.5 * (verts[t[a]] + verts[t[b]]))
                 conn[e, 4 + q] = edge_id[key]
         nodes = np.concatenate([verts, np.array(mids)])
+        tets = conn
+    elif degree > 2:
+        # a node is identified by its (vertex, count) pairs with nonzero count,
+        # so edge and face nodes are shared between the tets that meet there;
+        # new nodes are numbered in order of first appearance
+        counts = tet_lagrange_counts(degree)
+        key_id, extra = {}, []
+        conn = np.empty((tets.shape[0], len(counts)), dtype=np.int64)
+        for e, t in enumerate(tets):
+            for m, cnt in enumerate(counts):
+                if max(cnt) == degree:
+                    conn[e, m] = t[cnt.index(degree)]
+                    continue
+                key = tuple(sorted((int(t[i]), c) for i, c in enumerate(cnt) if c))
+                if key not in key_id:
+                    key_id[key] = verts.shape[0] + len(extra)
+                    extra.append(sum(c * verts[t[i]] for i, c in enumerate(cnt)) / degree)
+                conn[e, m] = key_id[key]
+        nodes = np.concatenate([verts, np.array(extra)])
         tets = conn
     n_nodes = nodes.shape[0]
     fixed = np.zeros((n_nodes, 3), dtype=bool)
@@ -721,12 +740,33 @@ KEAST11_C, KEAST11_D = 0.399403576166799, 0.100596423833201
 KEAST11_W = (-0.013155555555555, 0.007622222222222, 0.024888888888888)
 
 
+# P4 tetrahedra: Keast's 24-point rule (exact to degree 6), the reference's
+# digits (src/problems/slope_stability_3d/support/mesh.py:1003-1101): three
+# 4-point orbits (a, a, a, 1 - 3a) and one 12-point orbit of (p, p, q, r);
+# its weights are listed for the unit simplex and divided by 6 there.
+KEAST24_ORBITS4 = ((0.2146028712591517, 0.3561913862225449, 0.0399227502581679),
+                   (0.0406739585346113, 0.8779781243961660, 0.0100772110553207),
+                   (0.3223378901422757, 0.0329863295731731, 0.0553571815436544))
+KEAST24_PQR = (0.0636610018750175, 0.2696723314583159, 0.6030056647916491)
+KEAST24_W12 = 0.0482142857142857
+
+
 def tet_quadrature_reference(degree):
-    """(xi (3, nq), w (nq,)) of the reference's tetrahedral rule for element degree 1 or 2."""
+    """(xi (3, nq), w (nq,)) of the reference's tetrahedral rule for element degree 1, 2 or 4."""
     if degree == 1:
         return np.full((3, 1), 0.25), np.array([1.0 / 6.0])
+    if degree == 4:
+        pts, w = [], []
+        for a, b, wt in KEAST24_ORBITS4:                 # point order (b,a,a) (a,a,a) (a,a,b) (a,b,a)
+            pts += [(b, a, a), (a, a, a), (a, a, b), (a, b, a)]
+            w += [wt] * 4
+        p_, q_, r_ = KEAST24_PQR
+        pts += [(q_, p_, p_), (p_, q_, p_), (p_, p_, q_), (r_, p_, p_), (p_, r_, p_), (p_, p_, r_),
+                (p_, q_, r_), (q_, r_, p_), (r_, p_, q_), (p_, r_, q_), (q_, p_, r_), (r_, q_, p_)]
+        w += [KEAST24_W12] * 12
+        return np.array(pts, dtype=np.float64).T, np.array(w, dtype=np.float64) / 6.0
     if degree != 2:
-        raise ValueError("the reference's tetrahedral rules here: degree 1 or 2")
+        raise ValueError("the reference's tetrahedral rules here: degree 1, 2 or 4")
     a, b, c, d = KEAST11_A, KEAST11_B, KEAST11_C, KEAST11_D
     pts = [(0.25, 0.25, 0.25)]
     pts += [(a, a, a), (b, a, a), (a, b, a), (a, a, b)]                  # orbit (a, a, a, b)

@@ -3,8 +3,8 @@ oracle (``oracle/energies3d.py``: the reference's 3-D density restated, its
 stress and tangent by torch autodiff through ``eigvalsh``).
 
 A synthetic tetrahedral slope (P1: centroid rule; P2: the reference's
-11-point rule), states small enough to stay elastic and large enough to
-reach the plastic branches.  Mesh sizes are chosen with the number of free
+11-point rule; P4: its 24-point rule), states small enough to stay elastic
+and large enough to reach the plastic branches.  Mesh sizes are chosen with the number of free
 DOFs a multiple of 3: the reference's block_xyz permutation takes every
 third free DOF as a node id (reordered_element_base.py:150-161), which the
 layout builders restate.  Bars: FP64 mode 1e-12 relative (energy vs the
@@ -112,6 +112,16 @@ def test_mc3d_p2_matches_oracle_elastic_state(precision):
     p = meshes.slope3d_problem(nx=3, ny=2, nz=1, degree=2, lam=1.5)
     br = _compare(p, precision, amp=1e-5, seed=4)
     assert (br == 0).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_mc3d_p4_matches_oracle(precision):
+    """P4 tetrahedra (35 nodes, the reference's 24-point rule; the node-by-node
+    contraction of k_mc3d_elem_hi) against the oracle, elastic and plastic
+    points mixed."""
+    p = meshes.slope3d_problem(nx=3, ny=1, nz=1, degree=4, lam=1.5)
+    br = _compare(p, precision, amp=2e-2, seed=9)
+    assert len(set(br.tolist())) >= 2
 
 
 def test_mc3d_p1_matches_oracle():

@@ -131,8 +131,9 @@ def test_device_cg_argument_checks_on_host():
 
 def test_mc3d_descriptor_checks_on_host():
     """fne_create for the 3-D Mohr-Coulomb family checks its descriptor on the
-    host before any device call: nodes per element (4 or 10), block size 3,
-    1 to 16 quadrature points and the presence of the per-point arrays."""
+    host before any device call: nodes per element (4, 10 or 35), block size
+    3, 1 to 16 quadrature points (P1, P2) or 1 to 32 (P4) and the presence of
+    the per-point arrays."""
     import ctypes as C
 
     p = meshes.slope3d_problem(nx=2, ny=2, nz=1, degree=1)
@@ -151,7 +152,7 @@ def test_mc3d_descriptor_checks_on_host():
 
     h = C.c_void_p()
     for kw, what in (({"npe": 6}, "tetrahedra"), ({"block_size": 2}, "block_size"), ({"nq": 17}, "quadrature"),
-                     ({}, "missing")):
+                     ({"npe": 35, "nq": 33}, "quadrature"), ({}, "missing")):
         rc = _lib.lib.fne_create(C.byref(desc(**kw)), C.byref(h))
         assert rc == _lib.FNE_EINVAL, (kw, rc)
         assert what in _lib.lib.fne_last_error().decode(), _lib.lib.fne_last_error()

@@ -402,3 +402,32 @@ def test_device_point_near_degenerate_edges(mc3d_host, branch):
         if found == 3:
             break
     assert found == 3
+
+
+def test_p4_tet_rule_and_mesh():
+    """The P4 rule (the reference's 24-point Keast rule): weights sum to the
+    volume 1/6, exact on every monomial of degree <= 6; the P4 slope mesh
+    shares edge and face nodes between its tets (one hex: the 5^3 lattice)."""
+    import math
+
+    from fenics_nonlinear_energies_b200 import meshes
+
+    xi, w = meshes.tet_quadrature_reference(4)
+    assert xi.shape == (3, 24) and w.shape == (24,)
+    assert (xi > 0).all() and (xi.sum(0) < 1).all()
+    assert abs(w.sum() - 1.0 / 6.0) <= 1e-15
+    for i in range(7):
+        for j in range(7 - i):
+            for k in range(7 - i - j):
+                exact = math.factorial(i) * math.factorial(j) * math.factorial(k) / math.factorial(i + j + k + 3)
+                assert abs((w * xi[0] ** i * xi[1] ** j * xi[2] ** k).sum() - exact) <= 1e-14 * exact
+    p = meshes.slope3d_problem(nx=1, ny=1, nz=1, degree=4)
+    assert p["elems_scalar"].shape == (6, 35) and p["nodes"].shape == (125, 3)
+    assert p["dphix"].shape == (6, 24, 35)
+    # the nodes of every element sit at its P4 lattice points
+    pts = meshes.tet_lagrange_points(4)                    # (3, 35)
+    for e in range(6):
+        X = p["nodes"][p["elems_scalar"][e]]               # (35, 3)
+        V = X[:4]
+        np.testing.assert_allclose(X, V[0] + pts.T @ (V[1:] - V[0]), atol=1e-12)
+    np.testing.assert_allclose(p["quad_weight"].sum(), 40.0 * 10.0 * 15.0, rtol=1e-13)
