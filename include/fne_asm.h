@@ -56,7 +56,7 @@ typedef enum {
   FNE_GINZBURG_LANDAU = 2, /* P1 triangles, scalar, eps/2|grad u|^2+W(u) */
   FNE_NEOHOOKEAN = 3,      /* P1 tetrahedra, 3 dofs per node            */
   FNE_MOHR_COULOMB = 4,    /* Pk triangles, plane strain, 2 dofs/node   */
-  FNE_MOHR_COULOMB_3D = 5  /* P1 / P2 tetrahedra, 3 dofs/node           */
+  FNE_MOHR_COULOMB_3D = 5  /* P1 / P2 / P4 tetrahedra, 3 dofs/node      */
 } fne_family;
 
 typedef enum { FNE_FP64 = 0, FNE_FP32 = 1 } fne_precision;
@@ -159,7 +159,8 @@ typedef struct {
    *                    e0 = dphix, e1 = dphiy, e2 = dphiz [E*nq*npe],
    *                    e3 = [E*nq*6] (quad_weight, c_bar_q, sin_phi_q,
    *                    shear_q, bulk_q, lame_q) per point,
-   *                    npe = 4 or 10, block_size = 3, nq <= 16          */
+   *                    npe = 4, 10 or 35, block_size = 3, nq <= 16
+   *                    (P1, P2) or nq <= 32 (P4)                          */
   /* scalars:
    *   p-Laplace : s[0] = p
    *   GL        : s[0] = eps, s[1..9] = ip (3x3 row-major), s[10..12] = w
@@ -210,7 +211,7 @@ typedef struct {
                            * 8 banded sweep, push variant,
                            * 9 Mohr-Coulomb FP64 DMMA (mma.sync f64),
                            * 10 row clusters (P1 triangles),
-                           * 11 3-D Mohr-Coulomb warp-per-element kernel +
+                           * 11 3-D Mohr-Coulomb point-tile element kernel +
                            * node-block gather */
   int32_t row_lanes;      /* lanes per output row of the tet row kernel, else 1 */
 } fne_info;
