@@ -161,9 +161,12 @@ __global__ void __launch_bounds__(256) k_node_gather(NodeGatherArgs G, const Rea
 }
 
 // Shared-block fix-up for bs = 2 (direct-write epilogue): one thread per
-// shared output block sums its contributions (buffer slots of 4 values,
-// listed in element order) and writes the block's two rows.  SB: the
-// buffer's value type (float: tensor-core path; double: FP64 DMMA path).
+// shared output block sums its contributions (slots of 4 values, element
+// order) and writes the block's two rows.  slots == nullptr: the buffer is in
+// fix-up order and the block's contributions are the consecutive slots
+// desc.z .. desc.z + count - 1 (streamed); else they are the buffer slots
+// slots[desc.z .. desc.z + count) (gathered).  SB: the buffer's value type
+// (float: tensor-core path; double: FP64 DMMA path).
 template <typename HOut, typename SB>
 __global__ void __launch_bounds__(256) k_fixup2(int n_blk, const int4* __restrict__ desc,
                                                 const int* __restrict__ slots, const SB* __restrict__ sbuf,
@@ -172,38 +175,56 @@ __global__ void __launch_bounds__(256) k_fixup2(int n_blk, const int4* __restric
     const int4 ds = __ldg(desc + b);
     const int cnt = ds.w & 0xFFFF;
     const unsigned dm = (unsigned)(ds.w >> 16) & 3u;
-    // slot indices several at a time, so several buffer loads are in
-    // flight; the sums keep element order
     SB a00 = 0, a01 = 0, a10 = 0, a11 = 0;
-    const int* sl = slots + ds.z;
-    int j = 0;
-    if constexpr (sizeof(SB) == 4) {
-      const float4* sb = reinterpret_cast<const float4*>(sbuf);
-      for (; j + 4 <= cnt; j += 4) {
-        const float4 v0 = __ldg(sb + __ldg(sl + j)), v1 = __ldg(sb + __ldg(sl + j + 1));
-        const float4 v2 = __ldg(sb + __ldg(sl + j + 2)), v3 = __ldg(sb + __ldg(sl + j + 3));
-        a00 += v0.x; a01 += v0.y; a10 += v0.z; a11 += v0.w;
-        a00 += v1.x; a01 += v1.y; a10 += v1.z; a11 += v1.w;
-        a00 += v2.x; a01 += v2.y; a10 += v2.z; a11 += v2.w;
-        a00 += v3.x; a01 += v3.y; a10 += v3.z; a11 += v3.w;
-      }
-      for (; j < cnt; ++j) {
-        const float4 v = __ldg(sb + __ldg(sl + j));
-        a00 += v.x; a01 += v.y; a10 += v.z; a11 += v.w;
+    if (slots == nullptr) {
+      if constexpr (sizeof(SB) == 4) {
+        const float4* sb = reinterpret_cast<const float4*>(sbuf) + ds.z;
+#pragma unroll 4
+        for (int j = 0; j < cnt; ++j) {
+          const float4 v = __ldg(sb + j);
+          a00 += v.x; a01 += v.y; a10 += v.z; a11 += v.w;
+        }
+      } else {
+        const double2* sb = reinterpret_cast<const double2*>(sbuf) + 2LL * ds.z;
+#pragma unroll 2
+        for (int j = 0; j < cnt; ++j) {
+          const double2 u0 = __ldg(sb + 2 * j), w0 = __ldg(sb + 2 * j + 1);
+          a00 += u0.x; a01 += u0.y; a10 += w0.x; a11 += w0.y;
+        }
       }
     } else {
-      const double2* sb = reinterpret_cast<const double2*>(sbuf);
-      for (; j + 2 <= cnt; j += 2) {
-        const long long p0 = 2LL * __ldg(sl + j), p1 = 2LL * __ldg(sl + j + 1);
-        const double2 u0 = __ldg(sb + p0), w0 = __ldg(sb + p0 + 1);
-        const double2 u1 = __ldg(sb + p1), w1 = __ldg(sb + p1 + 1);
-        a00 += u0.x; a01 += u0.y; a10 += w0.x; a11 += w0.y;
-        a00 += u1.x; a01 += u1.y; a10 += w1.x; a11 += w1.y;
-      }
-      for (; j < cnt; ++j) {
-        const long long p0 = 2LL * __ldg(sl + j);
-        const double2 u0 = __ldg(sb + p0), w0 = __ldg(sb + p0 + 1);
-        a00 += u0.x; a01 += u0.y; a10 += w0.x; a11 += w0.y;
+      // slot indices several at a time, so several buffer loads are in
+      // flight; the sums keep element order
+      const int* sl = slots + ds.z;
+      int j = 0;
+      if constexpr (sizeof(SB) == 4) {
+        const float4* sb = reinterpret_cast<const float4*>(sbuf);
+        for (; j + 4 <= cnt; j += 4) {
+          const float4 v0 = __ldg(sb + __ldg(sl + j)), v1 = __ldg(sb + __ldg(sl + j + 1));
+          const float4 v2 = __ldg(sb + __ldg(sl + j + 2)), v3 = __ldg(sb + __ldg(sl + j + 3));
+          a00 += v0.x; a01 += v0.y; a10 += v0.z; a11 += v0.w;
+          a00 += v1.x; a01 += v1.y; a10 += v1.z; a11 += v1.w;
+          a00 += v2.x; a01 += v2.y; a10 += v2.z; a11 += v2.w;
+          a00 += v3.x; a01 += v3.y; a10 += v3.z; a11 += v3.w;
+        }
+        for (; j < cnt; ++j) {
+          const float4 v = __ldg(sb + __ldg(sl + j));
+          a00 += v.x; a01 += v.y; a10 += v.z; a11 += v.w;
+        }
+      } else {
+        const double2* sb = reinterpret_cast<const double2*>(sbuf);
+        for (; j + 2 <= cnt; j += 2) {
+          const long long p0 = 2LL * __ldg(sl + j), p1 = 2LL * __ldg(sl + j + 1);
+          const double2 u0 = __ldg(sb + p0), w0 = __ldg(sb + p0 + 1);
+          const double2 u1 = __ldg(sb + p1), w1 = __ldg(sb + p1 + 1);
+          a00 += u0.x; a01 += u0.y; a10 += w0.x; a11 += w0.y;
+          a00 += u1.x; a01 += u1.y; a10 += w1.x; a11 += w1.y;
+        }
+        for (; j < cnt; ++j) {
+          const long long p0 = 2LL * __ldg(sl + j);
+          const double2 u0 = __ldg(sb + p0), w0 = __ldg(sb + p0 + 1);
+          a00 += u0.x; a01 += u0.y; a10 += w0.x; a11 += w0.y;
+        }
       }
     }
     const SB r0[2] = {a00, a01}, r1[2] = {a10, a11};

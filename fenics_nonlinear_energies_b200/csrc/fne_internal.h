@@ -197,22 +197,28 @@ struct BlockPlan {
 // element and directed node pair (a -> b) a 16-bit code: 0xFFFF = no output
 // (row or column node without an owned free DOF); bit 15 set = the output
 // block (node(a), node(b)) has several contributing elements, bits 0-14 =
-// this element's slot among its shared blocks (the values go to the shared
-// buffer at (sbase[e] + slot) * bs * bs, row-major (c, d)); else bits 0-11 =
-// column offset of node(b) inside the rows of node(a), bits 12-14 = mask of
-// node(b)'s free components (the element writes the block straight into the
-// COO rows).  fix: node-block plan over the shared blocks only, whose
-// contribution codes are shared-buffer slots (element order per block).
+// this element's slot among its shared blocks (its values go to the shared
+// buffer at position sbase[e] + slot, or sidx[sbase[e] + slot] when the
+// buffer is in fix-up order, bs * bs values row-major (c, d));
+// else bits 0-11 = column offset of node(b) inside the rows of node(a), bits
+// 12-14 = mask of node(b)'s free components (the element writes the block
+// straight into the COO rows).  fix: node-block plan over the shared blocks
+// only, whose contribution codes are element slots (sbase[e] + slot, element
+// order per block).
 struct DirectPlan {
   std::vector<uint16_t> code;   // [n_local * npn * npn]
   std::vector<int32_t> sbase;   // [n_local]
   int64_t n_slots = 0;
   BlockPlan fix;
   // flat fix-up (bs = 2): per shared block 4 ints: COO position of its first
-  // column in row (A, 0) and in row (A, 1) (-1 if absent), first entry in
-  // fix.con (its contributions' buffer slots, element order), and
+  // column in row (A, 0) and in row (A, 1) (-1 if absent), its first entry
+  // in fix.con (= its first buffer position in fix-up order), and
   // count | component mask << 16
   std::vector<int32_t> fdesc;
+  // buffer position of every element slot for a buffer laid out in fix-up
+  // order (sidx[fix.con[j]] = j): the contributions of one shared block then
+  // sit at consecutive positions, in element order
+  std::vector<int32_t> sidx;
 };
 int build_direct_plan(const BlockPlan& bp, int64_t n_local, int npn, int bs, DirectPlan& D);
 

@@ -704,6 +704,9 @@ int build_direct_plan(const BlockPlan& bp, int64_t n_local, int npn, int bs, Dir
     }
   }
   F.n_rnodes = (int32_t)F.rn_blk.size() - 1;
+  // fix-up order of the slots (used when the buffer is laid out that way)
+  D.sidx.assign((size_t)tot, -1);
+  for (size_t j = 0; j < F.con.size(); ++j) D.sidx[(size_t)F.con[j]] = (int32_t)j;
   // flat fix-up (bs = 2): one descriptor per shared block; its contributions
   // are the buffer slots fix.con[start .. start + count)
   if (bs == 2) {
