@@ -225,9 +225,9 @@ __global__ void __launch_bounds__(32 * kM3Warps, 3) k_mc3d_elem(Mc3dArgs A, Real
       }
       // Hessian blocks B(a)^T (w D) B(b) over the node pairs a <= b.  Each
       // column of B has three nonzeros (DOF (b, d) feeds three strain rows), so
-      // per quadrature point the lanes over nodes first form T_b = (w D) B(b)
-      // (6 x 3, 18 products of three terms) and the lanes over pairs then add
-      // B(a)^T T_b (9 sums of three terms)
+      // per quadrature point the lanes first form T_b = (w D) B(b) (6 x 3, 18
+      // products of three terms) and the lanes over pairs then add B(a)^T T_b
+      // (9 sums of three terms)
       if (WANT & 4) {
         constexpr int PPL = (NPAIR + 31) / 32;  // pairs per lane
         Real K[PPL][3][3];
@@ -246,28 +246,34 @@ __global__ void __launch_bounds__(32 * kM3Warps, 3) k_mc3d_elem(Mc3dArgs A, Real
 #pragma unroll
             for (int d = 0; d < 3; ++d) K[k][c][d] = Real(0);
         }
+        // (w D) B(b): lanes over (node b, strain row i), each forming row i
+        // of T_b from row i of w D (upper-triangle positions precomputed)
+        constexpr int NTI = NP * 6, TPL = (NTI + 31) / 32;
+        int tb[TPL], ti[TPL], didx[TPL][6];
+#pragma unroll
+        for (int k = 0; k < TPL; ++k) {
+          const int it = min(lane + 32 * k, NTI - 1);
+          tb[k] = it / 6;
+          ti[k] = it - 6 * tb[k];
+#pragma unroll
+          for (int j = 0; j < 6; ++j) {
+            const int lo = min(ti[k], j), hi = max(ti[k], j);
+            didx[k][j] = lo * 6 - lo * (lo - 1) / 2 + (hi - lo);
+          }
+        }
         for (int q = 0; q < nq; ++q) {
-          if (lane < NP) {
+#pragma unroll
+          for (int k = 0; k < TPL; ++k) {
+            if (lane + 32 * k >= NTI) continue;
             const Real* Dq = sD[q];
-            Real D[6][6];
-            int t = 0;
-#pragma unroll
-            for (int i = 0; i < 6; ++i)
-#pragma unroll
-              for (int j = i; j < 6; ++j) {
-                D[i][j] = Dq[t];
-                D[j][i] = Dq[t];
-                ++t;
-              }
-            const Real gx = s_g[warp][0][q * NP + lane], gy = s_g[warp][1][q * NP + lane],
-                       gz = s_g[warp][2][q * NP + lane];
-            Real* T = s_T[warp][lane];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) {
-              T[i * 3 + 0] = D[i][0] * gx + D[i][3] * gy + D[i][5] * gz;
-              T[i * 3 + 1] = D[i][1] * gy + D[i][3] * gx + D[i][4] * gz;
-              T[i * 3 + 2] = D[i][2] * gz + D[i][4] * gy + D[i][5] * gx;
-            }
+            const Real d0 = Dq[didx[k][0]], d1 = Dq[didx[k][1]], d2 = Dq[didx[k][2]], d3 = Dq[didx[k][3]],
+                       d4 = Dq[didx[k][4]], d5 = Dq[didx[k][5]];
+            const Real gx = s_g[warp][0][q * NP + tb[k]], gy = s_g[warp][1][q * NP + tb[k]],
+                       gz = s_g[warp][2][q * NP + tb[k]];
+            Real* T = s_T[warp][tb[k]] + 3 * ti[k];
+            T[0] = d0 * gx + d3 * gy + d5 * gz;
+            T[1] = d1 * gy + d3 * gx + d4 * gz;
+            T[2] = d2 * gz + d4 * gy + d5 * gx;
           }
           __syncwarp();
 #pragma unroll
