@@ -129,7 +129,7 @@ def test_mc_accepts_reference_problem_data(variant):
 
 
 def test_plaplace_zero_state_matches_reference():
-    """BASELINE's p-Laplace assembly start: energy and gradient at u = 0."""
+    """The p-Laplace configuration's assembly start: energy and gradient at u = 0."""
     from fenics_nonlinear_energies_b200.assembler import PLaplaceCudaAssembler
 
     fx, z = load("plaplace"), load("plaplace_zero")

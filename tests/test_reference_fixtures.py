@@ -102,7 +102,7 @@ def test_host_layout_matches_reference(name):
 
 
 def test_plaplace_zero_state_energy_and_gradient():
-    """BASELINE's p-Laplace assembly start (u = 0): energy and gradient as the reference."""
+    """The p-Laplace configuration's assembly start (u = 0): energy and gradient as the reference."""
     fx, z = load("plaplace"), load("plaplace_zero")
     orc = OracleAssembler("plaplace", fixture_params(fx))
     u = np.zeros(orc.layout.n_free)
