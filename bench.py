@@ -400,14 +400,14 @@ def slope3d_state(params, amplitude=0.05):
     return u.ravel()
 
 
-def _mc3d(nx, ny, nz, precision):
+def _mc3d(nx, ny, nz, precision, degree=2):
     def build(rank):
         import torch
 
         from fenics_nonlinear_energies_b200 import meshes
         from fenics_nonlinear_energies_b200.assembler import SlopeStability3DCudaAssembler
 
-        params = meshes.slope3d_problem(nx=nx, ny=ny, nz=nz, degree=2, lam=1.0)
+        params = meshes.slope3d_problem(nx=nx, ny=ny, nz=nz, degree=degree, lam=1.0)
         hd = torch.float32 if precision == "fp32" else torch.float64
         asm = SlopeStability3DCudaAssembler(params, precision=precision, hess_dtype=hd)
         return asm, _reordered(asm, slope3d_state(params)[params["freedofs"]])
@@ -415,9 +415,10 @@ def _mc3d(nx, ny, nz, precision):
     def sample():
         from fenics_nonlinear_energies_b200 import meshes
 
-        params = meshes.slope3d_problem(nx=2, ny=2, nz=1, degree=2, lam=1.0)
+        n = (2, 2, 1) if degree == 2 else (1, 1, 1)
+        params = meshes.slope3d_problem(nx=n[0], ny=n[1], nz=n[2], degree=degree, lam=1.0)
         return "mc3d", {}, params, slope3d_state(params)[params["freedofs"]], int(params["elems"].shape[0]), \
-            "3-D slope 2x2x1 hexes, P2 tets"
+            f"3-D slope {n[0]}x{n[1]}x{n[2]} hexes, P{degree} tets"
 
     return build, sample
 
@@ -477,6 +478,11 @@ WORKLOADS = {
         "Mohr-Coulomb 3-D slope (length 40, width 10, heights 20 / 10), 40x16x16 hexes x 6 P2 tetrahedra "
         "(61,440 elements), reference 11-point rule, c=6, phi=45 deg, E=2e4, nu=0.3, lambda=1 (Davis-B), smooth "
         "synthetic state, FP64", *_mc3d(40, 16, 16, "fp64")),
+    "mc3d_p4_fp64": Workload(
+        "mc3d_p4_fp64", "mc3d", "fp64", False, 35, 2664, 8, True,
+        "Mohr-Coulomb 3-D slope (length 40, width 10, heights 20 / 10), 23x8x8 hexes x 6 P4 tetrahedra "
+        "(8,832 elements, 35 nodes each), reference 24-point rule, c=6, phi=45 deg, E=2e4, nu=0.3, lambda=1 "
+        "(Davis-B), smooth synthetic state, FP64", *_mc3d(23, 8, 8, "fp64", degree=4)),
     "plaplace128_newton_fp64": Workload(
         "plaplace128_newton_fp64", "plaplace", "fp64", False, 3, 7, 8, True,
         "Newton to ||g|| <= 1e-6 ||g_0||: p-Laplace p=3, f=-10, unit square 128x128 P1 triangles (32,768 "
