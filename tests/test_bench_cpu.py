@@ -89,12 +89,15 @@ def test_reference_arm_runs_the_full_configuration(tmp_path):
 
 
 @pytest.mark.timeout(300)
-def test_reference_arm_line_for_mc3d(tmp_path):
-    """--impl reference on the 3-D Mohr-Coulomb workload: the oracle's element loop on a small slope."""
+@pytest.mark.parametrize("workload", ["mc3d_p2_fp64", "mc3d_p4_fp64"])
+def test_reference_arm_line_for_mc3d(tmp_path, workload):
+    """--impl reference on the 3-D Mohr-Coulomb workloads (P2, P4 tets): the
+    oracle's element loop on a small slope."""
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
-                          "mc3d_p2_fp64", "--steps", "1", "--warmup", "0"], capture_output=True, text=True,
+                          workload, "--steps", "1", "--warmup", "0"], capture_output=True, text=True,
                          cwd=tmp_path, timeout=300)
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
     assert line["impl"] == "reference" and line["unit"] == "elements/s" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["config"]["workload"] == workload
