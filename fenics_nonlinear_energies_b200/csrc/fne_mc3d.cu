@@ -16,7 +16,7 @@
 //
 // k_mc3d_elem: a CTA of 128 threads takes a tile of 128 / nq elements.  One
 // thread per (element, quadrature point) forms the strain and runs the
-// constitutive point function (FP64: eigen-decomposition by fixed-sweep
+// constitutive point function (FP64: eigen-decomposition by cyclic
 // Jacobi, branch potentials, spectral tangent) and stores w sigma and the
 // upper triangle of w D in shared memory.  Then one warp per element: lanes
 // over (node, component) form the element gradient; per quadrature point,

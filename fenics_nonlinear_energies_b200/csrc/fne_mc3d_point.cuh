@@ -35,8 +35,8 @@
 namespace fne {
 namespace mc3d {
 
-// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations (fixed sweep
-// count); w descending, V columns the eigenvectors.
+// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations (at most 6
+// sweeps); w descending, V columns the eigenvectors.
 FNE_HD void eigh3(const double A0[3][3], double w[3], double V[3][3]) {
   double a[3][3];
   for (int i = 0; i < 3; ++i)
@@ -46,11 +46,16 @@ FNE_HD void eigh3(const double A0[3][3], double w[3], double V[3][3]) {
     }
   const int P[3] = {0, 0, 1}, Qi[3] = {1, 2, 2};
   for (int sweep = 0; sweep < 6; ++sweep) {
+    bool rotated = false;
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
       const int p = P[r], q = Qi[r];
       const double apq = a[p][q];
-      if (apq == 0.0) continue;
+      // a rotation by less than one ulp of angle (|t| ~ |apq / (aqq - app)|)
+      // changes nothing beyond rounding: skipped; a sweep without rotations
+      // ends the solve (3 to 4 sweeps for almost every strain)
+      if (apq == 0.0 || fabs(apq) <= 2.220446049250313e-16 * fabs(a[q][q] - a[p][p])) continue;
+      rotated = true;
       const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
       const double t = fabs(theta) > 1e100 ? 0.5 / theta
                                             : (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
@@ -72,6 +77,7 @@ FNE_HD void eigh3(const double A0[3][3], double w[3], double V[3][3]) {
         V[k][q] = s * vkp + c * vkq;
       }
     }
+    if (!rotated) break;
   }
   // sort descending: compare-swaps (0, 1), (1, 2), (0, 1) on the diagonal
   // and the eigenvector columns (constant indices, so everything stays in
