@@ -33,6 +33,14 @@ What is run (reference file:line):
   the reference's connectivity, operator, gravity and free-DOF code given
   that basis, not basix itself.
 * ``davis_b_reduction`` (``slope_stability/support/reduction.py:8-29``).
+* 3-D Mohr-Coulomb element functions (``slope_stability_3d/jax/jax_energy_3d.py``):
+  ``element_energy_3d`` (:214-236), its ``jax.grad`` (``element_residual_3d``,
+  :279) and ``constitutive_element_hessian_3d`` (:324-357, the assembler's
+  ``autodiff_tangent_mode="constitutive"``); the elastic mode's
+  ``elastic_element_energy_3d`` / ``constitutive_elastic_element_hessian_3d``.
+  Inputs: this repository's synthetic 3-D slope (``meshes.slope3d_problem``,
+  P1 / P2 / P4 tets) at a seeded state (``--only mc3d`` writes this fixture
+  alone).
 """
 
 from __future__ import annotations
@@ -237,8 +245,55 @@ def main(reference):
                      ranks=(1, 2) if degree == 2 else (1,), use_near_nullspace=False)
 
 
+def mc3d_case(reference):
+    """Element energy, residual and Hessians of the reference's 3-D density."""
+    refshim.install()
+    sys.path.insert(0, str(reference))
+    import torch
+
+    from src.problems.slope_stability_3d.jax import jax_energy_3d as R3
+
+    from fenics_nonlinear_energies_b200 import meshes
+
+    def t(a):
+        return torch.as_tensor(np.asarray(a, dtype=np.float64))
+
+    store = {}
+    for degree, n, n_el in ((1, (2, 1, 1), 12), (2, (2, 1, 1), 12), (4, (1, 1, 1), 2)):
+        p = meshes.slope3d_problem(nx=n[0], ny=n[1], nz=n[2], degree=degree, lam=1.5)
+        rng = np.random.default_rng(20 + degree)
+        u = p["u_0"].copy()
+        u[p["freedofs"]] = 4e-2 * rng.standard_normal(p["freedofs"].size)
+        keys = ("dphix", "dphiy", "dphiz", "quad_weight", "c_bar", "sin_phi", "shear", "bulk", "lame")
+        out = {k: [] for k in ("energy", "grad", "hess", "el_energy", "el_hess")}
+        ins = {k: np.asarray(p[k][:n_el]) for k in keys}
+        ue = np.stack([u[p["elems"][e]] for e in range(n_el)])
+        t0 = time.perf_counter()
+        for e in range(n_el):
+            args = [t(ins[k][e]) for k in keys]
+            x = t(ue[e])
+            out["energy"].append(float(R3.element_energy_3d(x, *args)))
+            out["grad"].append(R3.element_residual_3d(x, *args).numpy())
+            out["hess"].append(R3.constitutive_element_hessian_3d(x, *args).numpy())
+            el_args = [args[i] for i in (0, 1, 2, 3, 6, 7, 8)]
+            out["el_energy"].append(float(R3.elastic_element_energy_3d(x, *el_args)))
+            out["el_hess"].append(R3.constitutive_elastic_element_hessian_3d(x, *el_args).numpy())
+        print(f"  mc3d P{degree}: {n_el} elements, {time.perf_counter() - t0:.1f} s")
+        store[f"p{degree}_u_elem"] = ue
+        for k, v in ins.items():
+            store[f"p{degree}_{k}"] = v
+        for k, v in out.items():
+            if v:
+                store[f"p{degree}_{k}"] = np.asarray(v)
+    _savez("mc3d", **store)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=["all", "mc3d"], default="all",
+                    help="mc3d: write only the 3-D Mohr-Coulomb element fixture")
     args = ap.parse_args()
-    main(Path(args.reference))
+    if args.only == "all":
+        main(Path(args.reference))
+    mc3d_case(Path(args.reference))

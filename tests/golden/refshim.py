@@ -106,7 +106,7 @@ def _make_jnp():
         return torch.where(c, a, b)
 
     jnp.where = _where
-    jnp.einsum = lambda spec, *ops: torch.einsum(spec, *[_tensor(o) for o in ops])
+    jnp.einsum = lambda spec, *ops, **_kw: torch.einsum(spec, *[_tensor(o) for o in ops])  # optimize= ignored
     jnp.stack = lambda xs, axis=0: torch.stack([_tensor(v) for v in xs], dim=axis)
     jnp.concatenate = lambda xs, axis=0: torch.cat([_tensor(v) for v in xs], dim=axis)
     jnp.zeros = lambda shape, dtype=F64: torch.zeros(shape, dtype=_dt(dtype))

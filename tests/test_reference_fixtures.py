@@ -10,7 +10,9 @@ in for JAX).  These CPU tests check, on the same inputs:
 * the host C++ layout (``fne_layout_build`` through the C ABI) bit-exact;
 * this repository's mesh generators: the structured P1 geometry, the
   Neo-Hookean twist, the P2 slope generator and the P4 same-mesh builder
-  reproduce the reference's arrays; Davis-B values.
+  reproduce the reference's arrays; Davis-B values;
+* the 3-D oracle against the reference's 3-D element functions (energy,
+  residual, constitutive Hessian, elastic mode) on P1 / P2 / P4 tets.
 """
 
 from pathlib import Path
@@ -198,3 +200,45 @@ def test_geometry_recovered_from_reference_elem_B(degree):
     np.testing.assert_allclose(inv, ref_inv, rtol=0, atol=1e-13 * np.abs(ref_inv).max())
     ref_det = p["det_j"] if p["det_j"].ndim == 2 else np.broadcast_to(p["det_j"][:, None], det.shape)
     np.testing.assert_allclose(det, ref_det, rtol=1e-13)
+
+
+@pytest.mark.parametrize("degree", [1, 2, 4])
+def test_mc3d_oracle_matches_reference_elements(degree):
+    """The 3-D oracle (``oracle/energies3d.py``) against the reference's own
+    3-D element functions run on the same inputs (``reference_mc3d.npz``:
+    ``element_energy_3d``, ``element_residual_3d``,
+    ``constitutive_element_hessian_3d`` and the elastic mode's energy and
+    constitutive Hessian of ``slope_stability_3d/jax/jax_energy_3d.py``),
+    P1 / P2 / P4 tets at a state that reaches every return branch: 1e-12
+    relative (energy to |e|, gradient and Hessian to their largest entry)."""
+    from oracle import energies3d as E3
+
+    d = np.load(GOLDEN / "reference_mc3d.npz")
+    keys = ("dphix", "dphiy", "dphiz", "quad_weight", "c_bar", "sin_phi", "shear", "bulk", "lame")
+    ue = d[f"p{degree}_u_elem"]
+    branches = []
+    for e in range(ue.shape[0]):
+        args = [d[f"p{degree}_{k}"][e] for k in keys]
+        ee, ge, He, br = E3.element_derivatives(ue[e], *args)
+        branches.append(br)
+        er, gr, hr = float(d[f"p{degree}_energy"][e]), d[f"p{degree}_grad"][e], d[f"p{degree}_hess"][e]
+        assert abs(ee - er) <= 1e-12 * abs(er), (e, ee, er)
+        assert np.abs(ge - gr).max() <= 1e-12 * np.abs(gr).max(), e
+        assert np.abs(He - hr).max() <= 1e-12 * np.abs(hr).max(), e
+        # elastic mode: psi = lame/2 I1^2 + mu Q, tangent C (closed form)
+        dphix, dphiy, dphiz, w = args[:4]
+        shear, lame = args[6], args[8]
+        eps = E3.strain6(ue[e], dphix, dphiy, dphiz)
+        B = E3.strain_operator(dphix, dphiy, dphiz)
+        C = np.zeros((eps.shape[0], 6, 6))
+        C[:, :3, :3] = lame[:, None, None]
+        for i in range(3):
+            C[:, i, i] += 2.0 * shear
+            C[:, 3 + i, 3 + i] = shear
+        el_e = float(np.sum(w * E3.elastic_density(eps, shear, lame)))
+        el_h = np.einsum("qsi,qst,qtj,q->ij", B, C, B, w)
+        assert abs(el_e - float(d[f"p{degree}_el_energy"][e])) <= 1e-12 * abs(el_e)
+        ref_h = d[f"p{degree}_el_hess"][e]
+        assert np.abs(el_h - ref_h).max() <= 1e-12 * np.abs(ref_h).max()
+    if degree > 1:  # the fixture states reach the plastic branches
+        assert len(set(np.concatenate(branches).tolist())) >= 4
