@@ -431,3 +431,27 @@ def test_p4_tet_rule_and_mesh():
         V = X[:4]
         np.testing.assert_allclose(X, V[0] + pts.T @ (V[1:] - V[0]), atol=1e-12)
     np.testing.assert_allclose(p["quad_weight"].sum(), 40.0 * 10.0 * 15.0, rtol=1e-13)
+
+
+def test_device_point_function_matches_reference_elements(mc3d_host):
+    """The kernels' point function (fne_mc3d_point.cuh, compiled for the host)
+    contracted over P2 elements against the reference's own 3-D element
+    functions (tests/golden/reference_mc3d.npz: element_energy_3d,
+    element_residual_3d, constitutive_element_hessian_3d of
+    slope_stability_3d/jax/jax_energy_3d.py on the same inputs): 1e-12
+    relative to the energy, and to the largest gradient / Hessian entry over
+    the elements (an apex element's tangent is pure rounding of cancelling
+    terms, ~1e-11 against entries of ~1e4)."""
+    from pathlib import Path
+
+    d = np.load(Path(__file__).resolve().parent / "golden" / "reference_mc3d.npz")
+    ue = d["p2_u_elem"]
+    gs, hs = np.abs(d["p2_grad"]).max(), np.abs(d["p2_hess"]).max()
+    for e in range(ue.shape[0]):
+        prm = np.stack([d[f"p2_{k}"][e] for k in ("c_bar", "sin_phi", "shear", "bulk", "lame")], axis=1)
+        en, g, K = mc3d_host.element(ue[e], d["p2_dphix"][e], d["p2_dphiy"][e], d["p2_dphiz"][e],
+                                     d["p2_quad_weight"][e], prm)
+        er, gr, hr = float(d["p2_energy"][e]), d["p2_grad"][e], d["p2_hess"][e]
+        assert abs(en - er) <= 1e-12 * abs(er), (e, en, er)
+        assert np.abs(g - gr).max() <= 1e-12 * gs, e
+        assert np.abs(K - hr).max() <= 1e-12 * hs, e
